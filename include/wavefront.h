@@ -1,0 +1,350 @@
+/*
+ * wavefront.h -- C ABI of the B200 wavefront path tracer.
+ *
+ * Every entry point takes plain pointers and sizes, returns a wf_status and
+ * never exits the process.  Objects are not thread-safe: use one renderer per
+ * host thread.  All device work of a renderer runs on the stream it was
+ * created with.
+ *
+ * Each declaration cites the reference interface it replaces
+ * (Gh05ts/Wavefront-Path-Tracer, paths relative to that project).
+ */
+#ifndef WAVEFRONT_H
+#define WAVEFRONT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef int32_t wf_status;
+enum {
+    WF_OK = 0,
+    WF_ERR_INVALID_ARG = 1,
+    WF_ERR_OOM = 2,
+    WF_ERR_CUDA = 3,
+    WF_ERR_TIMEOUT = 4,
+    WF_ERR_FINGERPRINT = 5,
+    WF_ERR_CAPACITY = 6,
+    WF_ERR_IO = 7,
+    WF_ERR_FORMAT = 8,
+    WF_ERR_UNSUPPORTED = 9,
+    WF_ERR_STATE = 10
+};
+
+/* Thread-local text of the last error reported by this library. */
+const char* wf_last_error(void);
+/* Library version string ("wavefront-b200 <major>.<minor>"). */
+const char* wf_version(void);
+
+/* ------------------------------------------------------------------ scene */
+/* MaterialType, include/scene/material.cuh:22-28 */
+enum { WF_MAT_DIFFUSE = 0, WF_MAT_METAL = 1, WF_MAT_DIELECTRIC = 2,
+       WF_MAT_EMISSIVE = 3, WF_MAT_SPECGLOSS = 4 };
+/* AccelerationMode, include/scene/scene.cuh:21 (Bvh = 0, Direct = 1) */
+enum { WF_ACCEL_BVH = 0, WF_ACCEL_DIRECT = 1 };
+/* PunctualLightType, include/scene/punctual_light.cuh:6 */
+enum { WF_LIGHT_POINT = 0, WF_LIGHT_SPOT = 1, WF_LIGHT_DIRECTIONAL = 2 };
+enum { WF_NO_MATERIAL = 0xffffffffu };
+
+/* Material, include/scene/material.cuh:30-70 (texture bindings are not
+ * carried: every material is untextured, so texture lookups return the
+ * factors exactly as device_traversal.cuh:351-356 does without a texture). */
+typedef struct wf_material {
+    uint32_t type;
+    float albedo[3];
+    float emission[3];
+    float roughness;
+    float ior;
+    float dispersion;
+    float metallic;
+    float attenuation_color[3];
+    float attenuation_distance;
+    float volume_density;
+    float opacity;
+    float alpha_cutoff;
+    uint32_t alpha_masked;
+    uint32_t specgloss_workflow;
+    uint32_t gltf_pbr;
+    float specular[3];
+    float glossiness;
+    float specular_weight;
+    float specular_color[3];
+    float clearcoat;
+    float clearcoat_roughness;
+} wf_material;
+
+/* Fills the reference's default member values (material.cuh:30-70) with
+ * roughness 0 and ior 1 as makeMaterial sets them (src/scene/scene_host.cpp:44-52). */
+void wf_material_default(wf_material* material, uint32_t type);
+
+/* Triangle, include/scene/geometry.cuh:13-45 (positions, optional vertex
+ * normals and material; texture coordinates and tangents are not carried). */
+typedef struct wf_triangle {
+    float v0[3], v1[3], v2[3];
+    float n0[3], n1[3], n2[3];
+    uint32_t material;
+    uint32_t has_vertex_normals;
+} wf_triangle;
+
+/* SceneSphere, include/scene/scene_host.hpp:8-14 */
+typedef struct wf_sphere {
+    float center[3];
+    float radius;
+    uint32_t material;
+    uint32_t accel; /* WF_ACCEL_BVH: TLAS leaf; WF_ACCEL_DIRECT: tested directly */
+} wf_sphere;
+
+/* MeshAsset, include/scene/scene.cuh:117-119 */
+typedef struct wf_mesh {
+    const wf_triangle* triangles;
+    uint32_t triangle_count;
+} wf_mesh;
+
+/* SceneInstance + InstanceTransform, include/scene/scene.cuh:27-35,121-126.
+ * local_to_world[i] / world_to_local[i] are the reference's X, Y, Z basis
+ * vectors (localToWorldX = local_to_world[0], ...). */
+typedef struct wf_instance {
+    uint32_t mesh;
+    uint32_t material_override; /* WF_NO_MATERIAL = none */
+    uint32_t accel;
+    float local_to_world[3][3];
+    float world_to_local[3][3];
+    float translation[3];
+} wf_instance;
+
+/* PunctualLight, include/scene/punctual_light.cuh:8-16 */
+typedef struct wf_punctual_light {
+    uint32_t type;
+    float position[3];
+    float direction[3];
+    float intensity[3];
+    float range;
+    float inner_cone_cos;
+    float outer_cone_cos;
+} wf_punctual_light;
+
+/* HostEnvironment pixels (include/scene/environment.hpp:6-11): width*height
+ * RGBA float texels, row 0 = top (+Y). */
+typedef struct wf_environment {
+    uint32_t width;
+    uint32_t height;
+    const float* rgba;
+    float intensity;
+    float rotation_degrees;
+} wf_environment;
+
+/* HostScene, include/scene/scene_host.hpp:19-33 */
+typedef struct wf_scene_desc {
+    const wf_sphere* spheres;
+    uint32_t sphere_count;
+    const wf_triangle* triangles;        /* HostScene::triangles (own BVH2) */
+    uint32_t triangle_count;
+    const wf_triangle* static_triangles; /* HostScene::staticTriangles (linear) */
+    uint32_t static_triangle_count;
+    const wf_mesh* meshes;
+    uint32_t mesh_count;
+    const wf_instance* instances;
+    uint32_t instance_count;
+    const wf_material* materials;
+    uint32_t material_count;
+    const wf_punctual_light* punctual_lights;
+    uint32_t punctual_light_count;
+    uint32_t black_background;
+    uint32_t ignore_direct_light_occlusion;
+    /* 1 = register emissive mesh and static triangles as NEE lights in the
+     * order the reference's scene assembly does (addMeshTriangleLights then
+     * addStaticTriangleLights, src/scene/scene_host.cpp:60-106). */
+    uint32_t register_triangle_lights;
+    uint32_t build_threads; /* 0 = all host threads */
+} wf_scene_desc;
+
+typedef struct wf_scene wf_scene;
+
+/* Host-side acceleration/light build + device upload.
+ * Replaces DeviceScene uploadScene(const HostScene&), src/scene/scene.cu:336-389. */
+wf_status wf_scene_create(const wf_scene_desc* desc, wf_scene** out);
+/* Replaces uploadEnvironmentMap(DeviceScene&, const HostEnvironment&, float, float),
+ * src/scene/scene.cu:308-334, including buildEnvironmentDistribution
+ * (src/scene/environment.cpp:10-64).  env == NULL clears the map
+ * (clearEnvironmentMap, scene.cu:298-306). */
+wf_status wf_scene_set_environment(wf_scene* scene, const wf_environment* env);
+/* Replaces destroyDeviceScene, src/scene/scene.cu:391-420. */
+wf_status wf_scene_destroy(wf_scene* scene);
+
+typedef struct wf_scene_info {
+    uint32_t light_count;
+    uint32_t tlas_leaf_count;
+    uint32_t blas_count;
+    uint32_t material_count;
+    uint64_t device_bytes;
+    double build_seconds;
+} wf_scene_info;
+wf_status wf_scene_get_info(const wf_scene* scene, wf_scene_info* info);
+
+/* ------------------------------------------------------- ray-level queries */
+/* One ray: origin xyz, direction xyz (float). */
+typedef struct wf_ray {
+    float origin[3];
+    float direction[3];
+} wf_ray;
+
+/* Closest hit of one ray, the fields of Hit (include/scene/geometry.cuh:68-82)
+ * the shading stage uses plus the winning primitive's identity. */
+typedef struct wf_hit {
+    float t;
+    float position[3];
+    float geometric_normal[3];
+    float normal[3];
+    uint32_t material;    /* WF_NO_MATERIAL on a miss */
+    uint32_t light_index; /* 0xffffffff when not a registered light */
+    uint32_t kind;        /* WF_HIT_* */
+    uint32_t instance;    /* instance index for WF_HIT_MESH, else 0xffffffff */
+    uint32_t primitive;   /* sphere / triangle index within its list or mesh */
+    float u, v;           /* barycentrics (triangles) */
+} wf_hit;
+enum { WF_HIT_NONE = 0, WF_HIT_MESH = 1, WF_HIT_STATIC_TRIANGLE = 2,
+       WF_HIT_TRIANGLE = 3, WF_HIT_SPHERE = 4 };
+
+/* Batched traceRay (device_traversal.cuh:1115-1184).  rays/hits are DEVICE
+ * pointers; the call is asynchronous on `stream` (cudaStream_t, may be NULL). */
+wf_status wf_trace_closest(const wf_scene* scene, const wf_ray* rays, uint32_t count,
+                           wf_hit* hits, void* stream);
+/* Batched isOccluded (device_traversal.cuh:1035-1113): occluded[i] = 1 when
+ * something is hit at t < max_distance[i].  Device pointers, asynchronous. */
+wf_status wf_trace_any(const wf_scene* scene, const wf_ray* rays, const float* max_distance,
+                       uint32_t count, uint8_t* occluded, void* stream);
+
+/* ------------------------------------------------------------------ render */
+/* Camera, include/scene/camera.cuh:7-28 */
+typedef struct wf_camera {
+    float position[3];
+    float forward[3];
+    float right[3];
+    float up[3];
+    float vertical_fov; /* radians */
+    float aspect_ratio;
+} wf_camera;
+
+enum { WF_MODE_GRAPH = 0, WF_MODE_PERSISTENT = 1 };
+enum { WF_RNG_XORSHIFT32 = 0, WF_RNG_PCG32 = 1 };
+enum { WF_DEBUG_NONE = 0, WF_DEBUG_INTERSECTION = 1, WF_DEBUG_SHADING_NORMAL = 2 };
+
+/* RenderConfig, include/config.hpp:11-41 (the fields the render loop reads). */
+typedef struct wf_render_config {
+    uint32_t width, height;
+    uint32_t max_depth;
+    uint32_t rr_start_depth;
+    uint32_t mode;             /* WF_MODE_* */
+    uint32_t rng;              /* WF_RNG_* */
+    float indirect_clamp;      /* 0 disables */
+    uint32_t tile_width;       /* 0 = full frame; bounds queue memory */
+    uint32_t tile_height;
+    uint32_t block_size;       /* 0 = tuned default */
+    uint32_t persistent_blocks;/* 0 = SMs x resident blocks */
+    uint32_t chunk;            /* persistent work chunk in paths, 0 = default */
+    uint32_t debug;            /* WF_DEBUG_* */
+    /* photon caustics, src/renderer/photon_mapping.cu + render_driver.cu:180-234 */
+    uint32_t caustics;
+    uint32_t caustic_gather;
+    uint32_t photon_count;
+    uint32_t photon_max_depth;
+    float gather_radius;
+    float photon_grid_min[3];  /* grid bounds; min == max derives them from the scene */
+    float photon_grid_max[3];
+    uint32_t photon_grid_resolution;
+    uint32_t photon_seed;
+    uint32_t spectral;
+    uint32_t profile_queues;   /* record per-bounce queue counts */
+} wf_render_config;
+
+/* Defaults of RenderConfig (config.hpp:11-41) at the given resolution. */
+void wf_render_config_default(wf_render_config* config, uint32_t width, uint32_t height);
+
+typedef struct wf_renderer wf_renderer;
+
+/* Replaces RenderDriver(const DeviceScene&, Camera, RenderConfig, SceneConfig)
+ * + RenderDriver::prepare (render_driver.cu:422-449): validates the config,
+ * sizes the persistent grid, builds the photon map, allocates queues and
+ * captures the bounce chain into a CUDA graph (graph mode).
+ * `stream` is a cudaStream_t (NULL = renderer-owned non-blocking stream). */
+wf_status wf_renderer_create(const wf_scene* scene, const wf_camera* camera,
+                             const wf_render_config* config, void* stream,
+                             wf_renderer** out);
+wf_status wf_renderer_destroy(wf_renderer* renderer);
+
+/* Replaces RenderTaskRenderer::render(const RenderTask&), render_task.cu:26-114:
+ * renders absolute samples [sample_start, sample_start + sample_count) of the
+ * tile.  clear_tile = 1 zeroes the tile first (the task semantics: the tile
+ * then holds the unnormalized sum over the range); 0 accumulates.
+ * Asynchronous on the renderer stream. */
+wf_status wf_render(wf_renderer* renderer, uint32_t x, uint32_t y, uint32_t width,
+                    uint32_t height, uint32_t sample_start, uint32_t sample_count,
+                    uint32_t clear_tile);
+/* Replaces RenderDriver::renderSamples (render_driver.cu:354-401): renders
+ * sample_count samples over all tiles, continuing from the device sample
+ * index, which advances by one per sample.  Asynchronous. */
+wf_status wf_render_frame(wf_renderer* renderer, uint32_t sample_count);
+
+/* resetRenderSession / setRenderSessionSampleIndex / getRenderSessionSampleIndex,
+ * src/renderer/render_session.cu:28-42 */
+wf_status wf_framebuffer_reset(wf_renderer* renderer);
+wf_status wf_set_sample_index(wf_renderer* renderer, uint32_t sample_index);
+wf_status wf_get_sample_index(wf_renderer* renderer, uint32_t* sample_index);
+/* Copies the unnormalized FP32 RGB sums of a tile (row-major, 3 floats per
+ * pixel) into host memory; synchronizes the stream.  (cudaMemcpy2D of
+ * render_task.cu:101-108.) */
+wf_status wf_framebuffer_download(wf_renderer* renderer, uint32_t x, uint32_t y,
+                                  uint32_t width, uint32_t height, float* rgb);
+/* Device address of the width*height*3 float framebuffer. */
+wf_status wf_framebuffer_device(wf_renderer* renderer, float** rgb);
+wf_status wf_synchronize(wf_renderer* renderer);
+
+/* Per-bounce ray-queue sizes of the most recent sample of the most recent
+ * tile (the --profile-queues record, renderer.cu:89-90).  Requires
+ * profile_queues; writes min(n, max_depth) counts. */
+wf_status wf_queue_counts(wf_renderer* renderer, uint32_t* counts, uint32_t n);
+
+typedef struct wf_render_stats {
+    uint64_t extension_rays;
+    uint64_t shadow_rays;
+    uint64_t paths;
+} wf_render_stats;
+/* Ray counters accumulated since creation or the last reset (synchronizes). */
+wf_status wf_render_stats_get(wf_renderer* renderer, wf_render_stats* stats, uint32_t reset);
+
+/* Photon map (buildPhotonMap, render_driver.cu:180-234): number of photons
+ * stored on diffuse surfaces after >= 1 specular bounce. */
+wf_status wf_photon_stats(wf_renderer* renderer, uint32_t* stored, uint32_t* emitted);
+/* Downloads photon records as 8 floats each: position xyz, direction xyz,
+ * flux sum, valid flag (host memory, count = emitted). */
+wf_status wf_photons_download(wf_renderer* renderer, float* records, uint32_t count);
+
+/* -------------------------------------------------------------- checkpoint */
+/* Checkpoint file: header {magic "PTCHKPT1", version 3, width, height,
+ * sampleIndex, fingerprint} + width*height Vec3 (render_checkpoint.cpp:17-63).
+ * wf_checkpoint_save writes via a temporary file and rename. */
+wf_status wf_checkpoint_save(wf_renderer* renderer, const char* path, uint64_t fingerprint);
+/* Asynchronous variant (enqueueRenderSessionCheckpoint, render_checkpoint.cpp:108-138):
+ * copies the framebuffer into one of `slots` pinned buffers on the render
+ * stream and writes it from a worker thread.  *queued = 0 when every slot is
+ * busy (the checkpoint is skipped, as the reference does). */
+wf_status wf_checkpoint_enqueue(wf_renderer* renderer, const char* path, uint64_t fingerprint,
+                                uint32_t* queued);
+/* Waits for queued checkpoint writes (finishAsyncCheckpointWriter). */
+wf_status wf_checkpoint_flush(wf_renderer* renderer);
+/* Replaces loadRenderSessionCheckpoint (render_checkpoint.cpp:163-195); returns
+ * WF_ERR_FORMAT / WF_ERR_FINGERPRINT / WF_ERR_IO instead of exiting. */
+wf_status wf_checkpoint_load(wf_renderer* renderer, const char* path, uint64_t fingerprint,
+                             uint32_t* sample_index);
+/* FNV-1a 64 over bytes (the hash of render_fingerprint.cpp:11-83). */
+uint64_t wf_fnv1a64(const void* data, size_t size, uint64_t seed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WAVEFRONT_H */

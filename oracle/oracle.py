@@ -1,0 +1,147 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY.
+
+Loads the host-compiled reference (oracle/_ref/libwfref.so, built by
+oracle/Makefile from the reference's own sources) and its deterministic-math
+twin (libwfref_det.so: identical code, elementary functions from wf_math.h).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline use this
+module; the product never does.
+"""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+_libs = {}
+
+
+def available(det=False):
+    return (REF_DIR / ("libwfref_det.so" if det else "libwfref.so")).exists()
+
+
+def ref_lib(det=False):
+    """det=False: the reference as written (C-library math); det=True: the
+    reference with the renderer's deterministic elementary functions."""
+    key = bool(det)
+    if key not in _libs:
+        path = REF_DIR / ("libwfref_det.so" if det else "libwfref.so")
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle)")
+        lib = C.CDLL(str(path))
+        P, U32, I = C.c_void_p, C.c_uint32, C.c_int
+        lib.wfref_scene_create.restype = P
+        lib.wfref_scene_create.argtypes = [P, P, I]
+        lib.wfref_scene_destroy.argtypes = [P]
+        lib.wfref_scene_light_count.restype = U32
+        lib.wfref_scene_light_count.argtypes = [P]
+        lib.wfref_scene_lights.argtypes = [P, P, P]
+        lib.wfref_environment_distribution.restype = I
+        lib.wfref_environment_distribution.argtypes = [P, U32, U32, P, P, P]
+        lib.wfref_trace.argtypes = [P, P, U32, P, I]
+        lib.wfref_occluded.argtypes = [P, P, P, U32, P, I]
+        lib.wfref_photons.restype = I
+        lib.wfref_photons.argtypes = [P, P, P, P, P, I]
+        lib.wfref_render.restype = I
+        lib.wfref_render.argtypes = [P, P, P, U32, U32, U32, U32, U32, U32, P, P, P, I, I]
+        lib.wfref_dielectric_reflectance.restype = C.c_float
+        lib.wfref_dielectric_reflectance.argtypes = [C.c_float, C.c_float]
+        lib.wfref_checkpoint_roundtrip_read.restype = I
+        lib.wfref_checkpoint_roundtrip_read.argtypes = [C.c_char_p, U32, U32, C.c_uint64, P, P]
+        lib.wfref_checkpoint_write.restype = I
+        lib.wfref_checkpoint_write.argtypes = [C.c_char_p, U32, U32, C.c_uint64, P, U32]
+        _libs[key] = lib
+    return _libs[key]
+
+
+class RefScene:
+    """The reference's uploadScene() of a wfpt.Scene, in host memory."""
+
+    def __init__(self, scene, det=False, probe=False):
+        from wfpt import abi  # noqa: F401  (layouts shared with the C ABI)
+        self.lib = ref_lib(det)
+        d, keep = scene.desc()
+        env, rgba = scene.environment_struct()
+        self.handle = self.lib.wfref_scene_create(C.addressof(d), C.addressof(env) if env is not None else None,
+                                                  int(probe))
+        del keep, rgba
+        if not self.handle:
+            raise RuntimeError("reference scene creation failed")
+        self.probe = probe
+
+    def close(self):
+        if self.handle:
+            self.lib.wfref_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def light_count(self):
+        return self.lib.wfref_scene_light_count(self.handle)
+
+    def lights(self):
+        n = self.light_count()
+        rec = np.zeros((n, 16), np.float32)
+        alias = np.zeros(n, np.uint32)
+        if n:
+            self.lib.wfref_scene_lights(self.handle, rec.ctypes.data, alias.ctypes.data)
+        return rec, alias
+
+    def trace(self, rays, threads=0):
+        from wfpt import abi
+        rays = np.ascontiguousarray(rays, abi.RAY_DTYPE)
+        hits = np.zeros(len(rays), abi.HIT_DTYPE)
+        self.lib.wfref_trace(self.handle, rays.ctypes.data, len(rays), hits.ctypes.data, threads)
+        return hits
+
+    def occluded(self, rays, max_distance, threads=0):
+        from wfpt import abi
+        rays = np.ascontiguousarray(rays, abi.RAY_DTYPE)
+        md = np.ascontiguousarray(max_distance, np.float32)
+        out = np.zeros(len(rays), np.uint8)
+        self.lib.wfref_occluded(self.handle, rays.ctypes.data, md.ctypes.data, len(rays), out.ctypes.data, threads)
+        return out
+
+    def photons(self, config, threads=0):
+        n = config.photon_count
+        rec = np.zeros((n, 8), np.float32)
+        flux = np.zeros((n, 3), np.float32)
+        stored = C.c_uint32()
+        self.lib.wfref_photons(self.handle, C.addressof(config), rec.ctypes.data, flux.ctypes.data,
+                               C.addressof(stored), threads)
+        return rec, flux, stored.value
+
+    def render(self, camera, config, tile=None, sample_start=0, sample_count=1, threads=0, persistent=False,
+               fp64=False):
+        """Reference captured-graph (or persistent) render of a tile: FP32 sums,
+        optional FP64 sums, per-sample per-bounce queue counts."""
+        from wfpt.native import camera_struct
+        cam = camera_struct(camera)
+        x, y, w, h = tile if tile is not None else (0, 0, config.width, config.height)
+        fb32 = np.zeros((h, w, 3), np.float32)
+        fb64 = np.zeros((h, w, 3), np.float64) if fp64 else None
+        counts = np.zeros((sample_count, config.max_depth), np.uint32)
+        rc = self.lib.wfref_render(self.handle, C.addressof(cam), C.addressof(config), x, y, w, h, sample_start,
+                                   sample_count, fb32.ctypes.data, fb64.ctypes.data if fp64 else None,
+                                   counts.ctypes.data, threads, int(persistent))
+        if rc != 0:
+            raise RuntimeError("reference render failed")
+        return fb32, fb64, counts
+
+
+def environment_distribution(rgba, det=False):
+    """buildEnvironmentDistribution of the reference (environment.cpp:10-64)."""
+    rgba = np.ascontiguousarray(rgba, np.float32)
+    h, w = rgba.shape[:2]
+    p = np.zeros(w * h, np.float32)
+    ap = np.zeros(w * h, np.float32)
+    al = np.zeros(w * h, np.uint32)
+    rc = ref_lib(det).wfref_environment_distribution(rgba.ctypes.data, w, h, p.ctypes.data, ap.ctypes.data,
+                                                     al.ctypes.data)
+    if rc != 0:
+        raise ValueError("environment rejected")
+    return p, ap, al

@@ -1,0 +1,71 @@
+"""The C-ABI library loads on a CPU-only host and exports every entry point
+include/wavefront.h declares (no compute calls without a GPU)."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+
+import wfpt
+from wfpt import abi
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "wavefront.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(wf_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = wfpt.library()
+    names = declared_functions()
+    assert len(names) >= 29
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_mirror_declares_every_symbol():
+    lib = ctypes.CDLL(str(wfpt.native.LIB_PATH))
+    assert sorted(abi.declare(lib)) == declared_functions()
+
+
+def test_struct_layouts_match_header():
+    # Sizes printed by a C compiler for include/wavefront.h on x86-64.
+    assert abi.TRIANGLE_DTYPE.itemsize == 80
+    assert abi.MATERIAL_DTYPE.itemsize == 124
+    assert abi.HIT_DTYPE.itemsize == 68
+    assert ctypes.sizeof(abi.SceneDesc) == 128
+    assert ctypes.sizeof(abi.RenderConfig) == 112
+    assert ctypes.sizeof(abi.Camera) == 56
+
+
+def test_defaults_and_errors_without_gpu():
+    lib = wfpt.library()
+    assert lib.wf_version().decode().startswith("wavefront-b200")
+    cfg = wfpt.render_config(1920, 1080)
+    # RenderConfig defaults, include/config.hpp:11-41.
+    assert (cfg.max_depth, cfg.rr_start_depth, cfg.photon_count, cfg.photon_max_depth) == (32, 12, 1048576, 8)
+    assert abs(cfg.indirect_clamp - 10.0) < 1e-7 and abs(cfg.gather_radius - 0.06) < 1e-7
+    assert cfg.rng == abi.RNG_XORSHIFT32 and cfg.mode == abi.MODE_GRAPH
+    # Invalid descriptions are rejected on the host before any device work.
+    s = wfpt.Scene()
+    s.add_material(wfpt.material(abi.MAT_DIFFUSE, (1, 1, 1)))
+    sp = np.zeros(1, abi.SPHERE_DTYPE)
+    sp[0] = ((0, 0, 0), 1.0, 7, 0)
+    s.spheres = sp
+    d, keep = s.desc()
+    handle = ctypes.c_void_p()
+    status = lib.wf_scene_create(ctypes.byref(d), ctypes.byref(handle))
+    assert status == 1 and b"material" in lib.wf_last_error()
+
+
+def test_fnv1a_matches_reference_constants():
+    lib = wfpt.library()
+    data = np.frombuffer(b"abc", np.uint8)
+    # FNV-1a 64 (render_fingerprint.cpp:11-83): offset basis 1469598103934665603, prime 1099511628211.
+    h = 1469598103934665603
+    for b in b"abc":
+        h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    assert lib.wf_fnv1a64(data.ctypes.data, 3, 0) == h

@@ -1,0 +1,475 @@
+// C ABI entry points (include/wavefront.h).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+
+#include "wf_renderer.h"
+
+namespace wf {
+const char* last_error_text();
+}
+
+using namespace wf;
+
+#define WF_CUDA(call)                                              \
+    do {                                                           \
+        cudaError_t wf_e_ = (call);                                \
+        if (wf_e_ != cudaSuccess) return cuda_fail(wf_e_, #call); \
+    } while (0)
+
+namespace {
+
+template <typename T>
+cudaError_t upload(wf_scene* s, std::vector<void*>& list, uint64_t& bytes, const T** out, const std::vector<T>& v) {
+    *out = nullptr;
+    if (v.empty()) return cudaSuccess;
+    void* p = nullptr;
+    size_t n = sizeof(T) * v.size();
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) return e;
+    list.push_back(p);
+    bytes += n;
+    e = cudaMemcpy(p, v.data(), n, cudaMemcpyHostToDevice);
+    *out = static_cast<const T*>(p);
+    (void)s;
+    return e;
+}
+
+void free_list(std::vector<void*>& list) {
+    for (void* p : list) cudaFree(p);
+    list.clear();
+}
+
+// Checkpoint header, src/renderer/render_checkpoint.cpp:17-27 (v3).
+struct CheckpointHeader {
+    char magic[8];
+    uint32_t version;
+    uint32_t width;
+    uint32_t height;
+    uint32_t sample_index;
+    uint64_t fingerprint;
+};
+static_assert(sizeof(CheckpointHeader) == 32, "checkpoint header layout");
+constexpr char kMagic[8] = {'P', 'T', 'C', 'H', 'K', 'P', 'T', '1'};
+constexpr uint32_t kCheckpointVersion = 3;
+
+wf_status write_checkpoint(const char* path, const float* rgb, uint32_t width, uint32_t height, uint32_t sample,
+                           uint64_t fingerprint) {
+    CheckpointHeader header{};
+    std::memcpy(header.magic, kMagic, 8);
+    header.version = kCheckpointVersion;
+    header.width = width;
+    header.height = height;
+    header.sample_index = sample;
+    header.fingerprint = fingerprint;
+    std::string tmp = std::string(path) + ".tmp";
+    {
+        std::ofstream out(tmp, std::ios::binary | std::ios::trunc);
+        if (!out) return fail(WF_ERR_IO, "Could not open checkpoint for writing: %s", tmp.c_str());
+        out.write(reinterpret_cast<const char*>(&header), sizeof(header));
+        out.write(reinterpret_cast<const char*>(rgb), std::streamsize(sizeof(float) * 3 * size_t(width) * height));
+        out.close();
+        if (!out) return fail(WF_ERR_IO, "Could not write checkpoint: %s", tmp.c_str());
+    }
+    if (std::rename(tmp.c_str(), path) != 0) return fail(WF_ERR_IO, "Could not replace checkpoint: %s", path);
+    return WF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* wf_last_error(void) { return last_error_text(); }
+const char* wf_version(void) { return "wavefront-b200 1.0"; }
+
+void wf_material_default(wf_material* m, uint32_t type) {
+    std::memset(m, 0, sizeof(*m));
+    m->type = type;
+    m->ior = 1.0f;
+    m->attenuation_color[0] = m->attenuation_color[1] = m->attenuation_color[2] = 1.0f;
+    m->volume_density = 1.0f;
+    m->opacity = 1.0f;
+    m->alpha_cutoff = 0.5f;
+    m->specular[0] = m->specular[1] = m->specular[2] = 1.0f;
+    m->glossiness = 1.0f;
+    m->specular_weight = 1.0f;
+    m->specular_color[0] = m->specular_color[1] = m->specular_color[2] = 1.0f;
+}
+
+void wf_render_config_default(wf_render_config* c, uint32_t width, uint32_t height) {
+    std::memset(c, 0, sizeof(*c));
+    c->width = width;
+    c->height = height;
+    c->max_depth = 32;
+    c->rr_start_depth = 12;
+    c->mode = WF_MODE_GRAPH;
+    c->rng = WF_RNG_XORSHIFT32;
+    c->indirect_clamp = 10.0f;
+    c->caustic_gather = 1;
+    c->photon_count = 1048576;
+    c->photon_max_depth = 8;
+    c->gather_radius = 0.06f;
+    c->photon_grid_min[0] = -2.5f; c->photon_grid_min[1] = -1.0f; c->photon_grid_min[2] = -2.5f;
+    c->photon_grid_max[0] = 2.5f;  c->photon_grid_max[1] = 3.0f;  c->photon_grid_max[2] = 2.5f;
+    c->photon_grid_resolution = 64;
+    c->photon_seed = 0x13579bdfu;
+    c->profile_queues = 1;
+}
+
+wf_status wf_scene_create(const wf_scene_desc* desc, wf_scene** out) {
+    if (!out) return fail(WF_ERR_INVALID_ARG, "null output");
+    *out = nullptr;
+    auto t0 = std::chrono::steady_clock::now();
+    HostScene h;
+    if (wf_status e = build_host_scene(desc, h)) return e;
+    auto s = std::make_unique<wf_scene>();
+    WF_CUDA(cudaGetDevice(&s->device));
+    DeviceScene& v = s->view;
+    auto& L = s->allocations;
+    uint64_t& B = s->device_bytes;
+    cudaError_t e = cudaSuccess;
+    auto up = [&](auto** dst, const auto& vec) {
+        if (e == cudaSuccess) e = upload(s.get(), L, B, dst, vec);
+    };
+    up(&v.triangles, h.triangles);
+    up(&v.normals, h.normals);
+    up(&v.nodes, h.nodes);
+    up(&v.blases, h.blases);
+    up(&v.instances, h.instances);
+    up(&v.mesh_linear, h.mesh_linear);
+    up(&v.tlas_leaves, h.tlas_leaves);
+    up(&v.spheres, h.spheres);
+    up(&v.sphere_materials, h.sphere_materials);
+    up(&v.direct_spheres, h.direct_spheres);
+    up(&v.direct_instances, h.direct_instances);
+    up(&v.materials, h.materials);
+    up(&v.lights, h.lights);
+    up(&v.punctual, h.punctual);
+    if (e != cudaSuccess) {
+        free_list(L);
+        return e == cudaErrorMemoryAllocation ? fail(WF_ERR_OOM, "scene upload: out of device memory")
+                                              : cuda_fail(e, "scene upload");
+    }
+    v.env = Environment{};
+    v.tlas = h.tlas;
+    v.direct_bvh = h.direct_bvh;
+    v.static_first = h.static_first;
+    v.static_count = h.static_count;
+    v.direct_first = h.direct_first;
+    v.direct_count = h.direct_count;
+    v.direct_sphere_count = uint32_t(h.direct_spheres.size());
+    v.direct_instance_count = uint32_t(h.direct_instances.size());
+    v.instance_count = uint32_t(h.instances.size());
+    v.material_count = uint32_t(h.materials.size());
+    v.light_count = uint32_t(h.lights.size());
+    v.punctual_count = uint32_t(h.punctual.size());
+    v.directional_count = h.directional_count;
+    v.any_alpha_reject = h.any_alpha_reject ? 1u : 0u;
+    v.black_background = h.black_background ? 1u : 0u;
+    v.ignore_direct_light_occlusion = h.ignore_occlusion ? 1u : 0u;
+    s->light_count = v.light_count;
+    s->tlas_leaf_count = uint32_t(h.tlas_leaves.size());
+    s->blas_count = uint32_t(h.blases.size());
+    s->material_count = v.material_count;
+    s->bounds = h.bounds;
+    s->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = s.release();
+    return WF_OK;
+}
+
+wf_status wf_scene_set_environment(wf_scene* s, const wf_environment* env) {
+    if (!s) return fail(WF_ERR_INVALID_ARG, "null scene");
+    if (!env) {
+        WF_CUDA(cudaDeviceSynchronize());
+        free_list(s->env_allocations);
+        s->device_bytes -= s->env_bytes;
+        s->env_bytes = 0;
+        s->view.env = Environment{};
+        return WF_OK;
+    }
+    HostEnvironment map;
+    if (wf_status e = build_environment(env, map)) return e;
+    WF_CUDA(cudaDeviceSynchronize());
+    free_list(s->env_allocations);
+    s->device_bytes -= s->env_bytes;
+    s->env_bytes = 0;
+    Environment& ev = s->view.env;
+    ev = Environment{};
+    cudaError_t e = cudaSuccess;
+    auto up = [&](auto** dst, const auto& vec) {
+        if (e == cudaSuccess) e = upload(s, s->env_allocations, s->env_bytes, dst, vec);
+    };
+    up(&ev.pixels, map.pixels);
+    up(&ev.probabilities, map.probabilities);
+    up(&ev.alias, map.alias);
+    up(&ev.row_solid_angle, map.row_solid_angle);
+    if (e != cudaSuccess) {
+        free_list(s->env_allocations);
+        ev = Environment{};
+        return cuda_fail(e, "environment upload");
+    }
+    s->device_bytes += s->env_bytes;
+    ev.width = map.width;
+    ev.height = map.height;
+    ev.intensity = map.intensity;
+    ev.rotation = map.rotation;
+    ev.cos_rot = wfm::cosf(map.rotation);
+    ev.sin_rot = wfm::sinf(map.rotation);
+    ev.cos_neg = wfm::cosf(-map.rotation);
+    ev.sin_neg = wfm::sinf(-map.rotation);
+    ev.present = 1;
+    ev.sampling = map.intensity > 0.0f ? 1u : 0u;
+    return WF_OK;
+}
+
+wf_status wf_scene_destroy(wf_scene* s) {
+    if (!s) return WF_OK;
+    cudaDeviceSynchronize();
+    free_list(s->allocations);
+    free_list(s->env_allocations);
+    delete s;
+    return WF_OK;
+}
+
+wf_status wf_scene_get_info(const wf_scene* s, wf_scene_info* info) {
+    if (!s || !info) return fail(WF_ERR_INVALID_ARG, "null argument");
+    info->light_count = s->light_count;
+    info->tlas_leaf_count = s->tlas_leaf_count;
+    info->blas_count = s->blas_count;
+    info->material_count = s->material_count;
+    info->device_bytes = s->device_bytes;
+    info->build_seconds = s->build_seconds;
+    return WF_OK;
+}
+
+wf_status wf_trace_closest(const wf_scene* s, const wf_ray* rays, uint32_t count, wf_hit* hits, void* stream) {
+    if (!s || (count && (!rays || !hits))) return fail(WF_ERR_INVALID_ARG, "null argument");
+    return trace_closest_batch(s, rays, count, hits, static_cast<cudaStream_t>(stream));
+}
+
+wf_status wf_trace_any(const wf_scene* s, const wf_ray* rays, const float* max_distance, uint32_t count,
+                       uint8_t* occluded, void* stream) {
+    if (!s || (count && (!rays || !max_distance || !occluded))) return fail(WF_ERR_INVALID_ARG, "null argument");
+    return trace_any_batch(s, rays, max_distance, count, occluded, static_cast<cudaStream_t>(stream));
+}
+
+wf_status wf_renderer_create(const wf_scene* scene, const wf_camera* camera, const wf_render_config* config,
+                             void* stream, wf_renderer** out) {
+    return renderer_create(scene, camera, config, stream, out);
+}
+
+wf_status wf_renderer_destroy(wf_renderer* r) { return renderer_destroy(r); }
+
+wf_status wf_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_start,
+                    uint32_t sample_count, uint32_t clear_tile) {
+    if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
+    return renderer_render(r, x, y, w, h, sample_start, sample_count, clear_tile);
+}
+
+wf_status wf_render_frame(wf_renderer* r, uint32_t sample_count) {
+    if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
+    return renderer_render_frame(r, sample_count);
+}
+
+wf_status wf_framebuffer_reset(wf_renderer* r) {
+    if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
+    size_t pixels = size_t(r->config.width) * r->config.height;
+    WF_CUDA(cudaMemsetAsync(r->framebuffer, 0, sizeof(float) * 3 * pixels, r->stream));
+    WF_CUDA(cudaMemsetAsync(&r->counters->sample_index, 0, sizeof(uint32_t), r->stream));
+    return WF_OK;
+}
+
+wf_status wf_set_sample_index(wf_renderer* r, uint32_t sample_index) {
+    if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
+    WF_CUDA(cudaMemcpyAsync(&r->counters->sample_index, &sample_index, sizeof(uint32_t), cudaMemcpyHostToDevice,
+                            r->stream));
+    WF_CUDA(cudaStreamSynchronize(r->stream));
+    return WF_OK;
+}
+
+wf_status wf_get_sample_index(wf_renderer* r, uint32_t* sample_index) {
+    if (!r || !sample_index) return fail(WF_ERR_INVALID_ARG, "null argument");
+    WF_CUDA(cudaMemcpyAsync(sample_index, &r->counters->sample_index, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            r->stream));
+    WF_CUDA(cudaStreamSynchronize(r->stream));
+    return WF_OK;
+}
+
+wf_status wf_synchronize(wf_renderer* r) {
+    if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
+    WF_CUDA(cudaStreamSynchronize(r->stream));
+    uint32_t flags[2] = {0, 0};
+    WF_CUDA(cudaMemcpy(flags, &r->counters->overflow, sizeof(flags) / 2, cudaMemcpyDeviceToHost));
+    WF_CUDA(cudaMemcpy(&flags[1], &r->counters->error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (flags[1]) return fail(WF_ERR_TIMEOUT, "persistent kernel grid barrier timed out");
+    if (flags[0]) return fail(WF_ERR_CAPACITY, "shadow queue or term buffer overflow (flags %u)", flags[0]);
+    return WF_OK;
+}
+
+wf_status wf_framebuffer_download(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, uint32_t h, float* rgb) {
+    if (!r || !rgb) return fail(WF_ERR_INVALID_ARG, "null argument");
+    const wf_render_config& c = r->config;
+    if (w == 0 || h == 0 || x >= c.width || y >= c.height || w > c.width - x || h > c.height - y)
+        return fail(WF_ERR_INVALID_ARG, "download region outside the framebuffer");
+    WF_CUDA(cudaMemcpy2DAsync(rgb, size_t(w) * 12, r->framebuffer + (size_t(y) * c.width + x) * 3,
+                              size_t(c.width) * 12, size_t(w) * 12, h, cudaMemcpyDeviceToHost, r->stream));
+    return wf_synchronize(r);
+}
+
+wf_status wf_framebuffer_device(wf_renderer* r, float** rgb) {
+    if (!r || !rgb) return fail(WF_ERR_INVALID_ARG, "null argument");
+    *rgb = r->framebuffer;
+    return WF_OK;
+}
+
+wf_status wf_queue_counts(wf_renderer* r, uint32_t* counts, uint32_t n) {
+    if (!r || !counts) return fail(WF_ERR_INVALID_ARG, "null argument");
+    uint32_t m = std::min(n, r->config.max_depth);
+    WF_CUDA(cudaMemcpyAsync(counts, r->counters->profile, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost, r->stream));
+    WF_CUDA(cudaStreamSynchronize(r->stream));
+    return WF_OK;
+}
+
+wf_status wf_render_stats_get(wf_renderer* r, wf_render_stats* stats, uint32_t reset) {
+    if (!r || !stats) return fail(WF_ERR_INVALID_ARG, "null argument");
+    unsigned long long v[3];
+    WF_CUDA(cudaMemcpyAsync(v, &r->counters->extension_rays, sizeof(v), cudaMemcpyDeviceToHost, r->stream));
+    WF_CUDA(cudaStreamSynchronize(r->stream));
+    stats->extension_rays = v[0];
+    stats->shadow_rays = v[1];
+    stats->paths = v[2];
+    if (reset) {
+        WF_CUDA(cudaMemsetAsync(&r->counters->extension_rays, 0, sizeof(v), r->stream));
+        WF_CUDA(cudaStreamSynchronize(r->stream));
+    }
+    return WF_OK;
+}
+
+wf_status wf_photon_stats(wf_renderer* r, uint32_t* stored, uint32_t* emitted) {
+    if (!r || !stored || !emitted) return fail(WF_ERR_INVALID_ARG, "null argument");
+    *stored = r->photons_stored;
+    *emitted = r->photons_emitted;
+    return WF_OK;
+}
+
+wf_status wf_photons_download(wf_renderer* r, float* records, uint32_t count) {
+    if (!r || !records) return fail(WF_ERR_INVALID_ARG, "null argument");
+    if (!r->photon_raw || count > r->photons_emitted) return fail(WF_ERR_STATE, "no photon map of that size");
+    std::vector<float4> raw(size_t(count) * 4);
+    WF_CUDA(cudaMemcpyAsync(raw.data(), r->photon_raw, sizeof(float4) * raw.size(), cudaMemcpyDeviceToHost, r->stream));
+    WF_CUDA(cudaStreamSynchronize(r->stream));
+    for (uint32_t i = 0; i < count; ++i) {
+        const float4* p = &raw[4 * size_t(i)];
+        float* o = records + 8 * size_t(i);
+        o[0] = p[0].x; o[1] = p[0].y; o[2] = p[0].z;
+        o[3] = p[1].x; o[4] = p[1].y; o[5] = p[1].z;
+        o[6] = p[2].x + p[2].y + p[2].z;
+        o[7] = p[0].w;
+    }
+    return WF_OK;
+}
+
+wf_status wf_checkpoint_save(wf_renderer* r, const char* path, uint64_t fingerprint) {
+    if (!r || !path) return fail(WF_ERR_INVALID_ARG, "null argument");
+    size_t pixels = size_t(r->config.width) * r->config.height;
+    std::vector<float> rgb(pixels * 3);
+    uint32_t sample = 0;
+    WF_CUDA(cudaMemcpyAsync(rgb.data(), r->framebuffer, sizeof(float) * rgb.size(), cudaMemcpyDeviceToHost, r->stream));
+    WF_CUDA(cudaMemcpyAsync(&sample, &r->counters->sample_index, sizeof(uint32_t), cudaMemcpyDeviceToHost, r->stream));
+    WF_CUDA(cudaStreamSynchronize(r->stream));
+    return write_checkpoint(path, rgb.data(), r->config.width, r->config.height, sample, fingerprint);
+}
+
+wf_status wf_checkpoint_enqueue(wf_renderer* r, const char* path, uint64_t fingerprint, uint32_t* queued) {
+    if (!r || !path || !queued) return fail(WF_ERR_INVALID_ARG, "null argument");
+    *queued = 0;
+    size_t pixels = size_t(r->config.width) * r->config.height;
+    if (r->slots.empty()) {
+        for (int i = 0; i < 3; ++i) {
+            auto slot = std::make_unique<AsyncCheckpointSlot>();
+            WF_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&slot->pixels), sizeof(float) * 3 * pixels + 16,
+                                  cudaHostAllocDefault));
+            WF_CUDA(cudaEventCreateWithFlags(&slot->copied, cudaEventDisableTiming));
+            r->slots.push_back(std::move(slot));
+        }
+    }
+    for (auto& sp : r->slots) {
+        AsyncCheckpointSlot& slot = *sp;
+        bool expected = false;
+        if (!slot.busy.compare_exchange_strong(expected, true)) continue;
+        if (slot.writer.joinable()) slot.writer.join();
+        // The sample index travels with the pixels (last float slot).
+        WF_CUDA(cudaMemcpyAsync(slot.pixels, r->framebuffer, sizeof(float) * 3 * pixels, cudaMemcpyDeviceToHost,
+                                r->stream));
+        WF_CUDA(cudaMemcpyAsync(slot.pixels + 3 * pixels, &r->counters->sample_index, sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, r->stream));
+        WF_CUDA(cudaEventRecord(slot.copied, r->stream));
+        std::string file = path;
+        uint32_t width = r->config.width, height = r->config.height;
+        wf_renderer* rr = r;
+        slot.writer = std::thread([rr, &slot, file, fingerprint, width, height, pixels] {
+            cudaEventSynchronize(slot.copied);
+            uint32_t sample;
+            std::memcpy(&sample, slot.pixels + 3 * pixels, 4);
+            {
+                std::lock_guard<std::mutex> lock(rr->write_mutex);
+                if (sample >= rr->latest_written) {
+                    write_checkpoint(file.c_str(), slot.pixels, width, height, sample, fingerprint);
+                    rr->latest_written = sample;
+                }
+            }
+            slot.busy.store(false);
+        });
+        *queued = 1;
+        return WF_OK;
+    }
+    return WF_OK;
+}
+
+wf_status wf_checkpoint_flush(wf_renderer* r) {
+    if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
+    for (auto& slot : r->slots)
+        if (slot->writer.joinable()) slot->writer.join();
+    return WF_OK;
+}
+
+wf_status wf_checkpoint_load(wf_renderer* r, const char* path, uint64_t fingerprint, uint32_t* sample_index) {
+    if (!r || !path || !sample_index) return fail(WF_ERR_INVALID_ARG, "null argument");
+    std::ifstream in(path, std::ios::binary);
+    if (!in) return fail(WF_ERR_IO, "Could not open checkpoint: %s", path);
+    CheckpointHeader header{};
+    in.read(reinterpret_cast<char*>(&header), sizeof(header));
+    if (!in) return fail(WF_ERR_FORMAT, "Checkpoint is truncated or unreadable: %s", path);
+    if (std::memcmp(header.magic, kMagic, 8) != 0 || header.version != kCheckpointVersion)
+        return fail(WF_ERR_FORMAT, "Unsupported checkpoint format: %s", path);
+    if (header.width != r->config.width || header.height != r->config.height)
+        return fail(WF_ERR_FORMAT, "Checkpoint resolution does not match the current render: %s", path);
+    if (header.fingerprint != fingerprint)
+        return fail(WF_ERR_FINGERPRINT, "Checkpoint scene/config fingerprint does not match the current render: %s", path);
+    size_t pixels = size_t(header.width) * header.height;
+    std::vector<float> rgb(pixels * 3);
+    in.read(reinterpret_cast<char*>(rgb.data()), std::streamsize(sizeof(float) * rgb.size()));
+    if (!in) return fail(WF_ERR_FORMAT, "Checkpoint is truncated or unreadable: %s", path);
+    WF_CUDA(cudaMemcpyAsync(r->framebuffer, rgb.data(), sizeof(float) * rgb.size(), cudaMemcpyHostToDevice, r->stream));
+    WF_CUDA(cudaMemcpyAsync(&r->counters->sample_index, &header.sample_index, sizeof(uint32_t), cudaMemcpyHostToDevice,
+                            r->stream));
+    WF_CUDA(cudaStreamSynchronize(r->stream));
+    *sample_index = header.sample_index;
+    return WF_OK;
+}
+
+uint64_t wf_fnv1a64(const void* data, size_t size, uint64_t seed) {
+    uint64_t h = seed ? seed : 1469598103934665603ull;
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < size; ++i) {
+        h ^= p[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+}  // extern "C"

@@ -1,0 +1,887 @@
+// Wavefront kernels and the render loop.
+//
+// Graph mode (replaces RenderDriver::createWavefrontGraph,
+// src/renderer/render_driver.cu:264-297): per tile-sample the stream replays
+//   raygen, maxDepth x { trace, shade, shadow, finalize }, advance
+// captured once as a CUDA graph.  trace = closest hit of every queued path
+// (lean traversal kernel); shade = material/NEE evaluation that queues shadow
+// rays instead of tracing them inline; shadow = any-hit over the compacted
+// shadow queue; finalize = ordered radiance accumulation, framebuffer writes
+// of finished paths and warp-ballot compaction of survivors (the reference's
+// appendWarpCompacted, include/renderer/queue_compaction.cuh:8-29).
+//
+// Persistent mode (replaces persistentWavefrontTrace, renderer.cu:55-125): one
+// cooperative launch per tile-sample; warps pull 32-path chunks from a
+// per-bounce work counter, trace + shade + shadow inline, compact, and meet at
+// a bounded grid barrier between bounces.
+#include "wf_renderer.h"
+#include "wf_shade.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace wf {
+
+wf_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(WF_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define WF_CUDA(call)                                          \
+    do {                                                       \
+        cudaError_t wf_e_ = (call);                            \
+        if (wf_e_ != cudaSuccess) return cuda_fail(wf_e_, #call); \
+    } while (0)
+
+namespace {
+
+WF_DEV Path load_path(const PathSoA& ps, uint32_t p) {
+    float4 o = ps.origin[p], d = ps.direction[p], t = ps.throughput[p];
+    uint4 info = ps.info[p];
+    Path path;
+    path.origin = f4xyz(o);
+    path.prev_pdf = o.w;
+    path.direction = f4xyz(d);
+    path.eta_scale = d.w;
+    path.throughput = f4xyz(t);
+    path.medium_density = t.w;
+    path.pixel = info.x;
+    path.depth = info.y;
+    path.medium = info.z;
+    path.specular = (info.w & 1u) != 0;
+    path.active = (info.w & 2u) != 0;
+    path.rng = ps.rng[p];
+    return path;
+}
+
+WF_DEV void store_path(const PathSoA& ps, uint32_t p, const Path& path) {
+    ps.origin[p] = make_float4(path.origin.x, path.origin.y, path.origin.z, path.prev_pdf);
+    ps.direction[p] = make_float4(path.direction.x, path.direction.y, path.direction.z, path.eta_scale);
+    ps.throughput[p] = make_float4(path.throughput.x, path.throughput.y, path.throughput.z, path.medium_density);
+    ps.info[p] = make_uint4(path.pixel, path.depth, path.medium, (path.specular ? 1u : 0u) | (path.active ? 2u : 0u));
+    ps.rng[p] = path.rng;
+}
+
+// generatePrimaryRays, src/renderer/renderer.cu:10-42.
+WF_DEV void init_path(const RenderParams& rp, const TileDev& tile, uint32_t sample, uint32_t lp, Path& path) {
+    uint32_t x = tile.x + lp % tile.width;
+    uint32_t y = tile.y + lp / tile.width;
+    uint32_t pixel = y * rp.width + x;
+    uint64_t rng = make_rng_state(pixel_rng_key(pixel, sample, rp.rng), rp.rng);
+    float u = (float(x) + random_float(rng, rp.rng)) / float(rp.width);
+    float v = (float(y) + random_float(rng, rp.rng)) / float(rp.height);
+    camera_ray(rp.camera, u, v, path.origin, path.direction);
+    path.throughput = V3{1.0f, 1.0f, 1.0f};
+    path.pixel = pixel;
+    path.depth = 0;
+    path.rng = rng;
+    path.medium = kInvalid;
+    path.medium_density = 1.0f;
+    path.prev_pdf = 0.0f;
+    path.specular = true;
+    path.active = true;
+    path.eta_scale = 1.0f;
+}
+
+__global__ void k_raygen(RenderParams rp, const TileDev* tile_ptr, Counters* c, PathSoA ps, uint32_t* queue,
+                         uint32_t capacity) {
+    TileDev tile = *tile_ptr;
+    uint32_t n = min(tile.width * tile.height, capacity);
+    uint32_t sample = c->sample_index;
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) {
+        c->queue_count[0] = n;
+        c->paths += n;
+    }
+    for (uint32_t lp = gid; lp < n; lp += gridDim.x * blockDim.x) {
+        Path path;
+        init_path(rp, tile, sample, lp, path);
+        store_path(ps, lp, path);
+        ps.radiance[lp] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        queue[lp] = lp;
+    }
+}
+
+__global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
+                        uint32_t* hit_inst, Counters* c, uint32_t bounce) {
+    uint32_t n = *count;
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) {
+        c->shadow_count = 0;
+        if (bounce < kMaxBounces) c->profile[bounce] = n;
+        c->extension_rays += n;
+    }
+    for (uint32_t i = gid; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t p = queue[i];
+        float4 o = ps.origin[p], d = ps.direction[p];
+        TraceState h;
+        trace_closest(s, f4xyz(o), f4xyz(d), h);
+        hit_a[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
+        hit_inst[i] = h.inst;
+    }
+}
+
+__global__ void k_shade(DeviceScene s, RenderParams rp, PathSoA ps, const uint32_t* queue, const uint32_t* count,
+                        const float4* hit_a, const uint32_t* hit_inst, float4* terms, int4* shade_out,
+                        float4* shadow_origin, float4* shadow_dir, uint32_t shadow_capacity, Counters* c,
+                        uint32_t* next_count) {
+    uint32_t n = *count;
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) *next_count = 0;
+    for (uint32_t i = gid; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t p = queue[i];
+        Path path = load_path(ps, p);
+        float4 ha = hit_a[i];
+        SurfaceHit sh;
+        bool did_hit = finish_hit(s, path.origin, path.direction, ha.x, ha.y, ha.z, __float_as_uint(ha.w),
+                                  hit_inst[i], sh);
+        DeferredSink sink;
+        sink.shadow_origin = shadow_origin;
+        sink.shadow_dir = shadow_dir;
+        sink.shadow_count = &c->shadow_count;
+        sink.shadow_capacity = shadow_capacity;
+        sink.terms = terms + size_t(i) * kMaxTerms;
+        sink.owner = i;
+        sink.nterms = 0;
+        sink.kill = kUnconditional;
+        sink.overflow = &c->overflow;
+        bool alive = shade_path(s, rp, path, did_hit, sh, sink);
+        if (sink.nterms > kMaxTerms) atomicOr(&c->overflow, 2u);
+        store_path(ps, p, path);
+        shade_out[i] = make_int4(min(sink.nterms, kMaxTerms), sink.kill, alive ? 1 : 0, 0);
+    }
+}
+
+__global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float4* shadow_dir, uint8_t* result,
+                         Counters* c, uint32_t capacity) {
+    uint32_t n = min(c->shadow_count, capacity);
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) c->shadow_rays += n;
+    for (uint32_t j = gid; j < n; j += gridDim.x * blockDim.x) {
+        float4 o = shadow_origin[j], d = shadow_dir[j];
+        result[j] = trace_any(s, f4xyz(o), f4xyz(d), o.w) ? 1 : 0;
+    }
+}
+
+__global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* count, const float4* terms,
+                           const int4* shade_out, const uint8_t* shadow_result, uint32_t* next, uint32_t* next_count,
+                           uint32_t capacity, float* framebuffer) {
+    uint32_t n = *count;
+    uint32_t lane = threadIdx.x & 31;
+    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = warp * 32; base < n; base += warps * 32) {
+        uint32_t i = base + lane;
+        bool alive = false;
+        uint32_t p = 0;
+        if (i < n) {
+            p = queue[i];
+            int4 so = shade_out[i];
+            float4 r = ps.radiance[p];
+            V3 rad = f4xyz(r);
+            for (int k = 0; k < so.x; ++k) {
+                float4 t = terms[size_t(i) * kMaxTerms + k];
+                int h = __float_as_int(t.w);
+                if (h < 0 || !shadow_result[h]) rad += f4xyz(t);
+            }
+            alive = so.z != 0 && !(so.y >= 0 && !shadow_result[so.y]);
+            if (alive) {
+                ps.radiance[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+            } else {
+                uint32_t pixel = ps.info[p].x;
+                float* f = framebuffer + 3 * size_t(pixel);
+                f[0] += rad.x;
+                f[1] += rad.y;
+                f[2] += rad.z;
+            }
+        }
+        unsigned mask = __ballot_sync(0xffffffffu, alive);
+        uint32_t out = 0;
+        if (lane == 0 && mask) out = atomicAdd(next_count, uint32_t(__popc(mask)));
+        out = __shfl_sync(0xffffffffu, out, 0);
+        uint32_t rank = __popc(mask & ((1u << lane) - 1u));
+        if (alive && out + rank < capacity) next[out + rank] = p;
+    }
+}
+
+__global__ void k_advance(Counters* c, const TileDev* tile) {
+    if (tile->advance_sample) ++c->sample_index;
+}
+
+// Grid barrier with a bounded wait.  All blocks are co-resident (cooperative
+// launch).  A wait that exceeds ~2^31 cycles records an error and gives up;
+// callers then return and the host reports WF_ERR_TIMEOUT.
+WF_DEV bool grid_barrier(Counters* c, uint32_t blocks) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile uint32_t* gen = &c->barrier_generation;
+        uint32_t g = *gen;
+        __threadfence();
+        uint32_t arrived = atomicAdd(&c->barrier_count, 1u);
+        if (arrived == blocks - 1) {
+            c->barrier_count = 0;
+            __threadfence();
+            atomicAdd(&c->barrier_generation, 1u);
+        } else {
+            long long start = clock64();
+            while (*gen == g) {
+                if (*(volatile uint32_t*)&c->error) break;
+                if (clock64() - start > (1ll << 31)) {
+                    atomicExch(&c->error, 1u);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile uint32_t*)&c->error == 0;
+}
+
+__global__ void __launch_bounds__(128) k_persistent(DeviceScene s, RenderParams rp, const TileDev* tile_ptr,
+                                                    Counters* c, PathSoA ps, uint32_t* q0, uint32_t* q1,
+                                                    uint32_t capacity, float* framebuffer, uint32_t chunk_warps) {
+    TileDev tile = *tile_ptr;
+    uint32_t n0 = min(tile.width * tile.height, capacity);
+    uint32_t sample = c->sample_index;
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t lane = threadIdx.x & 31;
+    for (uint32_t lp = gid; lp < n0; lp += gridDim.x * blockDim.x) {
+        Path path;
+        init_path(rp, tile, sample, lp, path);
+        store_path(ps, lp, path);
+        ps.radiance[lp] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        q0[lp] = lp;
+    }
+    if (gid == 0) {
+        c->persistent_count[0] = n0;
+        c->paths += n0;
+    }
+    if (!grid_barrier(c, gridDim.x)) return;
+    unsigned long long shadow_rays = 0;
+    for (uint32_t bounce = 0; bounce < rp.max_depth && bounce < kMaxBounces; ++bounce) {
+        uint32_t n = *(volatile uint32_t*)&c->persistent_count[bounce];
+        if (gid == 0) {
+            c->profile[bounce] = n;
+            c->extension_rays += n;
+        }
+        if (n == 0) {
+            if (gid == 0)
+                for (uint32_t b = bounce + 1; b < rp.max_depth && b < kMaxBounces; ++b) c->profile[b] = 0;
+            break;
+        }
+        uint32_t* cur = (bounce & 1) ? q1 : q0;
+        uint32_t* next = (bounce & 1) ? q0 : q1;
+        uint32_t* next_count = &c->persistent_count[bounce + 1];
+        for (;;) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&c->persistent_work[bounce], 32u * chunk_warps);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= n) break;
+            for (uint32_t sub = 0; sub < chunk_warps && base + sub * 32 < n; ++sub) {
+                uint32_t i = base + sub * 32 + lane;
+                bool alive = false;
+                uint32_t p = 0;
+                if (i < n) {
+                    p = cur[i];
+                    Path path = load_path(ps, p);
+                    TraceState h;
+                    trace_closest(s, path.origin, path.direction, h);
+                    SurfaceHit sh;
+                    bool did_hit = finish_hit(s, path.origin, path.direction, h.t, h.u, h.v, h.prim, h.inst, sh);
+                    InlineSink sink;
+                    sink.scene = &s;
+                    sink.radiance = f4xyz(ps.radiance[p]);
+                    sink.killed = false;
+                    sink.requests = 0;
+                    alive = shade_path(s, rp, path, did_hit, sh, sink);
+                    alive = alive && !sink.killed;
+                    shadow_rays += sink.requests;
+                    store_path(ps, p, path);
+                    if (alive) {
+                        ps.radiance[p] = make_float4(sink.radiance.x, sink.radiance.y, sink.radiance.z, 0.0f);
+                    } else {
+                        float* f = framebuffer + 3 * size_t(path.pixel);
+                        f[0] += sink.radiance.x;
+                        f[1] += sink.radiance.y;
+                        f[2] += sink.radiance.z;
+                    }
+                }
+                unsigned mask = __ballot_sync(0xffffffffu, alive);
+                uint32_t out = 0;
+                if (lane == 0 && mask) out = atomicAdd(next_count, uint32_t(__popc(mask)));
+                out = __shfl_sync(0xffffffffu, out, 0);
+                uint32_t rank = __popc(mask & ((1u << lane) - 1u));
+                if (alive && out + rank < capacity) next[out + rank] = p;
+            }
+        }
+        if (!grid_barrier(c, gridDim.x)) return;
+    }
+    for (int off = 16; off > 0; off >>= 1) shadow_rays += __shfl_down_sync(0xffffffffu, shadow_rays, off);
+    if (lane == 0 && shadow_rays) atomicAdd(&c->shadow_rays, shadow_rays);
+}
+
+// ---------------------------------------------------------------- batch API
+__global__ void k_trace_batch(DeviceScene s, const wf_ray* rays, uint32_t count, wf_hit* hits) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    V3 o{rays[i].origin[0], rays[i].origin[1], rays[i].origin[2]};
+    V3 d{rays[i].direction[0], rays[i].direction[1], rays[i].direction[2]};
+    TraceState h;
+    trace_closest(s, o, d, h);
+    SurfaceHit sh;
+    wf_hit out;
+    memset(&out, 0, sizeof(out));
+    out.instance = kInvalid;
+    out.primitive = kInvalid;
+    if (!finish_hit(s, o, d, h.t, h.u, h.v, h.prim, h.inst, sh)) {
+        out.t = 1e30f;
+        out.material = kInvalid;
+        out.light_index = kInvalid;
+        out.kind = WF_HIT_NONE;
+        hits[i] = out;
+        return;
+    }
+    out.t = sh.t;
+    out.position[0] = sh.position.x; out.position[1] = sh.position.y; out.position[2] = sh.position.z;
+    out.geometric_normal[0] = sh.geometric_normal.x;
+    out.geometric_normal[1] = sh.geometric_normal.y;
+    out.geometric_normal[2] = sh.geometric_normal.z;
+    out.normal[0] = sh.normal.x; out.normal[1] = sh.normal.y; out.normal[2] = sh.normal.z;
+    out.material = sh.material;
+    out.light_index = sh.light;
+    uint32_t kind = hit_kind(h.prim), index = hit_index(h.prim);
+    if (kind == kHitSphere) {
+        out.kind = WF_HIT_SPHERE;
+        out.primitive = index;
+    } else {
+        uint32_t original = __float_as_uint(s.triangles[3 * size_t(index)].w) & kTriIndexMask;
+        out.primitive = original;
+        out.u = h.u;
+        out.v = h.v;
+        if (kind == kHitMesh) {
+            out.kind = WF_HIT_MESH;
+            out.instance = h.inst;
+        } else {
+            out.kind = index >= s.direct_first && index < s.direct_first + s.direct_count ? WF_HIT_TRIANGLE
+                                                                                         : WF_HIT_STATIC_TRIANGLE;
+        }
+    }
+    hits[i] = out;
+}
+
+__global__ void k_any_batch(DeviceScene s, const wf_ray* rays, const float* max_distance, uint32_t count,
+                            uint8_t* occluded) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    V3 o{rays[i].origin[0], rays[i].origin[1], rays[i].origin[2]};
+    V3 d{rays[i].direction[0], rays[i].direction[1], rays[i].direction[2]};
+    occluded[i] = trace_any(s, o, d, max_distance[i]) ? 1 : 0;
+}
+
+// ------------------------------------------------------------------ photons
+// emitPhotons / tracePhotons, src/renderer/photon_mapping.cu:4-74.  Each
+// photon is 4 float4: position (.w = valid), direction (.w = spectral channel),
+// flux, rng state (.xy) and specular bounce count (.z).
+__global__ void k_emit_photons(DeviceScene s, uint32_t count, uint32_t seed, uint32_t strategy, uint32_t spectral,
+                               float4* photons) {
+    uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= count || s.light_count == 0) return;
+    uint64_t rng = make_rng_state(photon_rng_key(index, seed, strategy), strategy);
+    uint32_t candidate = min(uint32_t(random_float(rng, strategy) * s.light_count), s.light_count - 1);
+    const Light* cl = &s.lights[candidate];
+    uint32_t li = random_float(rng, strategy) < cl->alias_probability ? candidate : cl->alias;
+    const Light& light = s.lights[li];
+    float root_u = sqrtf(random_float(rng, strategy));
+    float v = random_float(rng, strategy);
+    V3 point = (1.0f - root_u) * light.v0 + root_u * ((1.0f - v) * light.v1 + v * light.v2);
+    Path tmp;
+    tmp.rng = rng;
+    V3 direction = sample_cosine_hemisphere(light.normal, tmp, strategy);
+    rng = tmp.rng;
+    const Material& m = s.materials[light.material];
+    uint32_t channel = 3;
+    V3 flux = m.emission * (light.area * 3.14159265359f / float(count));
+    if (spectral) {
+        channel = min(uint32_t(random_float(rng, strategy) * 3.0f), 2u);
+        flux = V3{0.0f, 0.0f, 0.0f};
+        float cf = (channel == 0 ? m.emission.x : channel == 1 ? m.emission.y : m.emission.z) *
+                   (light.area * 3.14159265359f * 3.0f / float(count));
+        if (channel == 0) flux.x = cf;
+        else if (channel == 1) flux.y = cf;
+        else flux.z = cf;
+    }
+    V3 position = point + light.normal * 0.001f;
+    float4* ph = photons + 4 * size_t(index);
+    ph[0] = make_float4(position.x, position.y, position.z, 0.0f);
+    ph[1] = make_float4(direction.x, direction.y, direction.z, __uint_as_float(channel));
+    ph[2] = make_float4(flux.x, flux.y, flux.z, 0.0f);
+    ph[3] = make_float4(__uint_as_float(uint32_t(rng)), __uint_as_float(uint32_t(rng >> 32)), __uint_as_float(0u), 0.0f);
+}
+
+__global__ void k_trace_photons(DeviceScene s, uint32_t count, uint32_t max_depth, uint32_t strategy,
+                                float4* photons, uint32_t* stored) {
+    uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= count || s.light_count == 0) return;
+    float4* ph = photons + 4 * size_t(index);
+    float4 p0 = ph[0], p1 = ph[1], p2 = ph[2], p3 = ph[3];
+    uint32_t channel = __float_as_uint(p1.w);
+    V3 flux = f4xyz(p2);
+    Path rngp;
+    rngp.rng = uint64_t(__float_as_uint(p3.x)) | (uint64_t(__float_as_uint(p3.y)) << 32);
+    uint32_t specular_bounces = 0;
+    V3 o = f4xyz(p0), d = f4xyz(p1);
+    for (uint32_t depth = 0; depth < max_depth; ++depth) {
+        TraceState h;
+        trace_closest(s, o, d, h);
+        SurfaceHit hit;
+        if (!finish_hit(s, o, d, h.t, h.u, h.v, h.prim, h.inst, hit)) return;
+        if (hit.material >= s.material_count) return;
+        const Material& m = s.materials[hit.material];
+        V3 normal = dot(hit.normal, -d) >= 0.0f ? hit.normal : -hit.normal;
+        if (m.type == kDiffuse) {
+            if (specular_bounces == 0) return;
+            V3 back = -d;
+            ph[0] = make_float4(hit.position.x, hit.position.y, hit.position.z, 1.0f);
+            ph[1] = make_float4(back.x, back.y, back.z, __uint_as_float(channel));
+            ph[2] = make_float4(flux.x, flux.y, flux.z, 0.0f);
+            ph[3] = make_float4(__uint_as_float(uint32_t(rngp.rng)), __uint_as_float(uint32_t(rngp.rng >> 32)),
+                                __uint_as_float(specular_bounces), 0.0f);
+            atomicAdd(stored, 1u);
+            return;
+        }
+        V3 direction;
+        if (m.type == kMetal) {
+            direction = normalize(reflect(normalize(d), normal));
+        } else if (m.type == kDielectric) {
+            float ior = m.ior;
+            if (m.dispersion > 0.0f && channel < 3) ior += (float(channel) - 1.0f) * m.dispersion;
+            DielectricInterface b = dielectric_interface(normalize(d), hit.geometric_normal, hit.normal, ior);
+            bool reflected = b.reflectance >= 1.0f || b.reflectance > random_float(rngp.rng, strategy);
+            direction = reflected ? b.reflection : b.transmission;
+        } else {
+            direction = sample_cosine_hemisphere(normal, rngp, strategy);
+        }
+        if (m.type == kMetal || m.type == kDielectric) ++specular_bounces;
+        flux = hadamard(flux, m.albedo);
+        o = offset_ray_origin(hit.position, hit.geometric_normal, direction, hit.t);
+        d = direction;
+    }
+}
+
+WF_DEV uint32_t float_order(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+WF_DEV float order_float(uint32_t u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u); }
+
+__global__ void k_photon_bounds(const float4* photons, uint32_t count, uint32_t* bounds) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    float4 p = photons[4 * size_t(i)];
+    if (p.w != 1.0f) return;
+    atomicMin(&bounds[0], float_order(p.x));
+    atomicMin(&bounds[1], float_order(p.y));
+    atomicMin(&bounds[2], float_order(p.z));
+    atomicMax(&bounds[3], float_order(p.x));
+    atomicMax(&bounds[4], float_order(p.y));
+    atomicMax(&bounds[5], float_order(p.z));
+}
+
+// buildPhotonGrid cell rule (photon_mapping.cu:76-89); key = cell, then
+// descending photon index (the order serial insertion leaves in each list).
+__global__ void k_photon_keys(const float4* photons, uint32_t count, uint32_t padded, PhotonGridView g,
+                              unsigned long long* keys) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= padded) return;
+    unsigned long long key = ~0ull;
+    if (i < count) {
+        float4 p = photons[4 * size_t(i)];
+        if (p.w == 1.0f) {
+            V3 extent = g.maximum - g.minimum;
+            V3 offset = V3{p.x, p.y, p.z} - g.minimum;
+            V3 nrm{offset.x / extent.x, offset.y / extent.y, offset.z / extent.z};
+            int res = int(g.resolution);
+            int x = min(max(int(nrm.x * g.resolution), 0), res - 1);
+            int y = min(max(int(nrm.y * g.resolution), 0), res - 1);
+            int z = min(max(int(nrm.z * g.resolution), 0), res - 1);
+            bool inside = !(nrm.x < 0.0f || nrm.y < 0.0f || nrm.z < 0.0f || nrm.x > 1.0f || nrm.y > 1.0f || nrm.z > 1.0f);
+            if (inside) {
+                uint32_t cell = (uint32_t(z) * g.resolution + uint32_t(y)) * g.resolution + uint32_t(x);
+                key = (uint64_t(cell) << 32) | uint64_t(0xffffffffu - i);
+            }
+        }
+    }
+    keys[i] = key;
+}
+
+__global__ void k_bitonic(unsigned long long* keys, uint32_t j, uint32_t k, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t l = i ^ j;
+    if (l > i) {
+        unsigned long long a = keys[i], b = keys[l];
+        bool ascending = (i & k) == 0;
+        if ((a > b) == ascending) {
+            keys[i] = b;
+            keys[l] = a;
+        }
+    }
+}
+
+__global__ void k_photon_scatter(const unsigned long long* keys, uint32_t padded, const float4* photons,
+                                 float4* pos, float4* dir, float4* flux, uint32_t* cell_start, uint32_t* cell_end) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= padded) return;
+    unsigned long long key = keys[j];
+    if (key == ~0ull) return;
+    uint32_t index = 0xffffffffu - uint32_t(key);
+    uint32_t cell = uint32_t(key >> 32);
+    const float4* ph = photons + 4 * size_t(index);
+    pos[j] = ph[0];
+    dir[j] = ph[1];
+    flux[j] = ph[2];
+    if (j == 0 || uint32_t(keys[j - 1] >> 32) != cell) cell_start[cell] = j;
+    if (j + 1 == padded || keys[j + 1] == ~0ull || uint32_t(keys[j + 1] >> 32) != cell) cell_end[cell] = j + 1;
+}
+
+__global__ void k_cell_counts(const uint32_t* start, uint32_t* end_to_count, uint32_t cells) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < cells) end_to_count[c] = end_to_count[c] - start[c];
+}
+
+template <typename T>
+cudaError_t alloc(wf_renderer* r, T** p, size_t count) {
+    size_t bytes = sizeof(T) * std::max<size_t>(count, 1);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+    if (e == cudaSuccess) {
+        r->allocations.push_back(*p);
+        r->device_bytes += bytes;
+    }
+    return e;
+}
+
+uint32_t grid_for(const wf_renderer* r, uint32_t work, uint32_t block) {
+    uint32_t g = (work + block - 1) / block;
+    return std::max(1u, std::min(g, r->grid_cap));
+}
+
+wf_status build_photon_map(wf_renderer* r) {
+    const wf_render_config& c = r->config;
+    const DeviceScene& s = r->scene->view;
+    uint32_t n = c.photon_count;
+    r->photons_emitted = n;
+    if (s.light_count == 0 || n == 0) {
+        r->params.photons.enabled = 0;
+        return WF_OK;
+    }
+    WF_CUDA(alloc(r, &r->photon_raw, size_t(n) * 4));
+    uint32_t* stored = nullptr;
+    WF_CUDA(alloc(r, &stored, 8));
+    WF_CUDA(cudaMemsetAsync(r->photon_raw, 0, sizeof(float4) * 4 * size_t(n), r->stream));
+    WF_CUDA(cudaMemsetAsync(stored, 0, 8 * sizeof(uint32_t), r->stream));
+    uint32_t block = 128;
+    k_emit_photons<<<(n + block - 1) / block, block, 0, r->stream>>>(s, n, c.photon_seed, c.rng, c.spectral, r->photon_raw);
+    k_trace_photons<<<(n + block - 1) / block, block, 0, r->stream>>>(s, n, c.photon_max_depth, c.rng, r->photon_raw,
+                                                                     stored);
+    WF_CUDA(cudaGetLastError());
+    PhotonGridView& g = r->params.photons;
+    g.resolution = c.photon_grid_resolution ? c.photon_grid_resolution : 64;
+    bool derive = c.photon_grid_min[0] == c.photon_grid_max[0] && c.photon_grid_min[1] == c.photon_grid_max[1] &&
+                  c.photon_grid_min[2] == c.photon_grid_max[2];
+    if (derive) {
+        uint32_t init[8] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u, 0u, 0u};
+        uint32_t* bounds = stored + 2;
+        WF_CUDA(cudaMemcpyAsync(bounds, init, 6 * sizeof(uint32_t), cudaMemcpyHostToDevice, r->stream));
+        k_photon_bounds<<<(n + block - 1) / block, block, 0, r->stream>>>(r->photon_raw, n, bounds);
+    }
+    uint32_t host[8];
+    WF_CUDA(cudaMemcpyAsync(host, stored, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->stream));
+    WF_CUDA(cudaStreamSynchronize(r->stream));
+    r->photons_stored = host[0];
+    if (derive) {
+        auto dec = [](uint32_t u) {
+            uint32_t b = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+            float f;
+            std::memcpy(&f, &b, 4);
+            return f;
+        };
+        if (host[0] == 0) {
+            g.minimum = V3{-1, -1, -1};
+            g.maximum = V3{1, 1, 1};
+        } else {
+            g.minimum = V3{dec(host[2]), dec(host[3]), dec(host[4])};
+            g.maximum = V3{dec(host[5]), dec(host[6]), dec(host[7])};
+            // Degenerate axes get unit extent so the normalization stays finite.
+            if (!(g.maximum.x > g.minimum.x)) g.maximum.x = g.minimum.x + 1.0f;
+            if (!(g.maximum.y > g.minimum.y)) g.maximum.y = g.minimum.y + 1.0f;
+            if (!(g.maximum.z > g.minimum.z)) g.maximum.z = g.minimum.z + 1.0f;
+        }
+    } else {
+        g.minimum = V3{c.photon_grid_min[0], c.photon_grid_min[1], c.photon_grid_min[2]};
+        g.maximum = V3{c.photon_grid_max[0], c.photon_grid_max[1], c.photon_grid_max[2]};
+    }
+    uint32_t padded = 1;
+    while (padded < n) padded <<= 1;
+    unsigned long long* keys = nullptr;
+    uint32_t cells = g.resolution * g.resolution * g.resolution;
+    float4 *pos = nullptr, *dir = nullptr, *flux = nullptr;
+    uint32_t *start = nullptr, *end = nullptr;
+    WF_CUDA(alloc(r, &keys, padded));
+    WF_CUDA(alloc(r, &pos, padded));
+    WF_CUDA(alloc(r, &dir, padded));
+    WF_CUDA(alloc(r, &flux, padded));
+    WF_CUDA(alloc(r, &start, cells));
+    WF_CUDA(alloc(r, &end, cells));
+    WF_CUDA(cudaMemsetAsync(start, 0, sizeof(uint32_t) * cells, r->stream));
+    WF_CUDA(cudaMemsetAsync(end, 0, sizeof(uint32_t) * cells, r->stream));
+    uint32_t sb = 256;
+    k_photon_keys<<<(padded + sb - 1) / sb, sb, 0, r->stream>>>(r->photon_raw, n, padded, g, keys);
+    for (uint32_t k = 2; k <= padded; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1)
+            k_bitonic<<<(padded + sb - 1) / sb, sb, 0, r->stream>>>(keys, j, k, padded);
+    k_photon_scatter<<<(padded + sb - 1) / sb, sb, 0, r->stream>>>(keys, padded, r->photon_raw, pos, dir, flux, start,
+                                                                   end);
+    k_cell_counts<<<(cells + sb - 1) / sb, sb, 0, r->stream>>>(start, end, cells);
+    WF_CUDA(cudaGetLastError());
+    g.position = pos;
+    g.direction = dir;
+    g.flux = flux;
+    g.cell_start = start;
+    g.cell_count = end;
+    g.enabled = c.caustic_gather ? 1u : 0u;
+    return WF_OK;
+}
+
+wf_status capture_graph(wf_renderer* r) {
+    const DeviceScene& s = r->scene->view;
+    cudaStream_t st = r->stream;
+    WF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    uint32_t cap = r->capacity;
+    k_raygen<<<grid_for(r, cap, 256), 256, 0, st>>>(r->params, r->tile, r->counters, r->paths, r->queue[0], cap);
+    for (uint32_t b = 0; b < r->config.max_depth; ++b) {
+        uint32_t cur = b & 1, nxt = cur ^ 1;
+        uint32_t* cur_count = &r->counters->queue_count[cur];
+        uint32_t* next_count = &r->counters->queue_count[nxt];
+        k_trace<<<grid_for(r, cap, r->block_trace), r->block_trace, 0, st>>>(
+            s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b);
+        k_shade<<<grid_for(r, cap, r->block_shade), r->block_shade, 0, st>>>(
+            s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
+            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count);
+        k_shadow<<<grid_for(r, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
+            s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity);
+        k_finalize<<<grid_for(r, cap, r->block_finalize), r->block_finalize, 0, st>>>(
+            r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result, r->queue[nxt], next_count,
+            cap, r->framebuffer);
+    }
+    k_advance<<<1, 1, 0, st>>>(r->counters, r->tile);
+    cudaError_t e = cudaStreamEndCapture(st, &r->graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    WF_CUDA(cudaGraphInstantiate(&r->graph_exec, r->graph, 0));
+    return WF_OK;
+}
+
+wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
+    WF_CUDA(cudaMemcpyAsync(r->tile, &tile, sizeof(TileDev), cudaMemcpyHostToDevice, r->stream));
+    r->last_tile_width = tile.width;
+    r->last_tile_height = tile.height;
+    if (r->config.mode == WF_MODE_GRAPH) {
+        WF_CUDA(cudaGraphLaunch(r->graph_exec, r->stream));
+        return WF_OK;
+    }
+    WF_CUDA(cudaMemsetAsync(r->counters->persistent_count, 0, sizeof(uint32_t) * 2 * (kMaxBounces + 1), r->stream));
+    WF_CUDA(cudaMemsetAsync(&r->counters->barrier_count, 0, sizeof(uint32_t), r->stream));
+    DeviceScene s = r->scene->view;
+    RenderParams rp = r->params;
+    const TileDev* tp = r->tile;
+    Counters* c = r->counters;
+    PathSoA ps = r->paths;
+    uint32_t* q0 = r->queue[0];
+    uint32_t* q1 = r->queue[1];
+    uint32_t cap = r->capacity;
+    float* fb = r->framebuffer;
+    uint32_t chunk = r->chunk;
+    void* args[] = {&s, &rp, &tp, &c, &ps, &q0, &q1, &cap, &fb, &chunk};
+    WF_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_persistent), dim3(r->persistent_blocks),
+                                        dim3(r->persistent_block_size), args, 0, r->stream));
+    k_advance<<<1, 1, 0, r->stream>>>(r->counters, r->tile);
+    WF_CUDA(cudaGetLastError());
+    return WF_OK;
+}
+
+}  // namespace
+
+wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const wf_render_config* cfg, void* stream,
+                          wf_renderer** out) {
+    if (!scene || !camera || !cfg || !out) return fail(WF_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    const wf_render_config& c = *cfg;
+    if (!std::isfinite(c.indirect_clamp) || c.indirect_clamp < 0.0f)
+        return fail(WF_ERR_INVALID_ARG, "Indirect radiance clamp must be finite and nonnegative");
+    if (c.width == 0 || c.height == 0) return fail(WF_ERR_INVALID_ARG, "Render dimensions must be greater than zero");
+    if (c.max_depth == 0) return fail(WF_ERR_INVALID_ARG, "maximum depth must be greater than zero");
+    if (c.max_depth > kMaxBounces) return fail(WF_ERR_INVALID_ARG, "maximum depth above %d", kMaxBounces);
+    if (c.block_size > 1024) return fail(WF_ERR_INVALID_ARG, "CUDA block size must be between 1 and 1024");
+    if (c.mode > WF_MODE_PERSISTENT || c.rng > WF_RNG_PCG32 || c.debug > WF_DEBUG_SHADING_NORMAL)
+        return fail(WF_ERR_INVALID_ARG, "unknown mode, rng strategy or debug view");
+    if (c.caustics && c.photon_count == 0)
+        return fail(WF_ERR_INVALID_ARG, "Photon count must be greater than zero when caustics are enabled");
+    if (c.gather_radius <= 0.0f) return fail(WF_ERR_INVALID_ARG, "Caustic gather radius must be greater than zero");
+    if (scene->view.punctual_count - scene->view.directional_count > 0 && scene->view.directional_count > 2)
+        return fail(WF_ERR_UNSUPPORTED, "more than two directional lights");
+    uint64_t pixels = uint64_t(c.width) * c.height;
+    uint64_t capacity = (c.tile_width && c.tile_height) ? uint64_t(c.tile_width) * c.tile_height : pixels;
+    if (pixels > 0xffffffffull || capacity > 0xffffffffull)
+        return fail(WF_ERR_INVALID_ARG, "Render dimensions exceed the supported queue index range");
+
+    auto r = std::make_unique<wf_renderer>();
+    r->scene = scene;
+    r->config = c;
+    r->capacity = uint32_t(std::min(capacity, pixels));
+    WF_CUDA(cudaGetDevice(&r->device));
+    WF_CUDA(cudaDeviceGetAttribute(&r->sm_count, cudaDevAttrMultiProcessorCount, r->device));
+    r->grid_cap = uint32_t(r->sm_count) * 64;
+    if (c.block_size) r->block_trace = r->block_shade = c.block_size;
+    if (stream) {
+        r->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        WF_CUDA(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+        r->own_stream = true;
+    }
+    RenderParams& rp = r->params;
+    rp.width = c.width;
+    rp.height = c.height;
+    rp.max_depth = c.max_depth;
+    rp.rr_start = c.rr_start_depth;
+    rp.rng = c.rng;
+    rp.debug = c.debug;
+    rp.clamp = c.indirect_clamp;
+    rp.gather_radius = c.gather_radius;
+    rp.camera.position = V3{camera->position[0], camera->position[1], camera->position[2]};
+    rp.camera.forward = V3{camera->forward[0], camera->forward[1], camera->forward[2]};
+    rp.camera.right = V3{camera->right[0], camera->right[1], camera->right[2]};
+    rp.camera.up = V3{camera->up[0], camera->up[1], camera->up[2]};
+    rp.camera.aspect_ratio = camera->aspect_ratio;
+    rp.camera.tan_half_fov = wfm::tanf(camera->vertical_fov * 0.5f);
+    rp.photons = PhotonGridView{};
+
+    uint32_t cap = r->capacity;
+    wf_renderer* rr = r.get();
+    WF_CUDA(alloc(rr, &r->paths.origin, cap));
+    WF_CUDA(alloc(rr, &r->paths.direction, cap));
+    WF_CUDA(alloc(rr, &r->paths.throughput, cap));
+    WF_CUDA(alloc(rr, &r->paths.radiance, cap));
+    WF_CUDA(alloc(rr, &r->paths.info, cap));
+    WF_CUDA(alloc(rr, &r->paths.rng, cap));
+    WF_CUDA(alloc(rr, &r->queue[0], cap));
+    WF_CUDA(alloc(rr, &r->queue[1], cap));
+    WF_CUDA(alloc(rr, &r->counters, 1));
+    WF_CUDA(alloc(rr, &r->tile, 1));
+    WF_CUDA(alloc(rr, &r->framebuffer, size_t(pixels) * 3));
+    WF_CUDA(cudaMemsetAsync(r->counters, 0, sizeof(Counters), r->stream));
+    WF_CUDA(cudaMemsetAsync(r->framebuffer, 0, sizeof(float) * 3 * size_t(pixels), r->stream));
+    if (c.mode == WF_MODE_GRAPH) {
+        uint32_t requests_per_path = 5u + scene->view.directional_count;
+        uint64_t shadow = uint64_t(cap) * requests_per_path;
+        if (shadow > 0xffffffffull) shadow = 0xffffffffull;
+        r->shadow_capacity = uint32_t(shadow);
+        WF_CUDA(alloc(rr, &r->hit_a, cap));
+        WF_CUDA(alloc(rr, &r->hit_inst, cap));
+        WF_CUDA(alloc(rr, &r->terms, size_t(cap) * kMaxTerms));
+        WF_CUDA(alloc(rr, &r->shade_out, cap));
+        WF_CUDA(alloc(rr, &r->shadow_origin, r->shadow_capacity));
+        WF_CUDA(alloc(rr, &r->shadow_dir, r->shadow_capacity));
+        WF_CUDA(alloc(rr, &r->shadow_result, r->shadow_capacity));
+    } else {
+        int cooperative = 0;
+        WF_CUDA(cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, r->device));
+        if (!cooperative) return fail(WF_ERR_UNSUPPORTED, "device does not support cooperative launches");
+        r->persistent_block_size = 128;
+        int per_sm = 0;
+        WF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent, int(r->persistent_block_size), 0));
+        if (per_sm <= 0) return fail(WF_ERR_UNSUPPORTED, "the persistent kernel cannot be resident");
+        uint32_t resident = uint32_t(per_sm) * uint32_t(r->sm_count);
+        uint32_t wanted = c.persistent_blocks ? c.persistent_blocks : resident;
+        r->persistent_blocks = std::max(1u, std::min(wanted, resident));
+        r->chunk = c.chunk ? std::max(1u, c.chunk / 32) : 1u;
+    }
+    if (c.caustics) {
+        if (wf_status e = build_photon_map(rr)) return e;
+    }
+    if (c.mode == WF_MODE_GRAPH) {
+        if (wf_status e = capture_graph(rr)) return e;
+    }
+    WF_CUDA(cudaStreamSynchronize(r->stream));
+    *out = r.release();
+    return WF_OK;
+}
+
+wf_status renderer_destroy(wf_renderer* r) {
+    if (!r) return WF_OK;
+    cudaStreamSynchronize(r->stream);
+    for (auto& slot : r->slots) {
+        if (slot->writer.joinable()) slot->writer.join();
+        if (slot->pixels) cudaFreeHost(slot->pixels);
+        if (slot->copied) cudaEventDestroy(slot->copied);
+    }
+    if (r->graph_exec) cudaGraphExecDestroy(r->graph_exec);
+    if (r->graph) cudaGraphDestroy(r->graph);
+    for (void* p : r->allocations) cudaFree(p);
+    if (r->own_stream) cudaStreamDestroy(r->stream);
+    delete r;
+    return WF_OK;
+}
+
+wf_status renderer_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_start,
+                          uint32_t sample_count, uint32_t clear) {
+    const wf_render_config& c = r->config;
+    if (w == 0 || h == 0 || x >= c.width || y >= c.height || w > c.width - x || h > c.height - y ||
+        uint64_t(w) * h > r->capacity)
+        return fail(WF_ERR_INVALID_ARG, "Render task tile is outside the prepared renderer bounds");
+    if (sample_count == 0) return fail(WF_ERR_INVALID_ARG, "Render task sample range is empty");
+    if (clear) {
+        WF_CUDA(cudaMemset2DAsync(r->framebuffer + (size_t(y) * c.width + x) * 3, size_t(c.width) * 12, 0,
+                                  size_t(w) * 12, h, r->stream));
+    }
+    WF_CUDA(cudaMemcpyAsync(&r->counters->sample_index, &sample_start, sizeof(uint32_t), cudaMemcpyHostToDevice,
+                            r->stream));
+    TileDev tile{x, y, w, h, 1};
+    for (uint32_t s = 0; s < sample_count; ++s)
+        if (wf_status e = launch_tile(r, tile)) return e;
+    return WF_OK;
+}
+
+wf_status renderer_render_frame(wf_renderer* r, uint32_t sample_count) {
+    const wf_render_config& c = r->config;
+    uint32_t tw = c.tile_width && c.tile_height ? c.tile_width : c.width;
+    uint32_t th = c.tile_width && c.tile_height ? c.tile_height : c.height;
+    std::vector<TileDev> tiles;
+    for (uint32_t y = 0; y < c.height; y += th)
+        for (uint32_t x = 0; x < c.width; x += tw)
+            tiles.push_back(TileDev{x, y, std::min(tw, c.width - x), std::min(th, c.height - y), 0});
+    for (uint32_t s = 0; s < sample_count; ++s)
+        for (size_t t = 0; t < tiles.size(); ++t) {
+            TileDev tile = tiles[t];
+            tile.advance_sample = t + 1 == tiles.size() ? 1u : 0u;
+            if (wf_status e = launch_tile(r, tile)) return e;
+        }
+    return WF_OK;
+}
+
+wf_status trace_closest_batch(const wf_scene* scene, const wf_ray* rays, uint32_t count, wf_hit* hits,
+                              cudaStream_t stream) {
+    if (count == 0) return WF_OK;
+    k_trace_batch<<<(count + 127) / 128, 128, 0, stream>>>(scene->view, rays, count, hits);
+    WF_CUDA(cudaGetLastError());
+    return WF_OK;
+}
+
+wf_status trace_any_batch(const wf_scene* scene, const wf_ray* rays, const float* max_distance, uint32_t count,
+                          uint8_t* occluded, cudaStream_t stream) {
+    if (count == 0) return WF_OK;
+    k_any_batch<<<(count + 127) / 128, 128, 0, stream>>>(scene->view, rays, max_distance, count, occluded);
+    WF_CUDA(cudaGetLastError());
+    return WF_OK;
+}
+
+}  // namespace wf

@@ -1,0 +1,111 @@
+// Renderer object behind the C ABI (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "wf_internal.h"
+
+namespace wf {
+
+struct TileDev {
+    uint32_t x, y, width, height;
+    uint32_t advance_sample;
+};
+
+// Device counters of one renderer (one allocation, zeroed at creation).
+constexpr int kMaxBounces = 64;
+struct Counters {
+    uint32_t queue_count[2];
+    uint32_t shadow_count;
+    uint32_t overflow;
+    uint32_t sample_index;
+    uint32_t error;          // persistent-kernel barrier timeout
+    uint32_t barrier_count;
+    uint32_t barrier_generation;
+    unsigned long long extension_rays;
+    unsigned long long shadow_rays;
+    unsigned long long paths;
+    uint32_t profile[kMaxBounces];          // per-bounce queue sizes (latest sample)
+    uint32_t persistent_count[kMaxBounces + 1];
+    uint32_t persistent_work[kMaxBounces + 1];
+};
+
+struct PathSoA {
+    float4* origin;     // xyz, prev_pdf
+    float4* direction;  // xyz, eta_scale
+    float4* throughput; // xyz, medium_density
+    float4* radiance;   // xyz, -
+    uint4* info;        // pixel, depth, medium, flags (1 = specular, 2 = active)
+    unsigned long long* rng;
+};
+
+struct AsyncCheckpointSlot {
+    float* pixels = nullptr;
+    cudaEvent_t copied = nullptr;
+    std::atomic<bool> busy{false};
+    std::thread writer;
+};
+
+}  // namespace wf
+
+struct wf_renderer {
+    const wf_scene* scene = nullptr;
+    wf_render_config config{};
+    wf::RenderParams params{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    int sm_count = 148;
+    uint32_t capacity = 0;
+    uint32_t block_trace = 128, block_shade = 128, block_finalize = 256;
+    uint32_t grid_cap = 0;
+    std::vector<void*> allocations;
+    uint64_t device_bytes = 0;
+    wf::PathSoA paths{};
+    uint32_t* queue[2] = {nullptr, nullptr};
+    float4* hit_a = nullptr;
+    uint32_t* hit_inst = nullptr;
+    float4* terms = nullptr;
+    int4* shade_out = nullptr;
+    float4* shadow_origin = nullptr;
+    float4* shadow_dir = nullptr;
+    uint8_t* shadow_result = nullptr;
+    uint32_t shadow_capacity = 0;
+    wf::Counters* counters = nullptr;
+    wf::TileDev* tile = nullptr;
+    float* framebuffer = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    uint32_t persistent_blocks = 0;
+    uint32_t persistent_block_size = 128;
+    uint32_t chunk = 1;
+    // photon map
+    uint32_t photons_emitted = 0, photons_stored = 0;
+    float4* photon_raw = nullptr;  // 4 float4 per photon: pos(.w valid), dir, flux, rng/meta
+    // checkpoint writer
+    std::vector<std::unique_ptr<wf::AsyncCheckpointSlot>> slots;
+    std::mutex write_mutex;
+    uint32_t latest_written = 0;
+    uint32_t last_tile_width = 0, last_tile_height = 0;
+};
+
+namespace wf {
+wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const wf_render_config* config,
+                          void* stream, wf_renderer** out);
+wf_status renderer_destroy(wf_renderer* r);
+wf_status renderer_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_start,
+                          uint32_t sample_count, uint32_t clear);
+wf_status renderer_render_frame(wf_renderer* r, uint32_t sample_count);
+wf_status trace_closest_batch(const wf_scene* scene, const wf_ray* rays, uint32_t count, wf_hit* hits,
+                              cudaStream_t stream);
+wf_status trace_any_batch(const wf_scene* scene, const wf_ray* rays, const float* max_distance, uint32_t count,
+                          uint8_t* occluded, cudaStream_t stream);
+wf_status cuda_fail(cudaError_t e, const char* what);
+}  // namespace wf

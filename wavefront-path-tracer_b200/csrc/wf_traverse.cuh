@@ -1,0 +1,540 @@
+// Closest-hit and any-hit traversal.
+//
+// Semantics follow the reference's traceRay / isOccluded
+// (include/renderer/device_traversal.cuh:1035-1184) exactly: the same visit
+// order (direct spheres, direct instances, static triangles, TLAS, direct
+// triangle list), the same slab and Moller-Trumbore arithmetic, the same
+// strict "<" tie rule for triangles and lower-index rule for spheres, and the
+// same near-first child order (ties go to the right child).  The node layout
+// differs (both child boxes in the parent, see wf_device.cuh); a popped entry
+// carries the entry distance recorded when it was pushed, and re-testing
+// "entry < closestT" is exactly the reference's re-test of the popped node's
+// box (its other condition cannot change between push and pop).
+#pragma once
+
+#include <cfloat>
+
+#include "wf_device.cuh"
+
+namespace wf {
+
+constexpr int kStackSize = 64;  // leaf depth <= kMaxBvhDepth (60) < 64
+
+struct TraceState {
+    float t;          // closestT
+    float u, v;
+    uint32_t prim;    // make_prim(kind, index); kind kHitMiss = no hit
+    uint32_t inst;    // instance of a kHitMesh hit
+    uint32_t sphere;  // closestSphereIndex (reset to kInvalid by triangle hits)
+};
+
+WF_DEV void trace_state_init(TraceState& h, float t_max) {
+    h.t = t_max;
+    h.u = h.v = 0.0f;
+    h.prim = make_prim(kHitMiss, 0);
+    h.inst = kInvalid;
+    h.sphere = kInvalid;
+}
+
+// intersectAabb, device_traversal.cuh:182-197.
+WF_DEV bool slab(V3 o, V3 inv, float lox, float hix, float loy, float hiy, float loz, float hiz,
+                 float closest_t, float& near_t) {
+    float tx0 = (lox - o.x) * inv.x;
+    float tx1 = (hix - o.x) * inv.x;
+    float ty0 = (loy - o.y) * inv.y;
+    float ty1 = (hiy - o.y) * inv.y;
+    float tz0 = (loz - o.z) * inv.z;
+    float tz1 = (hiz - o.z) * inv.z;
+    float tmin = fmaxf(fminf(tx0, tx1), fmaxf(fminf(ty0, ty1), fminf(tz0, tz1)));
+    float tmax = fminf(fmaxf(tx0, tx1), fminf(fmaxf(ty0, ty1), fmaxf(tz0, tz1)));
+    near_t = tmin;
+    return tmax >= fmaxf(tmin, kRayMinDistance) && tmin < closest_t;
+}
+
+WF_DEV bool slab_box(V3 o, V3 inv, const Box& b, float closest_t, float& near_t) {
+    return slab(o, inv, b.lo[0], b.hi[0], b.lo[1], b.hi[1], b.lo[2], b.hi[2], closest_t, near_t);
+}
+
+WF_DEV V3 inverse_direction(V3 d) { return V3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z}; }
+
+// intersectSphere, device_traversal.cuh:24-53.
+WF_DEV bool intersect_sphere(V3 o, V3 d, float4 s, float& t) {
+    V3 oc = o - V3{s.x, s.y, s.z};
+    float a = dot(d, d);
+    float b = 2.0f * dot(oc, d);
+    float c = dot(oc, oc) - s.w * s.w;
+    float discriminant = b * b - 4.0f * a * c;
+    if (discriminant < 0.0f) return false;
+    float sq = sqrtf(discriminant);
+    float t0 = (-b - sq) / (2.0f * a);
+    float t1 = (-b + sq) / (2.0f * a);
+    if (t0 > kRayMinDistance) { t = t0; return true; }
+    if (t1 > kRayMinDistance) { t = t1; return true; }
+    return false;
+}
+
+// intersectTriangle, device_traversal.cuh:55-91 (Moller-Trumbore with the
+// determinant-scale cancellation guard).
+WF_DEV bool intersect_triangle(V3 o, V3 d, V3 v0, V3 v1, V3 v2, float& t, float& u, float& v) {
+    V3 e1 = v1 - v0;
+    V3 e2 = v2 - v0;
+    V3 p = cross(d, e2);
+    float det = dot(e1, p);
+    float scale = fabsf(e1.x) * (fabsf(d.y * e2.z) + fabsf(d.z * e2.y)) +
+                  fabsf(e1.y) * (fabsf(d.z * e2.x) + fabsf(d.x * e2.z)) +
+                  fabsf(e1.z) * (fabsf(d.x * e2.y) + fabsf(d.y * e2.x));
+    if (!isfinite(det) || fabsf(det) <= 8.0f * FLT_EPSILON * scale) return false;
+    float inv = 1.0f / det;
+    V3 ov = o - v0;
+    u = dot(ov, p) * inv;
+    if (u < 0.0f || u > 1.0f) return false;
+    V3 q = cross(ov, e1);
+    v = dot(d, q) * inv;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    t = dot(e2, q) * inv;
+    return t > kRayMinDistance;
+}
+
+struct TriVerts {
+    V3 v0, v1, v2;
+    uint32_t index_flags, material, light;
+};
+
+WF_DEV TriVerts load_triangle(const DeviceScene& s, uint32_t i) {
+    float4 a = __ldg(&s.triangles[3 * size_t(i)]);
+    float4 b = __ldg(&s.triangles[3 * size_t(i) + 1]);
+    float4 c = __ldg(&s.triangles[3 * size_t(i) + 2]);
+    return TriVerts{f4xyz(a), f4xyz(b), f4xyz(c), __float_as_uint(a.w), __float_as_uint(b.w),
+                    __float_as_uint(c.w)};
+}
+
+WF_DEV bool alpha_rejects(const DeviceScene& s, uint32_t material) {
+    return s.any_alpha_reject && (s.materials[material].flags & kMatAlphaReject);
+}
+
+// Local stack of (ref, entry distance).
+struct Stack {
+    int ref[kStackSize];
+    float t[kStackSize];
+    int size;
+};
+
+// Closest hit in one BVH over triangles (BLAS with a local ray, or the direct
+// list with the world ray).  intersectNexusBvh2, device_traversal.cuh:239-313.
+// kind/inst label accepted hits; override replaces the triangle material.
+WF_DEV void bvh_closest(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, TraceState& h,
+                        uint32_t kind, uint32_t inst, uint32_t material_override) {
+    V3 inv = inverse_direction(d);
+    float near_t;
+    if (bvh.root == kNoRoot || !slab_box(o, inv, bvh.box, h.t, near_t)) return;
+    Stack st;
+    st.size = 0;
+    int ref = bvh.root;
+    for (;;) {
+        if (ref < 0) {
+            uint32_t ti = uint32_t(~ref);
+            TriVerts tri = load_triangle(s, ti);
+            float t, u, v;
+            if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < h.t) {
+                uint32_t m = material_override == kInvalid ? tri.material : material_override;
+                if (!alpha_rejects(s, m)) {
+                    h.t = t;
+                    h.u = u;
+                    h.v = v;
+                    h.prim = make_prim(kind, ti);
+                    h.inst = inst;
+                }
+            }
+        } else {
+            const BvhNode* node = &s.nodes[ref];
+            float4 lxy = __ldg(&node->lxy);
+            float4 rxy = __ldg(&node->rxy);
+            float4 lrz = __ldg(&node->lrz);
+            int4 ch = __ldg(&node->child);
+            float tl, tr;
+            bool hl = slab(o, inv, lxy.x, lxy.y, lxy.z, lxy.w, lrz.x, lrz.y, h.t, tl);
+            bool hr = slab(o, inv, rxy.x, rxy.y, rxy.z, rxy.w, lrz.z, lrz.w, h.t, tr);
+            if (hl && hr) {
+                bool left_near = tl < tr;
+                if (st.size < kStackSize) {  // depth <= kMaxBvhDepth < kStackSize by construction
+                    st.ref[st.size] = left_near ? ch.y : ch.x;
+                    st.t[st.size] = left_near ? tr : tl;
+                    ++st.size;
+                }
+                ref = left_near ? ch.x : ch.y;
+                continue;
+            }
+            if (hl) { ref = ch.x; continue; }
+            if (hr) { ref = ch.y; continue; }
+        }
+        for (;;) {
+            if (st.size == 0) return;
+            --st.size;
+            if (st.t[st.size] < h.t) break;
+        }
+        ref = st.ref[st.size];
+    }
+}
+
+// Any hit with t < t_max in one triangle BVH.
+WF_DEV bool bvh_any(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, float t_max,
+                    uint32_t material_override) {
+    V3 inv = inverse_direction(d);
+    float near_t;
+    if (bvh.root == kNoRoot || !slab_box(o, inv, bvh.box, t_max, near_t)) return false;
+    int stack[kStackSize];
+    int size = 0;
+    int ref = bvh.root;
+    for (;;) {
+        if (ref < 0) {
+            uint32_t ti = uint32_t(~ref);
+            TriVerts tri = load_triangle(s, ti);
+            float t, u, v;
+            if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < t_max) {
+                uint32_t m = material_override == kInvalid ? tri.material : material_override;
+                if (!alpha_rejects(s, m)) return true;
+            }
+        } else {
+            const BvhNode* node = &s.nodes[ref];
+            float4 lxy = __ldg(&node->lxy);
+            float4 rxy = __ldg(&node->rxy);
+            float4 lrz = __ldg(&node->lrz);
+            int4 ch = __ldg(&node->child);
+            float tl, tr;
+            bool hl = slab(o, inv, lxy.x, lxy.y, lxy.z, lxy.w, lrz.x, lrz.y, t_max, tl);
+            bool hr = slab(o, inv, rxy.x, rxy.y, rxy.z, rxy.w, lrz.z, lrz.w, t_max, tr);
+            if (hl && hr) {
+                bool left_near = tl < tr;
+                if (size < kStackSize) stack[size++] = left_near ? ch.y : ch.x;
+                ref = left_near ? ch.x : ch.y;
+                continue;
+            }
+            if (hl) { ref = ch.x; continue; }
+            if (hr) { ref = ch.y; continue; }
+        }
+        if (size == 0) return false;
+        ref = stack[--size];
+    }
+}
+
+// inverseTransformVector(T, v), include/scene/scene.cuh:44-47.
+WF_DEV V3 to_local_vector(const Instance& in, V3 v) {
+    V3 x{in.w2l_x.x, in.w2l_x.y, in.w2l_x.z};
+    V3 y{in.w2l_y.x, in.w2l_y.y, in.w2l_y.z};
+    V3 z{in.w2l_z.x, in.w2l_z.y, in.w2l_z.z};
+    return x * v.x + y * v.y + z * v.z;
+}
+WF_DEV V3 instance_translation(const Instance& in) { return V3{in.w2l_x.w, in.w2l_y.w, in.w2l_z.w}; }
+
+WF_DEV Instance load_instance(const DeviceScene& s, uint32_t i) {
+    const Instance* p = &s.instances[i];
+    Instance in;
+    in.w2l_x = __ldg(&p->w2l_x);
+    in.w2l_y = __ldg(&p->w2l_y);
+    in.w2l_z = __ldg(&p->w2l_z);
+    in.blas = __ldg(&p->blas);
+    in.light_offset = __ldg(&p->light_offset);
+    in.material_override = __ldg(&p->material_override);
+    return in;
+}
+
+// Linear scan of a mesh in original triangle order (intersectMeshInstance
+// with useBvh = false, device_traversal.cuh:814-821).
+WF_DEV void mesh_linear_closest(const DeviceScene& s, const Blas& b, V3 o, V3 d, TraceState& h,
+                                uint32_t inst, uint32_t material_override) {
+    for (uint32_t i = 0; i < b.count; ++i) {
+        uint32_t ti = s.mesh_linear[b.first_linear + i];
+        TriVerts tri = load_triangle(s, ti);
+        float t, u, v;
+        if (!intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
+        uint32_t m = material_override == kInvalid ? tri.material : material_override;
+        if (alpha_rejects(s, m)) continue;
+        h.t = t;
+        h.u = u;
+        h.v = v;
+        h.prim = make_prim(kHitMesh, ti);
+        h.inst = inst;
+    }
+}
+
+// intersectMeshInstance, device_traversal.cuh:802-834 (attribute transforms
+// are deferred to finish_hit).
+WF_DEV void instance_closest(const DeviceScene& s, uint32_t inst, V3 o, V3 d, TraceState& h, bool use_bvh) {
+    Instance in = load_instance(s, inst);
+    Blas b = s.blases[in.blas];
+    V3 lo = to_local_vector(in, o - instance_translation(in));
+    V3 ld = to_local_vector(in, d);
+    float previous = h.t;
+    if (use_bvh && b.bvh.root != kNoRoot)
+        bvh_closest(s, b.bvh, lo, ld, h, kHitMesh, inst, in.material_override);
+    else
+        mesh_linear_closest(s, b, lo, ld, h, inst, in.material_override);
+    if (h.t >= previous) return;
+    h.sphere = kInvalid;
+}
+
+WF_DEV bool instance_any(const DeviceScene& s, uint32_t inst, V3 o, V3 d, float t_max, bool use_bvh) {
+    Instance in = load_instance(s, inst);
+    Blas b = s.blases[in.blas];
+    V3 lo = to_local_vector(in, o - instance_translation(in));
+    V3 ld = to_local_vector(in, d);
+    if (use_bvh && b.bvh.root != kNoRoot) return bvh_any(s, b.bvh, lo, ld, t_max, in.material_override);
+    for (uint32_t i = 0; i < b.count; ++i) {
+        TriVerts tri = load_triangle(s, s.mesh_linear[b.first_linear + i]);
+        float t, u, v;
+        if (!intersect_triangle(lo, ld, tri.v0, tri.v1, tri.v2, t, u, v) || t >= t_max) continue;
+        uint32_t m = in.material_override == kInvalid ? tri.material : in.material_override;
+        if (!alpha_rejects(s, m)) return true;
+    }
+    return false;
+}
+
+// intersectSphereHit, device_traversal.cuh:789-800.
+WF_DEV void sphere_closest(const DeviceScene& s, uint32_t index, V3 o, V3 d, TraceState& h) {
+    float t;
+    if (!intersect_sphere(o, d, __ldg(&s.spheres[index]), t) || t > h.t) return;
+    if (t == h.t && index >= h.sphere) return;
+    h.t = t;
+    h.prim = make_prim(kHitSphere, index);
+    h.sphere = index;
+}
+
+// intersectSceneTlas, device_traversal.cuh:836-878.
+WF_DEV void tlas_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h) {
+    if (s.tlas.root == kNoRoot) return;
+    V3 inv = inverse_direction(d);
+    float near_t;
+    if (!slab_box(o, inv, s.tlas.box, h.t, near_t)) return;
+    Stack st;
+    st.size = 0;
+    int ref = s.tlas.root;
+    for (;;) {
+        if (ref < 0) {
+            uint32_t leaf = __ldg(&s.tlas_leaves[~ref]);
+            if (leaf & 0x80000000u)
+                sphere_closest(s, leaf & 0x7fffffffu, o, d, h);
+            else
+                instance_closest(s, leaf, o, d, h, true);
+        } else {
+            const BvhNode* node = &s.nodes[ref];
+            float4 lxy = __ldg(&node->lxy);
+            float4 rxy = __ldg(&node->rxy);
+            float4 lrz = __ldg(&node->lrz);
+            int4 ch = __ldg(&node->child);
+            float tl, tr;
+            bool hl = slab(o, inv, lxy.x, lxy.y, lxy.z, lxy.w, lrz.x, lrz.y, h.t, tl);
+            bool hr = slab(o, inv, rxy.x, rxy.y, rxy.z, rxy.w, lrz.z, lrz.w, h.t, tr);
+            if (hl && hr) {
+                bool left_near = tl < tr;
+                if (st.size < kStackSize) {  // depth <= kMaxBvhDepth < kStackSize by construction
+                    st.ref[st.size] = left_near ? ch.y : ch.x;
+                    st.t[st.size] = left_near ? tr : tl;
+                    ++st.size;
+                }
+                ref = left_near ? ch.x : ch.y;
+                continue;
+            }
+            if (hl) { ref = ch.x; continue; }
+            if (hr) { ref = ch.y; continue; }
+        }
+        for (;;) {
+            if (st.size == 0) return;
+            --st.size;
+            if (st.t[st.size] < h.t) break;
+        }
+        ref = st.ref[st.size];
+    }
+}
+
+WF_DEV bool tlas_any(const DeviceScene& s, V3 o, V3 d, float t_max) {
+    if (s.tlas.root == kNoRoot) return false;
+    V3 inv = inverse_direction(d);
+    float near_t;
+    if (!slab_box(o, inv, s.tlas.box, t_max, near_t)) return false;
+    int stack[kStackSize];
+    int size = 0;
+    int ref = s.tlas.root;
+    for (;;) {
+        if (ref < 0) {
+            uint32_t leaf = __ldg(&s.tlas_leaves[~ref]);
+            if (leaf & 0x80000000u) {
+                float t;
+                if (intersect_sphere(o, d, __ldg(&s.spheres[leaf & 0x7fffffffu]), t) && t < t_max) return true;
+            } else if (instance_any(s, leaf, o, d, t_max, true)) {
+                return true;
+            }
+        } else {
+            const BvhNode* node = &s.nodes[ref];
+            float4 lxy = __ldg(&node->lxy);
+            float4 rxy = __ldg(&node->rxy);
+            float4 lrz = __ldg(&node->lrz);
+            int4 ch = __ldg(&node->child);
+            float tl, tr;
+            bool hl = slab(o, inv, lxy.x, lxy.y, lxy.z, lxy.w, lrz.x, lrz.y, t_max, tl);
+            bool hr = slab(o, inv, rxy.x, rxy.y, rxy.z, rxy.w, lrz.z, lrz.w, t_max, tr);
+            if (hl && hr) {
+                bool left_near = tl < tr;
+                if (size < kStackSize) stack[size++] = left_near ? ch.y : ch.x;
+                ref = left_near ? ch.x : ch.y;
+                continue;
+            }
+            if (hl) { ref = ch.x; continue; }
+            if (hr) { ref = ch.y; continue; }
+        }
+        if (size == 0) return false;
+        ref = stack[--size];
+    }
+}
+
+// traceRay, device_traversal.cuh:1115-1150 (visit order and sphere reset rules).
+WF_DEV void trace_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h) {
+    trace_state_init(h, 1e30f);
+    for (uint32_t i = 0; i < s.direct_sphere_count; ++i) sphere_closest(s, s.direct_spheres[i], o, d, h);
+    for (uint32_t i = 0; i < s.direct_instance_count; ++i) instance_closest(s, s.direct_instances[i], o, d, h, false);
+    for (uint32_t i = 0; i < s.static_count; ++i) {
+        uint32_t ti = s.static_first + i;
+        TriVerts tri = load_triangle(s, ti);
+        float t, u, v;
+        if (!intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
+        if (alpha_rejects(s, tri.material)) continue;
+        h.t = t;
+        h.u = u;
+        h.v = v;
+        h.prim = make_prim(kHitTriangle, ti);
+        h.inst = kInvalid;
+        h.sphere = kInvalid;
+    }
+    tlas_closest(s, o, d, h);
+    if (s.direct_count > 0) {
+        float previous = h.t;
+        if (s.direct_bvh.root != kNoRoot) {
+            bvh_closest(s, s.direct_bvh, o, d, h, kHitTriangle, kInvalid, kInvalid);
+        } else {
+            for (uint32_t i = 0; i < s.direct_count; ++i) {
+                uint32_t ti = s.direct_first + i;
+                TriVerts tri = load_triangle(s, ti);
+                float t, u, v;
+                if (!intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
+                if (alpha_rejects(s, tri.material)) continue;
+                h.t = t;
+                h.u = u;
+                h.v = v;
+                h.prim = make_prim(kHitTriangle, ti);
+                h.inst = kInvalid;
+            }
+        }
+        if (h.t < previous) h.sphere = kInvalid;
+    }
+}
+
+// isOccluded, device_traversal.cuh:1035-1113.  A pure disjunction of
+// independent tests, so an early return at the first hit gives the same bit.
+WF_DEV bool trace_any(const DeviceScene& s, V3 o, V3 d, float t_max) {
+    for (uint32_t i = 0; i < s.direct_sphere_count; ++i) {
+        float t;
+        if (intersect_sphere(o, d, __ldg(&s.spheres[s.direct_spheres[i]]), t) && t < t_max) return true;
+    }
+    for (uint32_t i = 0; i < s.direct_instance_count; ++i)
+        if (instance_any(s, s.direct_instances[i], o, d, t_max, false)) return true;
+    for (uint32_t i = 0; i < s.static_count; ++i) {
+        TriVerts tri = load_triangle(s, s.static_first + i);
+        float t, u, v;
+        if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < t_max &&
+            !alpha_rejects(s, tri.material))
+            return true;
+    }
+    if (tlas_any(s, o, d, t_max)) return true;
+    if (s.direct_count > 0) {
+        if (s.direct_bvh.root != kNoRoot) return bvh_any(s, s.direct_bvh, o, d, t_max, kInvalid);
+        for (uint32_t i = 0; i < s.direct_count; ++i) {
+            TriVerts tri = load_triangle(s, s.direct_first + i);
+            float t, u, v;
+            if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < t_max &&
+                !alpha_rejects(s, tri.material))
+                return true;
+        }
+    }
+    return false;
+}
+
+// Surface attributes of the winning primitive (the Hit fields the shading
+// stage uses), computed once after traversal exactly as the reference
+// computes them at acceptance time: getTriangleGeometricNormal /
+// getTriangleNormal with the (local) ray, transformNormal for instances
+// (device_traversal.cuh:104-125,149-152,824-832; scene.cuh:50-55), sphere
+// normals at the end of traceRay (:1152-1160).
+struct SurfaceHit {
+    float t;
+    V3 position;
+    V3 geometric_normal;
+    V3 normal;
+    uint32_t material;
+    uint32_t light;
+};
+
+WF_DEV V3 triangle_geometric_normal(const TriVerts& tri, V3 d, bool face_forward) {
+    V3 n = normalize(cross(tri.v1 - tri.v0, tri.v2 - tri.v0));
+    return face_forward && dot(n, d) > 0.0f ? -n : n;
+}
+
+WF_DEV V3 triangle_shading_normal(const DeviceScene& s, uint32_t ti, const TriVerts& tri, V3 d, float u,
+                                  float v, bool face_forward) {
+    V3 n;
+    if ((tri.index_flags & kTriHasNormals) && s.normals) {
+        V3 n0 = f4xyz(s.normals[3 * size_t(ti)]);
+        V3 n1 = f4xyz(s.normals[3 * size_t(ti) + 1]);
+        V3 n2 = f4xyz(s.normals[3 * size_t(ti) + 2]);
+        n = normalize((1.0f - u - v) * n0 + u * n1 + v * n2);
+    } else {
+        n = normalize(cross(tri.v1 - tri.v0, tri.v2 - tri.v0));
+    }
+    return face_forward && dot(n, d) > 0.0f ? -n : n;
+}
+
+// transformNormal, include/scene/scene.cuh:50-55.
+WF_DEV V3 transform_normal(const Instance& in, V3 n) {
+    V3 x{in.w2l_x.x, in.w2l_x.y, in.w2l_x.z};
+    V3 y{in.w2l_y.x, in.w2l_y.y, in.w2l_y.z};
+    V3 z{in.w2l_z.x, in.w2l_z.y, in.w2l_z.z};
+    return normalize(V3{dot(x, n), dot(y, n), dot(z, n)});
+}
+
+WF_DEV bool finish_hit(const DeviceScene& s, V3 o, V3 d, float t, float u, float v, uint32_t prim,
+                       uint32_t inst, SurfaceHit& out) {
+    uint32_t kind = hit_kind(prim), index = hit_index(prim);
+    if (kind == kHitMiss) return false;
+    out.t = t;
+    if (kind == kHitSphere) {
+        float4 sp = __ldg(&s.spheres[index]);
+        V3 at = o + d * t;
+        out.normal = normalize(at - V3{sp.x, sp.y, sp.z});
+        out.geometric_normal = out.normal;
+        out.material = s.sphere_materials[index];
+        out.light = kInvalid;
+    } else if (kind == kHitTriangle) {
+        TriVerts tri = load_triangle(s, index);
+        out.material = tri.material;
+        bool ff = s.materials[tri.material].type != kDielectric;
+        out.geometric_normal = triangle_geometric_normal(tri, d, ff);
+        out.normal = triangle_shading_normal(s, index, tri, d, u, v, ff);
+        out.light = tri.light;
+    } else {
+        Instance in = load_instance(s, inst);
+        TriVerts tri = load_triangle(s, index);
+        V3 ld = to_local_vector(in, d);
+        uint32_t m = in.material_override == kInvalid ? tri.material : in.material_override;
+        out.material = m;
+        bool ff = s.materials[m].type != kDielectric;
+        V3 gn = triangle_geometric_normal(tri, ld, ff);
+        V3 n = triangle_shading_normal(s, index, tri, ld, u, v, ff);
+        out.geometric_normal = transform_normal(in, gn);
+        out.normal = transform_normal(in, n);
+        uint32_t light = in.material_override == kInvalid ? tri.light : kInvalid;
+        if (light != kInvalid) light += in.light_offset;
+        out.light = light;
+    }
+    out.position = o + d * t;
+    return true;
+}
+
+}  // namespace wf

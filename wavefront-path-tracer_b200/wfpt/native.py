@@ -1,0 +1,320 @@
+"""Host-side mirror of the reference's render interface over the C ABI.
+
+`Scene` plays the role of the reference's HostScene (include/scene/scene_host.hpp),
+`DeviceScene` of DeviceScene/uploadScene (src/scene/scene.cu:336-389),
+`Renderer` of RenderDriver + RenderTaskRenderer (render_driver.cuh,
+render_task.cuh).  All compute runs in libwavefront_b200.so; this module only
+marshals arrays.  There is no fallback: a missing library is an error.
+"""
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+
+PACKAGE_DIR = Path(__file__).resolve().parents[1]
+LIB_PATH = PACKAGE_DIR / "libwavefront_b200.so"
+_lib = None
+
+
+class WavefrontError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def library():
+    """Loads libwavefront_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {PACKAGE_DIR}` "
+                               "or __graft_entry__.build()")
+        lib = C.CDLL(str(LIB_PATH))
+        abi.declare(lib)
+        _lib = lib
+    return _lib
+
+
+def check(status):
+    if status != abi.WF_OK:
+        msg = library().wf_last_error()
+        raise WavefrontError(status, msg.decode() if msg else "")
+
+
+def material(kind, albedo=(0.0, 0.0, 0.0), emission=(0.0, 0.0, 0.0), roughness=0.0, ior=1.0, **extra):
+    """One wf_material record with the reference's member defaults
+    (include/scene/material.cuh:30-70; roughness 0 and ior 1 as makeMaterial
+    sets them, src/scene/scene_host.cpp:44-52)."""
+    m = np.zeros(1, abi.MATERIAL_DTYPE)
+    m["type"] = kind
+    m["attenuation_color"] = 1.0
+    m["volume_density"] = 1.0
+    m["opacity"] = 1.0
+    m["alpha_cutoff"] = 0.5
+    m["specular"] = 1.0
+    m["glossiness"] = 1.0
+    m["specular_weight"] = 1.0
+    m["specular_color"] = 1.0
+    m["albedo"] = albedo
+    m["emission"] = emission
+    m["roughness"] = roughness
+    m["ior"] = ior
+    for k, v in extra.items():
+        m[k] = v
+    return m[0]
+
+
+class Scene:
+    """HostScene equivalent: numpy arrays in wf_* layouts."""
+
+    def __init__(self):
+        self.spheres = np.zeros(0, abi.SPHERE_DTYPE)
+        self.triangles = np.zeros(0, abi.TRIANGLE_DTYPE)
+        self.static_triangles = np.zeros(0, abi.TRIANGLE_DTYPE)
+        self.meshes = []
+        self.instances = np.zeros(0, abi.INSTANCE_DTYPE)
+        self.materials = np.zeros(0, abi.MATERIAL_DTYPE)
+        self.punctual = np.zeros(0, abi.PUNCTUAL_DTYPE)
+        self.environment = None  # dict(rgba=float32[h, w, 4], intensity=, rotation=)
+        self.black_background = False
+        self.ignore_direct_light_occlusion = False
+        self.register_triangle_lights = True
+        self.build_threads = 0
+
+    def add_material(self, record):
+        self.materials = np.concatenate([self.materials, np.array([record], abi.MATERIAL_DTYPE)])
+        return len(self.materials) - 1
+
+    def add_mesh(self, triangles):
+        self.meshes.append(np.ascontiguousarray(triangles, abi.TRIANGLE_DTYPE))
+        return len(self.meshes) - 1
+
+    def triangle_count(self):
+        return len(self.triangles) + len(self.static_triangles) + sum(len(m) for m in self.meshes)
+
+    def desc(self):
+        """(SceneDesc, keepalive list) for the C ABI."""
+        keep = []
+
+        def arr(a, dtype):
+            a = np.ascontiguousarray(a, dtype)
+            keep.append(a)
+            return a
+
+        meshes = np.zeros(len(self.meshes), abi.MESH_DTYPE)
+        for i, m in enumerate(self.meshes):
+            m = arr(m, abi.TRIANGLE_DTYPE)
+            meshes[i]["triangles"] = m.ctypes.data if len(m) else 0
+            meshes[i]["triangle_count"] = len(m)
+        keep.append(meshes)
+        d = abi.SceneDesc()
+        for name, src, dtype in [("spheres", self.spheres, abi.SPHERE_DTYPE),
+                                 ("triangles", self.triangles, abi.TRIANGLE_DTYPE),
+                                 ("static_triangles", self.static_triangles, abi.TRIANGLE_DTYPE),
+                                 ("instances", self.instances, abi.INSTANCE_DTYPE),
+                                 ("materials", self.materials, abi.MATERIAL_DTYPE),
+                                 ("punctual_lights", self.punctual, abi.PUNCTUAL_DTYPE)]:
+            a = arr(src, dtype)
+            setattr(d, name, abi.ptr(a))
+            count_name = "punctual_light_count" if name == "punctual_lights" else name[:-1] + "_count"
+            setattr(d, count_name, len(a))
+        d.meshes = abi.ptr(meshes)
+        d.mesh_count = len(meshes)
+        d.black_background = int(self.black_background)
+        d.ignore_direct_light_occlusion = int(self.ignore_direct_light_occlusion)
+        d.register_triangle_lights = int(self.register_triangle_lights)
+        d.build_threads = self.build_threads
+        return d, keep
+
+    def environment_struct(self):
+        if self.environment is None:
+            return None, None
+        rgba = np.ascontiguousarray(self.environment["rgba"], np.float32)
+        e = abi.Environment(rgba.shape[1], rgba.shape[0], rgba.ctypes.data,
+                            float(self.environment.get("intensity", 1.0)),
+                            float(self.environment.get("rotation", 0.0)))
+        return e, rgba
+
+
+class DeviceScene:
+    """A scene uploaded to the current CUDA device (wf_scene_create)."""
+
+    def __init__(self, scene):
+        lib = library()
+        d, keep = scene.desc()
+        handle = C.c_void_p()
+        check(lib.wf_scene_create(C.byref(d), C.byref(handle)))
+        self.handle = handle
+        env, rgba = scene.environment_struct()
+        if env is not None:
+            check(lib.wf_scene_set_environment(self.handle, C.byref(env)))
+        del keep, rgba
+
+    def info(self):
+        info = abi.SceneInfo()
+        check(library().wf_scene_get_info(self.handle, C.byref(info)))
+        return info
+
+    def set_environment(self, environment):
+        lib = library()
+        if environment is None:
+            check(lib.wf_scene_set_environment(self.handle, None))
+            return
+        rgba = np.ascontiguousarray(environment["rgba"], np.float32)
+        e = abi.Environment(rgba.shape[1], rgba.shape[0], rgba.ctypes.data,
+                            float(environment.get("intensity", 1.0)), float(environment.get("rotation", 0.0)))
+        check(lib.wf_scene_set_environment(self.handle, C.byref(e)))
+
+    def close(self):
+        if self.handle:
+            library().wf_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def trace_closest(self, rays):
+        """Closest hits of a numpy RAY_DTYPE batch (device round trip via torch)."""
+        import torch
+        rays = np.ascontiguousarray(rays, abi.RAY_DTYPE)
+        n = len(rays)
+        d_rays = torch.from_numpy(rays.view(np.uint8).copy()).cuda()
+        d_hits = torch.empty(n * abi.HIT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        check(library().wf_trace_closest(self.handle, d_rays.data_ptr(), n, d_hits.data_ptr(), stream))
+        torch.cuda.synchronize()
+        return d_hits.cpu().numpy().view(abi.HIT_DTYPE)
+
+    def trace_any(self, rays, max_distance):
+        import torch
+        rays = np.ascontiguousarray(rays, abi.RAY_DTYPE)
+        n = len(rays)
+        d_rays = torch.from_numpy(rays.view(np.uint8).copy()).cuda()
+        d_max = torch.from_numpy(np.ascontiguousarray(max_distance, np.float32)).cuda()
+        d_out = torch.empty(n, dtype=torch.uint8, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        check(library().wf_trace_any(self.handle, d_rays.data_ptr(), d_max.data_ptr(), n, d_out.data_ptr(), stream))
+        torch.cuda.synchronize()
+        return d_out.cpu().numpy()
+
+
+def camera_struct(cam):
+    c = abi.Camera()
+    for k in ("position", "forward", "right", "up"):
+        getattr(c, k)[:] = [float(x) for x in cam[k]]
+    c.vertical_fov = float(cam["vertical_fov"])
+    c.aspect_ratio = float(cam["aspect_ratio"])
+    return c
+
+
+def render_config(width, height, **fields):
+    """wf_render_config with the reference's defaults (config.hpp:11-41)."""
+    cfg = abi.RenderConfig()
+    library().wf_render_config_default(C.byref(cfg), width, height)
+    for k, v in fields.items():
+        if k in ("photon_grid_min", "photon_grid_max"):
+            getattr(cfg, k)[:] = [float(x) for x in v]
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+class Renderer:
+    """RenderDriver / RenderTaskRenderer equivalent (wf_renderer_*)."""
+
+    def __init__(self, device_scene, camera, config, stream=None):
+        self.scene = device_scene
+        self.config = config
+        self.width, self.height = config.width, config.height
+        handle = C.c_void_p()
+        cam = camera_struct(camera)
+        check(library().wf_renderer_create(device_scene.handle, C.byref(cam), C.byref(config), stream,
+                                           C.byref(handle)))
+        self.handle = handle
+
+    def close(self):
+        if getattr(self, "handle", None):
+            library().wf_renderer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, x, y, w, h, sample_start, sample_count, clear_tile=True):
+        check(library().wf_render(self.handle, x, y, w, h, sample_start, sample_count, int(clear_tile)))
+
+    def render_task(self, tile, sample_start, sample_count):
+        """RenderTaskRenderer::render: unnormalized tile sums over the sample range."""
+        x, y, w, h = tile
+        self.render(x, y, w, h, sample_start, sample_count, True)
+        return self.download(x, y, w, h)
+
+    def render_frame(self, sample_count):
+        check(library().wf_render_frame(self.handle, sample_count))
+
+    def synchronize(self):
+        check(library().wf_synchronize(self.handle))
+
+    def reset(self):
+        check(library().wf_framebuffer_reset(self.handle))
+
+    def download(self, x=0, y=0, w=None, h=None):
+        w = self.width if w is None else w
+        h = self.height if h is None else h
+        out = np.empty((h, w, 3), np.float32)
+        check(library().wf_framebuffer_download(self.handle, x, y, w, h, out.ctypes.data))
+        return out
+
+    def sample_index(self):
+        v = C.c_uint32()
+        check(library().wf_get_sample_index(self.handle, C.byref(v)))
+        return v.value
+
+    def set_sample_index(self, value):
+        check(library().wf_set_sample_index(self.handle, value))
+
+    def queue_counts(self):
+        out = np.zeros(self.config.max_depth, np.uint32)
+        check(library().wf_queue_counts(self.handle, out.ctypes.data, len(out)))
+        return out
+
+    def stats(self, reset=False):
+        s = abi.RenderStats()
+        check(library().wf_render_stats_get(self.handle, C.byref(s), int(reset)))
+        return {"extension_rays": s.extension_rays, "shadow_rays": s.shadow_rays, "paths": s.paths}
+
+    def photon_stats(self):
+        stored, emitted = C.c_uint32(), C.c_uint32()
+        check(library().wf_photon_stats(self.handle, C.byref(stored), C.byref(emitted)))
+        return stored.value, emitted.value
+
+    def photons(self):
+        _, emitted = self.photon_stats()
+        out = np.zeros((emitted, 8), np.float32)
+        check(library().wf_photons_download(self.handle, out.ctypes.data, emitted))
+        return out
+
+    def checkpoint_save(self, path, fingerprint):
+        check(library().wf_checkpoint_save(self.handle, os.fsencode(path), fingerprint))
+
+    def checkpoint_enqueue(self, path, fingerprint):
+        q = C.c_uint32()
+        check(library().wf_checkpoint_enqueue(self.handle, os.fsencode(path), fingerprint, C.byref(q)))
+        return bool(q.value)
+
+    def checkpoint_flush(self):
+        check(library().wf_checkpoint_flush(self.handle))
+
+    def checkpoint_load(self, path, fingerprint):
+        s = C.c_uint32()
+        check(library().wf_checkpoint_load(self.handle, os.fsencode(path), fingerprint, C.byref(s)))
+        return s.value

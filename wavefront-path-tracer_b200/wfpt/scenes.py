@@ -1,0 +1,374 @@
+"""Synthetic scene generators for the benchmark and parity workloads.
+
+No public dataset is involved: every scene is generated from a seed.  Scene
+randomness uses the reference's scene LCG, state * 1664525 + 1013904223 with
+(state >> 8) / 2^24 (src/scene/scene_host.cpp:55-58), so a scene is fully
+determined by its seed.
+
+Workloads (sizes as stated in the task's configuration list):
+  * cornell_box            256x256 Cornell box, 36 triangles, one emissive quad.
+  * sphere_field           22x22 jittered spheres + ground sphere + 3 instances
+                           of a displaced geodesic sphere (frequency 256 =
+                           1,310,720 triangles), sky gradient.
+  * large_mesh             2236x2236-quad fBm terrain (9,999,392 triangles,
+                           1% emissive), 500 instances of a 200,000-triangle
+                           displaced geodesic sphere, 20 glass spheres, HDR
+                           environment with a 0.5 degree sun.
+All sizes are parameters so tests can run reduced versions.
+"""
+import math
+
+import numpy as np
+
+from . import abi
+from .native import Scene, material
+
+# ------------------------------------------------------------------- RNG
+
+
+class SceneRng:
+    """The reference's scene LCG (scene_host.cpp:55-58), vectorised."""
+
+    A = 1664525
+    C = 1013904223
+
+    def __init__(self, seed):
+        self.state = np.uint32(seed)
+
+    def next(self):
+        self.state = np.uint32((int(self.state) * self.A + self.C) & 0xFFFFFFFF)
+        return float(np.float32(int(self.state) >> 8) * np.float32(1.0 / 16777216.0))
+
+    def stream(self, n):
+        """n successive draws (same values as n calls of next())."""
+        out = np.empty(n, np.float32)
+        lanes = min(n, 4096) if n > 0 else 0
+        if n == 0:
+            return out
+        # First `lanes` states sequentially, then leapfrog by `lanes` steps.
+        states = np.empty(lanes, np.uint64)
+        s = int(self.state)
+        for i in range(lanes):
+            s = (s * self.A + self.C) & 0xFFFFFFFF
+            states[i] = s
+        a_k, c_k = 1, 0
+        for _ in range(lanes):
+            a_k, c_k = (a_k * self.A) & 0xFFFFFFFF, (c_k * self.A + self.C) & 0xFFFFFFFF
+        rows = (n + lanes - 1) // lanes
+        block = np.empty((rows, lanes), np.uint64)
+        cur = states.copy()
+        for r in range(rows):
+            block[r] = cur
+            cur = (cur * np.uint64(a_k) + np.uint64(c_k)) & np.uint64(0xFFFFFFFF)
+        flat = block.reshape(-1)[:n]
+        self.state = np.uint32(int(flat[-1]))
+        out[:] = (flat >> np.uint64(8)).astype(np.float32) * np.float32(1.0 / 16777216.0)
+        return out
+
+
+# ------------------------------------------------------------ geometry
+
+
+def triangles(v0, v1, v2, mat):
+    t = np.zeros(len(v0), abi.TRIANGLE_DTYPE)
+    t["v0"], t["v1"], t["v2"] = v0, v1, v2
+    t["material"] = mat
+    return t
+
+
+def quad(v0, v1, v2, v3, mat):
+    """addQuad (scene_host.cpp:21-24): (v0, v1, v2) and (v0, v2, v3)."""
+    a = np.array([v0, v0], np.float32)
+    b = np.array([v1, v2], np.float32)
+    c = np.array([v2, v3], np.float32)
+    return triangles(a, b, c, mat)
+
+
+def box(center, size, yaw_deg, mat):
+    """Axis-aligned box rotated about +Y: 12 outward-wound triangles."""
+    cx, cy, cz = center
+    sx, sy, sz = size
+    corners = np.array([[x, y, z] for z in (-0.5, 0.5) for y in (-0.5, 0.5) for x in (-0.5, 0.5)], np.float64)
+    corners *= np.array([sx, sy, sz])
+    a = math.radians(yaw_deg)
+    rot = np.array([[math.cos(a), 0, math.sin(a)], [0, 1, 0], [-math.sin(a), 0, math.cos(a)]])
+    p = corners @ rot.T + np.array([cx, cy, cz])
+    faces = [(0, 2, 3, 1), (4, 5, 7, 6), (0, 1, 5, 4), (2, 6, 7, 3), (0, 4, 6, 2), (1, 3, 7, 5)]
+    out = [quad(p[f[0]], p[f[1]], p[f[2]], p[f[3]], mat) for f in faces]
+    return np.concatenate(out)
+
+
+def transform(translation=(0, 0, 0), scale=1.0, yaw_deg=0.0):
+    """(local_to_world, world_to_local) basis vectors of S * R_y."""
+    a = math.radians(yaw_deg)
+    rot = np.array([[math.cos(a), 0, math.sin(a)], [0, 1, 0], [-math.sin(a), 0, math.cos(a)]])
+    l2w = rot * scale
+    w2l = np.linalg.inv(l2w)
+    # Basis vectors: localToWorldX is the image of local +X = column 0.
+    return l2w.T.astype(np.float32), w2l.T.astype(np.float32), np.array(translation, np.float32)
+
+
+def instance(mesh, translation=(0, 0, 0), scale=1.0, yaw_deg=0.0, override=abi.NO_MATERIAL,
+             accel=abi.ACCEL_BVH):
+    r = np.zeros(1, abi.INSTANCE_DTYPE)
+    l2w, w2l, t = transform(translation, scale, yaw_deg)
+    r["mesh"] = mesh
+    r["material_override"] = override
+    r["accel"] = accel
+    r["local_to_world"] = l2w
+    r["world_to_local"] = w2l
+    r["translation"] = t
+    return r
+
+
+def _hash3(ix, iy, iz, seed):
+    h = (ix.astype(np.uint32) * np.uint32(73856093)) ^ (iy.astype(np.uint32) * np.uint32(19349663)) \
+        ^ (iz.astype(np.uint32) * np.uint32(83492791)) ^ np.uint32(seed * 2654435761 & 0xFFFFFFFF)
+    h ^= h >> np.uint32(13)
+    h *= np.uint32(0x5BD1E995)
+    h ^= h >> np.uint32(15)
+    return (h & np.uint32(0xFFFFFF)).astype(np.float64) / float(0xFFFFFF) * 2.0 - 1.0
+
+
+def value_noise(p, seed, octaves=3, frequency=2.0):
+    """Seeded fractal value noise in [-1, 1] (trilinear lattice, smoothstep)."""
+    total = np.zeros(len(p))
+    amp, norm = 1.0, 0.0
+    with np.errstate(over="ignore"):
+        for o in range(octaves):
+            q = p * frequency * (2 ** o)
+            i = np.floor(q).astype(np.int64)
+            f = q - i
+            f = f * f * (3 - 2 * f)
+            acc = np.zeros(len(p))
+            for dz in (0, 1):
+                for dy in (0, 1):
+                    for dx in (0, 1):
+                        w = (f[:, 0] if dx else 1 - f[:, 0]) * (f[:, 1] if dy else 1 - f[:, 1]) * \
+                            (f[:, 2] if dz else 1 - f[:, 2])
+                        acc += w * _hash3(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz, seed + o)
+            total += amp * acc
+            norm += amp
+            amp *= 0.5
+    return total / norm
+
+
+def geodesic_sphere(frequency, mat=0, displacement=0.0, seed=0, octaves=3):
+    """Icosahedron with every face split into frequency^2 triangles
+    (20 * frequency^2 total), vertices on the unit sphere, radially displaced
+    by seeded value noise."""
+    t = (1 + 5 ** 0.5) / 2
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    f = frequency
+    ii, jj = np.meshgrid(np.arange(f + 1), np.arange(f + 1), indexing="ij")
+    mask = ii + jj <= f
+    ii, jj = ii[mask], jj[mask]
+    index = -np.ones((f + 1, f + 1), np.int64)
+    index[ii, jj] = np.arange(len(ii))
+    ui, uj = np.meshgrid(np.arange(f), np.arange(f), indexing="ij")
+    up = ui + uj <= f - 1
+    a_up = index[ui[up], uj[up]], index[ui[up] + 1, uj[up]], index[ui[up], uj[up] + 1]
+    dn = ui + uj <= f - 2
+    a_dn = index[ui[dn] + 1, uj[dn]], index[ui[dn] + 1, uj[dn] + 1], index[ui[dn], uj[dn] + 1]
+    tri_idx = np.concatenate([np.stack(a_up, 1), np.stack(a_dn, 1)])
+    out = []
+    for (a, b, c) in faces:
+        pts = v[a] + (v[b] - v[a]) * (ii[:, None] / f) + (v[c] - v[a]) * (jj[:, None] / f)
+        pts /= np.linalg.norm(pts, axis=1, keepdims=True)
+        if displacement:
+            pts *= (1.0 + displacement * value_noise(pts, seed, octaves))[:, None]
+        out.append(pts[tri_idx])
+    tri = np.concatenate(out)
+    return triangles(tri[:, 0].astype(np.float32), tri[:, 1].astype(np.float32), tri[:, 2].astype(np.float32), mat)
+
+
+def look_at_camera(position, target, vertical_fov_deg, width, height):
+    """Camera as the reference's presets build it (src/scene/camera.cu:3-42)."""
+    p = np.array(position, np.float32)
+    fwd = np.array(target, np.float32) - p
+    fwd = fwd * np.float32(1.0 / math.sqrt(float(np.dot(fwd, fwd))))
+    up0 = np.array([0, 0, 1], np.float32) if abs(fwd[1]) > 0.999 else np.array([0, 1, 0], np.float32)
+    right = np.cross(fwd, up0).astype(np.float32)
+    right = right * np.float32(1.0 / math.sqrt(float(np.dot(right, right))))
+    up = np.cross(right, fwd).astype(np.float32)
+    return {"position": p, "forward": fwd, "right": right, "up": up,
+            "vertical_fov": np.float32(vertical_fov_deg * 3.14159265359 / 180.0),
+            "aspect_ratio": np.float32(width / height)}
+
+
+# --------------------------------------------------------------- scenes
+
+
+def cornell_box(width=256, height=256):
+    """Plain Cornell box: 5 walls (10 triangles), a 2-triangle ceiling light of
+    radiance 15 and two boxes rotated +-18 degrees (24 triangles), all 36 in one
+    mesh with one identity instance (TLAS/BLAS path).  Room, palette and light
+    placement follow assembleCornellScene (scene_host.cpp:325-341)."""
+    s = Scene()
+    white = s.add_material(material(abi.MAT_DIFFUSE, (0.73, 0.73, 0.73)))
+    red = s.add_material(material(abi.MAT_DIFFUSE, (0.65, 0.05, 0.05)))
+    green = s.add_material(material(abi.MAT_DIFFUSE, (0.12, 0.45, 0.15)))
+    box_white = s.add_material(material(abi.MAT_DIFFUSE, (0.72, 0.72, 0.72)))
+    light = s.add_material(material(abi.MAT_EMISSIVE, (1.0, 1.0, 1.0), (15.0, 15.0, 15.0)))
+    w, fy, cy, bz, fz = 2.5, -1.0, 3.0, -2.5, 2.5
+    tris = [
+        quad((-w, fy, fz), (w, fy, fz), (w, fy, bz), (-w, fy, bz), white),
+        quad((-w, cy, bz), (w, cy, bz), (w, cy, fz), (-w, cy, fz), white),
+        quad((-w, fy, bz), (w, fy, bz), (w, cy, bz), (-w, cy, bz), white),
+        quad((-w, fy, fz), (-w, fy, bz), (-w, cy, bz), (-w, cy, fz), red),
+        quad((w, fy, bz), (w, fy, fz), (w, cy, fz), (w, cy, bz), green),
+    ]
+    corner, eu, ev = np.array([-0.75, 2.95, -0.75]), np.array([1.5, 0, 0]), np.array([0, 0, 1.5])
+    tris.append(quad(corner, corner + eu, corner + eu + ev, corner + ev, light))
+    tris.append(box((0.85, -0.4, 0.55), (1.2, 1.2, 1.2), -18.0, box_white))
+    tris.append(box((-0.8, 0.2, -0.65), (1.2, 2.4, 1.2), 18.0, box_white))
+    mesh = s.add_mesh(np.concatenate(tris))
+    s.instances = instance(mesh)
+    s.black_background = True
+    cam = look_at_camera((0.0, 1.2, 6.5), (0.0, 0.8, -0.6), 42.0, width, height)
+    return s, cam
+
+
+def sphere_field(width=1280, height=720, frequency=256, grid=22, seed=7):
+    """22x22 radius-0.2 spheres jittered +-0.45 (80% Lambertian albedo u*u,
+    15% metal albedo U(0.5,1) fuzz U(0,0.5), 5% glass ior 1.5), a radius-1000
+    ground sphere tested directly, three instances (glass, metal, diffuse) of
+    one displaced geodesic sphere BLAS, sky gradient."""
+    s = Scene()
+    rng = SceneRng(seed)
+    ground = s.add_material(material(abi.MAT_DIFFUSE, (0.5, 0.5, 0.5)))
+    glass = s.add_material(material(abi.MAT_DIELECTRIC, (1.0, 1.0, 1.0), ior=1.5))
+    metal = s.add_material(material(abi.MAT_METAL, (0.8, 0.82, 0.9), roughness=0.05))
+    diffuse = s.add_material(material(abi.MAT_DIFFUSE, (0.8, 0.3, 0.3)))
+    spheres = [((0.0, -1000.0, 0.0), 1000.0, ground, abi.ACCEL_DIRECT)]
+    mats = []
+    half = grid // 2
+    for a in range(-half, grid - half):
+        for b in range(-half, grid - half):
+            choose = rng.next()
+            cx = a + (rng.next() - 0.5) * 0.9
+            cz = b + (rng.next() - 0.5) * 0.9
+            if choose < 0.80:
+                m = material(abi.MAT_DIFFUSE, (rng.next() * rng.next(), rng.next() * rng.next(), rng.next() * rng.next()))
+            elif choose < 0.95:
+                alb = (0.5 + 0.5 * rng.next(), 0.5 + 0.5 * rng.next(), 0.5 + 0.5 * rng.next())
+                m = material(abi.MAT_METAL, alb, roughness=0.5 * rng.next())
+            else:
+                m = material(abi.MAT_DIELECTRIC, (1.0, 1.0, 1.0), ior=1.5)
+            mats.append(m)
+            spheres.append(((cx, 0.2, cz), 0.2, len(s.materials) + len(mats) - 1, abi.ACCEL_BVH))
+    s.materials = np.concatenate([s.materials, np.array(mats, abi.MATERIAL_DTYPE)])
+    sp = np.zeros(len(spheres), abi.SPHERE_DTYPE)
+    for i, (c, r, m, acc) in enumerate(spheres):
+        sp[i] = (c, r, m, acc)
+    s.spheres = sp
+    mesh = s.add_mesh(geodesic_sphere(frequency, ground, displacement=0.08, seed=seed))
+    s.instances = np.concatenate([
+        instance(mesh, (-4.0, 1.0, 0.0), 1.0, 0.0, glass),
+        instance(mesh, (4.0, 1.0, 0.0), 1.0, 30.0, metal),
+        instance(mesh, (0.0, 1.0, 0.0), 1.0, 60.0, diffuse),
+    ])
+    s.black_background = False
+    cam = look_at_camera((13.0, 2.0, 3.0), (0.0, 0.8, 0.0), 32.0, width, height)
+    return s, cam
+
+
+def sun_sky_environment(width=2048, height=1024, sun_radius_deg=0.5, sun_intensity=5.0e4,
+                        sun_elevation_deg=35.0, sun_azimuth_deg=120.0):
+    """Synthetic HDR equirect map: a sky gradient plus a 0.5 degree sun disk.
+    Row 0 = +Y; columns follow environmentUv (environment.cuh:26-33)."""
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    theta = v * math.pi
+    phi = (u - 0.5) * 2 * math.pi
+    st, ct = np.sin(theta)[:, None], np.cos(theta)[:, None]
+    d = np.stack([st * np.cos(phi)[None, :], np.broadcast_to(ct, (height, width)), st * np.sin(phi)[None, :]], -1)
+    up = np.clip(d[..., 1], -1, 1)
+    sky = np.stack([0.45 + 0.25 * (1 - up), 0.6 + 0.2 * (1 - up), 1.0 + 0.0 * up], -1) * np.clip(up + 0.3, 0.05, 1.3)[..., None]
+    el, az = math.radians(sun_elevation_deg), math.radians(sun_azimuth_deg)
+    sun = np.array([math.cos(el) * math.cos(az), math.sin(el), math.cos(el) * math.sin(az)])
+    cosang = d @ sun
+    disk = cosang > math.cos(math.radians(sun_radius_deg))
+    rgba = np.zeros((height, width, 4), np.float32)
+    rgba[..., :3] = sky
+    rgba[disk, :3] = sun_intensity
+    rgba[..., 3] = 1.0
+    return {"rgba": rgba, "intensity": 1.0, "rotation": 0.0}
+
+
+def heightfield(n, extent, amplitude, seed):
+    """fBm terrain over an n x n quad grid: 2 n^2 triangles."""
+    xs = np.linspace(-extent, extent, n + 1)
+    gx, gz = np.meshgrid(xs, xs, indexing="xy")
+    p = np.stack([gx.ravel() / extent, np.zeros(gx.size), gz.ravel() / extent], 1)
+    h = amplitude * value_noise(p, seed, octaves=5, frequency=3.0)
+    pts = np.stack([gx.ravel(), h, gz.ravel()], 1).astype(np.float32).reshape(n + 1, n + 1, 3)
+    a = pts[:-1, :-1].reshape(-1, 3)
+    b = pts[:-1, 1:].reshape(-1, 3)
+    c = pts[1:, 1:].reshape(-1, 3)
+    d = pts[1:, :-1].reshape(-1, 3)
+    v0 = np.concatenate([a, a])
+    v1 = np.concatenate([d, c])
+    v2 = np.concatenate([c, b])
+    return v0, v1, v2, pts
+
+
+def large_mesh(width=1920, height=1080, terrain_quads=2236, instance_count=500, instance_frequency=100,
+               emissive_fraction=0.01, glass_spheres=20, env_size=(2048, 1024), seed=3):
+    """Large mesh with lights: fBm terrain, emissive terrain triangles
+    (radiance log-uniform in [1, 50], quantized to 64 materials), instanced
+    displaced geodesic spheres (scale U(0.5, 3), random yaw), glass spheres for
+    caustics, HDR sun-and-sky environment."""
+    s = Scene()
+    rng = np.random.default_rng(seed)
+    extent = 60.0
+    terrain_mat = s.add_material(material(abi.MAT_DIFFUSE, (0.45, 0.42, 0.38)))
+    rock_mats = [s.add_material(material(abi.MAT_DIFFUSE, (0.3 + 0.5 * rng.random(), 0.3 + 0.4 * rng.random(),
+                                                             0.25 + 0.3 * rng.random()))) for _ in range(4)]
+    rock_mats.append(s.add_material(material(abi.MAT_METAL, (0.9, 0.85, 0.7), roughness=0.2)))
+    glass = s.add_material(material(abi.MAT_DIELECTRIC, (1.0, 1.0, 1.0), ior=1.5))
+    levels = np.exp(np.linspace(math.log(1.0), math.log(50.0), 64))
+    emissive = [s.add_material(material(abi.MAT_EMISSIVE, (1, 1, 1), (float(l), float(l * 0.85), float(l * 0.6))))
+                for l in levels]
+    v0, v1, v2, pts = heightfield(terrain_quads, extent, 4.0, seed)
+    terrain = triangles(v0, v1, v2, terrain_mat)
+    n = len(terrain)
+    k = int(round(n * emissive_fraction))
+    pick = rng.choice(n, size=k, replace=False)
+    terrain["material"][pick] = np.array(emissive, np.uint32)[rng.integers(0, 64, size=k)]
+    tmesh = s.add_mesh(terrain)
+    rock = s.add_mesh(geodesic_sphere(instance_frequency, terrain_mat, displacement=0.15, seed=seed + 1))
+    inst = [instance(tmesh)]
+    grid_res = terrain_quads + 1
+
+    def ground_height(x, z):
+        i = np.clip(np.round((x + extent) / (2 * extent) * terrain_quads).astype(int), 0, grid_res - 1)
+        j = np.clip(np.round((z + extent) / (2 * extent) * terrain_quads).astype(int), 0, grid_res - 1)
+        return pts[j, i, 1]
+
+    xs = rng.uniform(-extent * 0.8, extent * 0.8, instance_count)
+    zs = rng.uniform(-extent * 0.8, extent * 0.8, instance_count)
+    scales = rng.uniform(0.5, 3.0, instance_count)
+    yaws = rng.uniform(0.0, 360.0, instance_count)
+    hs = ground_height(xs, zs)
+    for i in range(instance_count):
+        inst.append(instance(rock, (xs[i], hs[i] + 0.6 * scales[i], zs[i]), scales[i], yaws[i],
+                             rock_mats[i % len(rock_mats)]))
+    s.instances = np.concatenate(inst)
+    sp = np.zeros(glass_spheres, abi.SPHERE_DTYPE)
+    gx = rng.uniform(-12, 12, glass_spheres)
+    gz = rng.uniform(-12, 12, glass_spheres)
+    gr = rng.uniform(0.6, 1.6, glass_spheres)
+    gh = ground_height(gx, gz)
+    for i in range(glass_spheres):
+        sp[i] = ((gx[i], gh[i] + gr[i] + 0.2, gz[i]), gr[i], glass, abi.ACCEL_BVH)
+    s.spheres = sp
+    s.environment = sun_sky_environment(*env_size)
+    s.black_background = False
+    cam = look_at_camera((0.0, 14.0, 38.0), (0.0, 0.0, 0.0), 50.0, width, height)
+    return s, cam

@@ -1,0 +1,345 @@
+#!/usr/bin/env python3
+"""Throughput benchmark of the B200 wavefront path tracer.
+
+Workload (default): the large-mesh-with-lights configuration -- 1920x1080,
+max depth 12, a 9,999,392-triangle fBm terrain (1% emissive, radiance
+log-uniform in [1, 50]), 500 instances of a 200,000-triangle displaced
+geodesic sphere, 20 glass spheres, a 2048x1024 HDR sun-and-sky environment
+with MIS, and a 2M-photon caustic map.  Synthetic and seeded (no dataset).
+
+One step = one sample per pixel over the full frame (2,073,600 paths)
+through the captured-graph wavefront.  `value` = Mpaths/s over the timed
+steps with the scene resident in HBM; `e2e` = the same metric through the
+C-ABI task call (RenderTaskRenderer::render semantics: task in from the host,
+unnormalized radiance sums back to pinned host memory every step).
+
+--impl reference times the reference's own renderer code (host-compiled from
+its sources, oracle/_ref) on the host cores for the same workload.
+Multi-GPU (torchrun): every rank renders its own absolute sample range of the
+same frame (weak scaling); the framebuffers are summed with one NCCL reduce
+after the timed region.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "wavefront-path-tracer_b200"))
+
+WORKLOADS = {
+    # name: (scene kwargs, render kwargs)
+    "large_mesh": (dict(width=1920, height=1080), dict(max_depth=12, caustics=1, photon_count=2_000_000)),
+    "large_mesh_small": (dict(width=480, height=270, terrain_quads=256, instance_count=50, instance_frequency=30,
+                              glass_spheres=6, env_size=(512, 256)),
+                         dict(max_depth=12, caustics=1, photon_count=200_000)),
+    "sphere_field": (dict(width=1280, height=720), dict(max_depth=16)),
+    "cornell": (dict(width=256, height=256), dict(max_depth=8, rr_start_depth=3)),
+}
+HBM_FALLBACK_GBS = 6650.0
+
+
+def make_scene(name):
+    from wfpt import scenes
+    kw, rkw = WORKLOADS[name]
+    if name.startswith("large_mesh"):
+        scene, cam = scenes.large_mesh(**kw)
+    elif name == "sphere_field":
+        scene, cam = scenes.sphere_field(**kw)
+    else:
+        scene, cam = scenes.cornell_box(**kw)
+    return scene, cam, kw["width"], kw["height"], dict(rkw)
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(profile, kernel):
+    """Algorithmic bytes of one kernel's launches in the profiled pass.
+    Per ray state: 32 B ray in + 16 B hit/result out.  Traversal: 32 B per
+    node visit (one pair of child boxes), 48 B per triangle test, 16 B per
+    sphere test, 64 B per instance entry."""
+    if kernel == "trace":
+        rays, nodes, tris, sph, inst = (profile["extension_rays"], profile["closest_nodes"],
+                                        profile["closest_triangles"], profile["closest_spheres"],
+                                        profile["closest_instances"])
+    else:
+        rays, nodes, tris, sph, inst = (profile["shadow_rays"], profile["any_nodes"], profile["any_triangles"],
+                                        profile["any_spheres"], profile["any_instances"])
+    return 48 * rays + 32 * nodes + 48 * tris + 16 * sph + 64 * inst
+
+
+def ncu_traffic(kernel, workload):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / f"{kernel}_{workload}.json"
+    if p.exists():
+        data = json.loads(p.read_text())
+        return data.get("dram_bytes_per_launch_full_size")
+    return None
+
+
+def cpu_reference_rate(ref, cam, width, height, render_kwargs, seconds_target=15.0, threads=0):
+    """Mpaths/s of the host-compiled reference (an oracle.RefScene) on a band
+    of rows at 1 spp, sized to about `seconds_target` seconds."""
+    import wfpt
+    cfg = wfpt.render_config(width, height, **render_kwargs)
+    cores = threads or os.cpu_count() or 1
+    # One untimed row first: builds the reference's photon map once (it is
+    # built in RenderDriver::prepare, outside the trace timing).
+    ref.render(cam, cfg, tile=(0, height // 2, width, 1), sample_start=0, sample_count=1, threads=cores)
+    band = max(1, height // 64)
+    y0 = height // 2 - band // 2
+    t0 = time.perf_counter()
+    ref.render(cam, cfg, tile=(0, y0, width, band), sample_start=0, sample_count=1, threads=cores)
+    dt = time.perf_counter() - t0
+    if dt < seconds_target / 4:
+        band = min(height, max(band + 1, int(band * seconds_target / max(dt, 1e-3))))
+        y0 = max(0, height // 2 - band // 2)
+        t0 = time.perf_counter()
+        ref.render(cam, cfg, tile=(0, y0, width, band), sample_start=0, sample_count=1, threads=cores)
+        dt = time.perf_counter() - t0
+    return width * band / dt / 1e6, cores, f"{width}x{band} rows at 1 spp (a band of one sample pass)", dt
+
+
+def reference_scene(scene):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    return oracle.RefScene(scene)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    scene, cam, width, height, rkw = make_scene(args.workload)
+    # photon map is part of the reference render path when caustics are on
+    rkw = dict(rkw)
+    rkw.setdefault("photon_grid_min", (0, 0, 0))
+    rkw.setdefault("photon_grid_max", (0, 0, 0))
+    rates = []
+    cores = os.cpu_count() or 1
+    sample_desc = ""
+    ref = reference_scene(scene)
+    for step in range(args.warmup + args.steps):
+        rate, cores, sample_desc, _ = cpu_reference_rate(ref, cam, width, height, rkw,
+                                                          seconds_target=args.cpu_seconds)
+        if step >= args.warmup:
+            rates.append(rate)
+    value = statistics.median(rates)
+    line = {"metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": width * height / (value * 1e6) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": args.workload, "width": width, "height": height,
+                       "max_depth": rkw.get("max_depth")},
+            "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": cores, "kind": "reference",
+                             "sample": sample_desc},
+            "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="large_mesh", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import wfpt
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    t_setup = time.perf_counter()
+    scene, cam, width, height, rkw = make_scene(args.workload)
+    if rkw.get("caustics"):
+        rkw.setdefault("photon_grid_min", (0, 0, 0))  # min == max: grid bounds derived from the photons
+        rkw.setdefault("photon_grid_max", (0, 0, 0))
+    stream = torch.cuda.Stream()
+    dev_scene = wfpt.DeviceScene(scene)
+    cfg = wfpt.render_config(width, height, **rkw)
+    renderer = wfpt.Renderer(dev_scene, cam, cfg, stream=stream.cuda_stream)
+    setup_s = time.perf_counter() - t_setup
+    pixels = width * height
+    # Each rank owns the absolute sample range [rank * 2^20, ...).
+    base = rank << 20
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    renderer.set_sample_index(base)
+    for _ in range(args.warmup):
+        renderer.render_frame(1)
+    renderer.synchronize()
+    renderer.stats(reset=True)
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        renderer.render_frame(1)
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clock_record = clocks.stop()
+    ms = start.elapsed_time(end)
+    stats = renderer.stats(reset=True)
+    renderer.synchronize()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    seconds = ms / 1e3
+    value = world * pixels * args.steps / seconds / 1e6
+    mrays = (stats["extension_rays"] + stats["shadow_rays"]) / seconds / 1e6
+
+    # End to end through the C-ABI task call with host buffers.
+    host = torch.empty((height, width, 3), dtype=torch.float32, pin_memory=True)
+    lib = wfpt.library()
+    renderer.render_task((0, 0, width, height), base + 999_000, 1)
+    barrier()
+    torch.cuda.synchronize()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for i in range(args.steps):
+        wfpt.check(lib.wf_render(renderer.handle, 0, 0, width, height, base + 1000 + i, 1, 1))
+        wfpt.check(lib.wf_framebuffer_download(renderer.handle, 0, 0, width, height, host.data_ptr()))
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e_start.elapsed_time(e_end)
+    if world > 1:
+        t = torch.tensor([e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e2e_value = world * pixels * args.steps / (e_ms / 1e3) / 1e6
+
+    # Kernel-level roofline from one profiled pass (event-timed eager launches).
+    profile = renderer.profile_sample()
+    kernels = {k: v for k, v in profile.items() if isinstance(v, dict) and v["launches"]}
+    dominant = max(("trace", "shadow"), key=lambda k: kernels.get(k, {"ms": 0})["ms"])
+    total_ms = sum(v["ms"] for v in kernels.values())
+    launches = kernels[dominant]["launches"]
+    avg_ms = kernels[dominant]["ms"] / launches
+    bytes_per_launch = algorithmic_bytes(profile, dominant) / launches
+    peak, peak_kind = measured_peak()
+    achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": f"k_{dominant}", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": ncu_traffic(f"k_{dominant}", args.workload),
+                "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
+                "kernel_share": {k: v["ms"] / total_ms for k, v in kernels.items()}}
+
+    # Multi-GPU merge: one NCCL reduce of the framebuffers to rank 0.
+    if world > 1:
+        fb = torch.from_numpy(renderer.download()).cuda()
+        dist.reduce(fb, dst=0, op=dist.ReduceOp.SUM)
+        if rank == 0:
+            assert torch.isfinite(fb).all()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            ref = reference_scene(scene)
+            rate, cores, sample, _ = cpu_reference_rate(ref, cam, width, height, rkw,
+                                                        seconds_target=args.cpu_seconds)
+            ref.close()
+            cpu = {"value": rate, "unit": "Mpaths/s", "cores": cores, "kind": "reference", "sample": sample}
+        except FileNotFoundError as e:
+            cpu = {"value": None, "unit": "Mpaths/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": args.workload, "width": width, "height": height, "spp_per_step": 1,
+                       "max_depth": cfg.max_depth, "rr_start_depth": cfg.rr_start_depth,
+                       "triangles": int(scene.triangle_count()), "instances": int(len(scene.instances)),
+                       "photons": int(cfg.photon_count) if cfg.caustics else 0, "mode": "graph",
+                       "l2": "inputs larger than L2 (scene BVH + triangles > 1 GB)",
+                       "parallelism": f"sample-range x{world}"},
+            "mrays_per_s": mrays,
+            "rays_per_step": (stats["extension_rays"] + stats["shadow_rays"]) / args.steps,
+            "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 24,
+                    "d2h_bytes_per_step": pixels * 12},
+            "gpu_launches": int(args.steps * (2 + 4 * cfg.max_depth)),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clock_record,
+            "setup_seconds": setup_s,
+        }
+        print(json.dumps(line), flush=True)
+    renderer.close()
+    dev_scene.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -316,6 +316,25 @@ typedef struct wf_render_stats {
 /* Ray counters accumulated since creation or the last reset (synchronizes). */
 wf_status wf_render_stats_get(wf_renderer* renderer, wf_render_stats* stats, uint32_t reset);
 
+/* Kernel-level profile of one sample pass over the whole frame. */
+enum { WF_KERNEL_RAYGEN = 0, WF_KERNEL_TRACE = 1, WF_KERNEL_SHADE = 2, WF_KERNEL_SHADOW = 3,
+       WF_KERNEL_FINALIZE = 4, WF_KERNEL_PERSISTENT = 5, WF_KERNEL_KINDS = 6 };
+typedef struct wf_kernel_profile {
+    uint32_t launches[WF_KERNEL_KINDS];
+    float milliseconds[WF_KERNEL_KINDS];   /* summed CUDA-event durations */
+    uint64_t extension_rays;
+    uint64_t shadow_rays;
+    /* traversal work of the pass: closest-hit kernel, then shadow kernel */
+    uint64_t closest_nodes, closest_triangles, closest_spheres, closest_instances;
+    uint64_t any_nodes, any_triangles, any_spheres, any_instances;
+} wf_kernel_profile;
+/* Renders one more sample over all tiles with every kernel launched eagerly
+ * and bracketed by CUDA events on the renderer stream (the timing replay),
+ * then one more with counting traversal kernels (the work tally).  The two
+ * samples accumulate into the framebuffer and advance the sample index.
+ * Supplements the reference's --profile-queues record (render_driver.cu:393-400). */
+wf_status wf_profile_sample(wf_renderer* renderer, wf_kernel_profile* profile);
+
 /* Photon map (buildPhotonMap, render_driver.cu:180-234): number of photons
  * stored on diffuse surfaces after >= 1 specular bounce. */
 wf_status wf_photon_stats(wf_renderer* renderer, uint32_t* stored, uint32_t* emitted);

@@ -145,3 +145,96 @@ def environment_distribution(rgba, det=False):
     if rc != 0:
         raise ValueError("environment rejected")
     return p, ap, al
+
+
+# ---------------------------------------------------------------------------
+# The oracle's own CPU restatement (pt_oracle.cpp), pinned against the
+# host-compiled reference above.
+PORT_DIR = HERE / "_build"
+_port_libs = {}
+
+
+def port_available(det=False):
+    return (PORT_DIR / ("liboracle_det.so" if det else "liboracle.so")).exists()
+
+
+def port_lib(det=False):
+    key = bool(det)
+    if key not in _port_libs:
+        path = PORT_DIR / ("liboracle_det.so" if det else "liboracle.so")
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle port)")
+        lib = C.CDLL(str(path))
+        P, U32, I = C.c_void_p, C.c_uint32, C.c_int
+        lib.oracle_scene_create.restype = P
+        lib.oracle_scene_create.argtypes = [P, P]
+        lib.oracle_scene_destroy.argtypes = [P]
+        lib.oracle_light_count.restype = U32
+        lib.oracle_light_count.argtypes = [P]
+        lib.oracle_trace.argtypes = [P, P, U32, P]
+        lib.oracle_occluded.argtypes = [P, P, P, U32, P]
+        lib.oracle_photons.restype = U32
+        lib.oracle_photons.argtypes = [P, P, P]
+        lib.oracle_render.restype = I
+        lib.oracle_render.argtypes = [P, P, P, U32, U32, U32, U32, U32, U32, P, P, I]
+        _port_libs[key] = lib
+    return _port_libs[key]
+
+
+class PortScene:
+    """The CPU restatement's scene (det selects wf_math.h elementary functions)."""
+
+    def __init__(self, scene, det=False):
+        self.lib = port_lib(det)
+        d, keep = scene.desc()
+        env, rgba = scene.environment_struct()
+        self.handle = self.lib.oracle_scene_create(C.addressof(d), C.addressof(env) if env is not None else None)
+        del keep, rgba
+        if not self.handle:
+            raise RuntimeError("oracle scene creation failed")
+
+    def close(self):
+        if self.handle:
+            self.lib.oracle_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def light_count(self):
+        return self.lib.oracle_light_count(self.handle)
+
+    def trace(self, rays):
+        from wfpt import abi
+        rays = np.ascontiguousarray(rays, abi.RAY_DTYPE)
+        hits = np.zeros(len(rays), abi.HIT_DTYPE)
+        self.lib.oracle_trace(self.handle, rays.ctypes.data, len(rays), hits.ctypes.data)
+        return hits
+
+    def occluded(self, rays, max_distance):
+        from wfpt import abi
+        rays = np.ascontiguousarray(rays, abi.RAY_DTYPE)
+        md = np.ascontiguousarray(max_distance, np.float32)
+        out = np.zeros(len(rays), np.uint8)
+        self.lib.oracle_occluded(self.handle, rays.ctypes.data, md.ctypes.data, len(rays), out.ctypes.data)
+        return out
+
+    def photons(self, config):
+        rec = np.zeros((config.photon_count, 8), np.float32)
+        stored = self.lib.oracle_photons(self.handle, C.addressof(config), rec.ctypes.data)
+        return rec, stored
+
+    def render(self, camera, config, tile=None, sample_start=0, sample_count=1, threads=0):
+        from wfpt.native import camera_struct
+        cam = camera_struct(camera)
+        x, y, w, h = tile if tile is not None else (0, 0, config.width, config.height)
+        fb = np.zeros((h, w, 3), np.float32)
+        counts = np.zeros((sample_count, config.max_depth), np.uint32)
+        rc = self.lib.oracle_render(self.handle, C.addressof(cam), C.addressof(config), x, y, w, h, sample_start,
+                                    sample_count, fb.ctypes.data, counts.ctypes.data, threads)
+        if rc != 0:
+            raise RuntimeError("oracle render failed")
+        return fb, counts

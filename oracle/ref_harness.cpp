@@ -223,10 +223,15 @@ Material to_material(const wf_material& m) {
     return r;
 }
 
+}  // namespace
+struct RefPhotonMap;
+namespace {
 struct RefScene {
     DeviceScene device;
     uint32_t original_material_count = 0;
     bool probe = false;
+    std::shared_ptr<RefPhotonMap> photons;  // cached map (built once, like RenderDriver::prepare)
+    std::string photon_key;
 };
 }  // namespace
 
@@ -235,7 +240,8 @@ extern "C" {
 
 // probe != 0 builds the hit-identity probe copy: light registration off,
 // triangle lightIndex = identity code, instance lightOffset = index << 24,
-// material overrides dropped, one private material per sphere.
+// material overrides baked into per-instance mesh copies, one private
+// material per sphere.
 void* wfref_scene_create(const wf_scene_desc* d, const wf_environment* env, int probe) {
     try {
         HostScene h;
@@ -279,7 +285,20 @@ void* wfref_scene_create(const wf_scene_desc* d, const wf_environment* env, int 
             t.worldToLocalY = v3(in.world_to_local[1]);
             t.worldToLocalZ = v3(in.world_to_local[2]);
             t.translation = v3(in.translation);
-            SceneInstance si{in.mesh, t, probe ? invalidMaterialIndex : in.material_override,
+            uint32_t mesh = in.mesh;
+            uint32_t override_material = in.material_override;
+            if (probe && override_material != invalidMaterialIndex) {
+                // The override would hide the triangle's identity code
+                // (lightIndex is dropped for overridden instances): bake it
+                // into a private copy of the mesh instead.  Same positions,
+                // so the builder produces the same tree.
+                MeshAsset copy = h.meshes[in.mesh];
+                for (Triangle& tri : copy.triangles) tri.material = override_material;
+                mesh = uint32_t(h.meshes.size());
+                h.meshes.push_back(std::move(copy));
+                override_material = invalidMaterialIndex;
+            }
+            SceneInstance si{mesh, t, override_material,
                              in.accel == WF_ACCEL_DIRECT ? AccelerationMode::Direct : AccelerationMode::Bvh};
             h.instances.push_back(si);
         }
@@ -452,6 +471,30 @@ static RefPhotonMap* build_photons(Scene scene, const wf_render_config* c, int t
     map->grid.resolution = c->photon_grid_resolution;
     map->grid.minimum = v3(c->photon_grid_min);
     map->grid.maximum = v3(c->photon_grid_max);
+    bool derive = c->photon_grid_min[0] == c->photon_grid_max[0] && c->photon_grid_min[1] == c->photon_grid_max[1] &&
+                  c->photon_grid_min[2] == c->photon_grid_max[2];
+    if (derive) {
+        // The build's grid bounds are the bounding box of the stored photons
+        // (the reference hard-codes Cornell bounds, render_driver.cu:211-213);
+        // degenerate axes get unit extent.
+        Vec3 lo(INFINITY, INFINITY, INFINITY), hi(-INFINITY, -INFINITY, -INFINITY);
+        bool any = false;
+        for (const Photon& p : map->photons) {
+            if (!p.valid) continue;
+            any = true;
+            lo = Vec3(fminf(lo.x, p.position.x), fminf(lo.y, p.position.y), fminf(lo.z, p.position.z));
+            hi = Vec3(fmaxf(hi.x, p.position.x), fmaxf(hi.y, p.position.y), fmaxf(hi.z, p.position.z));
+        }
+        if (!any) {
+            lo = Vec3(-1, -1, -1);
+            hi = Vec3(1, 1, 1);
+        }
+        if (!(hi.x > lo.x)) hi.x = lo.x + 1.0f;
+        if (!(hi.y > lo.y)) hi.y = lo.y + 1.0f;
+        if (!(hi.z > lo.z)) hi.z = lo.z + 1.0f;
+        map->grid.minimum = lo;
+        map->grid.maximum = hi;
+    }
     size_t cells = size_t(c->photon_grid_resolution) * c->photon_grid_resolution * c->photon_grid_resolution;
     map->heads.assign(cells, 0xffffffffu);
     map->next.assign(n, 0xffffffffu);
@@ -519,11 +562,18 @@ int wfref_render(void* handle, const wf_camera* cam, const wf_render_config* c, 
         RngStrategy strategy = RngStrategy(c->rng);
         bool intersectionDebug = c->debug == WF_DEBUG_INTERSECTION;
         bool normalDebug = c->debug == WF_DEBUG_SHADING_NORMAL;
-        std::unique_ptr<RefPhotonMap> photons;
         PhotonGrid shadingGrid{};
         if (c->caustics && c->photon_count) {
-            photons.reset(build_photons(scene, c, threads));
-            shadingGrid = photons->grid;
+            char key[256];
+            std::snprintf(key, sizeof(key), "%u/%u/%u/%u/%u/%u/%a/%a/%a/%a/%a/%a", c->photon_count, c->photon_seed,
+                          c->photon_max_depth, c->photon_grid_resolution, c->rng, c->spectral,
+                          c->photon_grid_min[0], c->photon_grid_min[1], c->photon_grid_min[2],
+                          c->photon_grid_max[0], c->photon_grid_max[1], c->photon_grid_max[2]);
+            if (!r->photons || r->photon_key != key) {
+                r->photons.reset(build_photons(scene, c, threads));
+                r->photon_key = key;
+            }
+            shadingGrid = r->photons->grid;
             if (!c->caustic_gather) shadingGrid.heads = nullptr;
         }
         std::vector<uint32_t> counts(c->max_depth);

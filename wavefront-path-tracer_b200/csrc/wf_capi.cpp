@@ -275,6 +275,11 @@ wf_status wf_render_frame(wf_renderer* r, uint32_t sample_count) {
     return renderer_render_frame(r, sample_count);
 }
 
+wf_status wf_profile_sample(wf_renderer* r, wf_kernel_profile* profile) {
+    if (!r || !profile) return fail(WF_ERR_INVALID_ARG, "null argument");
+    return renderer_profile(r, profile);
+}
+
 wf_status wf_framebuffer_reset(wf_renderer* r) {
     if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
     size_t pixels = size_t(r->config.width) * r->config.height;

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 namespace wf {
 
@@ -101,8 +102,18 @@ __global__ void k_raygen(RenderParams rp, const TileDev* tile_ptr, Counters* c, 
     }
 }
 
+// Sums a thread's tally into per-launch totals (profiling pass only).
+WF_DEV void flush_tally(const CountTally& t, TallyTotals* totals) {
+    unsigned long long v[4] = {t.nodes, t.triangles, t.spheres, t.instances};
+    for (int k = 0; k < 4; ++k) {
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+        if ((threadIdx.x & 31) == 0 && v[k]) atomicAdd(&totals->v[k], v[k]);
+    }
+}
+
+template <typename Tally>
 __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
-                        uint32_t* hit_inst, Counters* c, uint32_t bounce) {
+                        uint32_t* hit_inst, Counters* c, uint32_t bounce, TallyTotals* totals) {
     uint32_t n = *count;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
@@ -110,14 +121,16 @@ __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const 
         if (bounce < kMaxBounces) c->profile[bounce] = n;
         c->extension_rays += n;
     }
+    Tally tally;
     for (uint32_t i = gid; i < n; i += gridDim.x * blockDim.x) {
         uint32_t p = queue[i];
         float4 o = ps.origin[p], d = ps.direction[p];
         TraceState h;
-        trace_closest(s, f4xyz(o), f4xyz(d), h);
+        trace_closest(s, f4xyz(o), f4xyz(d), h, tally);
         hit_a[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
         hit_inst[i] = h.inst;
     }
+    if constexpr (std::is_same<Tally, CountTally>::value) flush_tally(tally, totals);
 }
 
 __global__ void k_shade(DeviceScene s, RenderParams rp, PathSoA ps, const uint32_t* queue, const uint32_t* count,
@@ -151,15 +164,18 @@ __global__ void k_shade(DeviceScene s, RenderParams rp, PathSoA ps, const uint32
     }
 }
 
+template <typename Tally>
 __global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float4* shadow_dir, uint8_t* result,
-                         Counters* c, uint32_t capacity) {
+                         Counters* c, uint32_t capacity, TallyTotals* totals) {
     uint32_t n = min(c->shadow_count, capacity);
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) c->shadow_rays += n;
+    Tally tally;
     for (uint32_t j = gid; j < n; j += gridDim.x * blockDim.x) {
         float4 o = shadow_origin[j], d = shadow_dir[j];
-        result[j] = trace_any(s, f4xyz(o), f4xyz(d), o.w) ? 1 : 0;
+        result[j] = trace_any(s, f4xyz(o), f4xyz(d), o.w, tally) ? 1 : 0;
     }
+    if constexpr (std::is_same<Tally, CountTally>::value) flush_tally(tally, totals);
 }
 
 __global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* count, const float4* terms,
@@ -286,7 +302,8 @@ __global__ void __launch_bounds__(128) k_persistent(DeviceScene s, RenderParams 
                     p = cur[i];
                     Path path = load_path(ps, p);
                     TraceState h;
-                    trace_closest(s, path.origin, path.direction, h);
+                    NoTally tally;
+                    trace_closest(s, path.origin, path.direction, h, tally);
                     SurfaceHit sh;
                     bool did_hit = finish_hit(s, path.origin, path.direction, h.t, h.u, h.v, h.prim, h.inst, sh);
                     InlineSink sink;
@@ -328,7 +345,8 @@ __global__ void k_trace_batch(DeviceScene s, const wf_ray* rays, uint32_t count,
     V3 o{rays[i].origin[0], rays[i].origin[1], rays[i].origin[2]};
     V3 d{rays[i].direction[0], rays[i].direction[1], rays[i].direction[2]};
     TraceState h;
-    trace_closest(s, o, d, h);
+    NoTally tally;
+    trace_closest(s, o, d, h, tally);
     SurfaceHit sh;
     wf_hit out;
     memset(&out, 0, sizeof(out));
@@ -376,7 +394,8 @@ __global__ void k_any_batch(DeviceScene s, const wf_ray* rays, const float* max_
     if (i >= count) return;
     V3 o{rays[i].origin[0], rays[i].origin[1], rays[i].origin[2]};
     V3 d{rays[i].direction[0], rays[i].direction[1], rays[i].direction[2]};
-    occluded[i] = trace_any(s, o, d, max_distance[i]) ? 1 : 0;
+    NoTally tally;
+    occluded[i] = trace_any(s, o, d, max_distance[i], tally) ? 1 : 0;
 }
 
 // ------------------------------------------------------------------ photons
@@ -433,7 +452,8 @@ __global__ void k_trace_photons(DeviceScene s, uint32_t count, uint32_t max_dept
     V3 o = f4xyz(p0), d = f4xyz(p1);
     for (uint32_t depth = 0; depth < max_depth; ++depth) {
         TraceState h;
-        trace_closest(s, o, d, h);
+        NoTally tally;
+        trace_closest(s, o, d, h, tally);
         SurfaceHit hit;
         if (!finish_hit(s, o, d, h.t, h.u, h.v, h.prim, h.inst, hit)) return;
         if (hit.material >= s.material_count) return;
@@ -663,13 +683,13 @@ wf_status capture_graph(wf_renderer* r) {
         uint32_t cur = b & 1, nxt = cur ^ 1;
         uint32_t* cur_count = &r->counters->queue_count[cur];
         uint32_t* next_count = &r->counters->queue_count[nxt];
-        k_trace<<<grid_for(r, cap, r->block_trace), r->block_trace, 0, st>>>(
-            s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b);
+        k_trace<NoTally><<<grid_for(r, cap, r->block_trace), r->block_trace, 0, st>>>(
+            s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr);
         k_shade<<<grid_for(r, cap, r->block_shade), r->block_shade, 0, st>>>(
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
             r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count);
-        k_shadow<<<grid_for(r, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
-            s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity);
+        k_shadow<NoTally><<<grid_for(r, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
+            s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr);
         k_finalize<<<grid_for(r, cap, r->block_finalize), r->block_finalize, 0, st>>>(
             r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result, r->queue[nxt], next_count,
             cap, r->framebuffer);
@@ -865,6 +885,151 @@ wf_status renderer_render_frame(wf_renderer* r, uint32_t sample_count) {
             tile.advance_sample = t + 1 == tiles.size() ? 1u : 0u;
             if (wf_status e = launch_tile(r, tile)) return e;
         }
+    return WF_OK;
+}
+
+namespace {
+std::vector<TileDev> frame_tiles(const wf_render_config& c) {
+    uint32_t tw = c.tile_width && c.tile_height ? c.tile_width : c.width;
+    uint32_t th = c.tile_width && c.tile_height ? c.tile_height : c.height;
+    std::vector<TileDev> tiles;
+    for (uint32_t y = 0; y < c.height; y += th)
+        for (uint32_t x = 0; x < c.width; x += tw)
+            tiles.push_back(TileDev{x, y, std::min(tw, c.width - x), std::min(th, c.height - y), 0});
+    tiles.back().advance_sample = 1;
+    return tiles;
+}
+}  // namespace
+
+wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
+    std::memset(out, 0, sizeof(*out));
+    std::vector<TileDev> tiles = frame_tiles(r->config);
+    cudaStream_t st = r->stream;
+    cudaEvent_t e0, e1;
+    WF_CUDA(cudaEventCreate(&e0));
+    WF_CUDA(cudaEventCreate(&e1));
+    auto timed = [&](int kind, auto&& launch) -> wf_status {
+        WF_CUDA(cudaEventRecord(e0, st));
+        launch();
+        WF_CUDA(cudaGetLastError());
+        WF_CUDA(cudaEventRecord(e1, st));
+        WF_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        WF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        out->milliseconds[kind] += ms;
+        out->launches[kind] += 1;
+        return WF_OK;
+    };
+    unsigned long long before[2], after[2];
+    WF_CUDA(cudaMemcpy(before, &r->counters->extension_rays, sizeof(before), cudaMemcpyDeviceToHost));
+    if (r->config.mode == WF_MODE_PERSISTENT) {
+        for (const TileDev& tile : tiles) {
+            WF_CUDA(cudaMemcpyAsync(r->tile, &tile, sizeof(TileDev), cudaMemcpyHostToDevice, st));
+            WF_CUDA(cudaMemsetAsync(r->counters->persistent_count, 0, sizeof(uint32_t) * 2 * (kMaxBounces + 1), st));
+            WF_CUDA(cudaMemsetAsync(&r->counters->barrier_count, 0, sizeof(uint32_t), st));
+            DeviceScene s = r->scene->view;
+            RenderParams rp = r->params;
+            const TileDev* tp = r->tile;
+            Counters* c = r->counters;
+            PathSoA ps = r->paths;
+            uint32_t *q0 = r->queue[0], *q1 = r->queue[1];
+            uint32_t cap = r->capacity;
+            float* fb = r->framebuffer;
+            uint32_t chunk = r->chunk;
+            void* args[] = {&s, &rp, &tp, &c, &ps, &q0, &q1, &cap, &fb, &chunk};
+            cudaError_t launch_error = cudaSuccess;
+            if (wf_status e = timed(WF_KERNEL_PERSISTENT, [&] {
+                    launch_error = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_persistent),
+                                                               dim3(r->persistent_blocks),
+                                                               dim3(r->persistent_block_size), args, 0, st);
+                }))
+                return e;
+            WF_CUDA(launch_error);
+            k_advance<<<1, 1, 0, st>>>(r->counters, r->tile);
+        }
+    } else {
+        if (!r->tally) WF_CUDA(alloc(r, &r->tally, 2));
+        const DeviceScene& s = r->scene->view;
+        uint32_t cap = r->capacity;
+        for (int pass = 0; pass < 2; ++pass) {
+            bool count = pass == 1;
+            if (count) WF_CUDA(cudaMemsetAsync(r->tally, 0, 2 * sizeof(TallyTotals), st));
+            for (const TileDev& tile : tiles) {
+                WF_CUDA(cudaMemcpyAsync(r->tile, &tile, sizeof(TileDev), cudaMemcpyHostToDevice, st));
+                auto raygen = [&] {
+                    k_raygen<<<grid_for(r, cap, 256), 256, 0, st>>>(r->params, r->tile, r->counters, r->paths,
+                                                                     r->queue[0], cap);
+                };
+                if (count) raygen(); else if (wf_status e = timed(WF_KERNEL_RAYGEN, raygen)) return e;
+                for (uint32_t b = 0; b < r->config.max_depth; ++b) {
+                    uint32_t cur = b & 1, nxt = cur ^ 1;
+                    uint32_t* cur_count = &r->counters->queue_count[cur];
+                    uint32_t* next_count = &r->counters->queue_count[nxt];
+                    auto trace = [&] {
+                        if (count)
+                            k_trace<CountTally><<<grid_for(r, cap, r->block_trace), r->block_trace, 0, st>>>(
+                                s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
+                                r->tally);
+                        else
+                            k_trace<NoTally><<<grid_for(r, cap, r->block_trace), r->block_trace, 0, st>>>(
+                                s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
+                                nullptr);
+                    };
+                    auto shade = [&] {
+                        k_shade<<<grid_for(r, cap, r->block_shade), r->block_shade, 0, st>>>(
+                            s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms,
+                            r->shade_out, r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters,
+                            next_count);
+                    };
+                    auto shadow = [&] {
+                        if (count)
+                            k_shadow<CountTally><<<grid_for(r, r->shadow_capacity, r->block_trace), r->block_trace,
+                                                   0, st>>>(s, r->shadow_origin, r->shadow_dir, r->shadow_result,
+                                                            r->counters, r->shadow_capacity, r->tally + 1);
+                        else
+                            k_shadow<NoTally><<<grid_for(r, r->shadow_capacity, r->block_trace), r->block_trace, 0,
+                                                st>>>(s, r->shadow_origin, r->shadow_dir, r->shadow_result,
+                                                      r->counters, r->shadow_capacity, nullptr);
+                    };
+                    auto finalize = [&] {
+                        k_finalize<<<grid_for(r, cap, r->block_finalize), r->block_finalize, 0, st>>>(
+                            r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result,
+                            r->queue[nxt], next_count, cap, r->framebuffer);
+                    };
+                    if (count) {
+                        trace();
+                        shade();
+                        shadow();
+                        finalize();
+                    } else {
+                        if (wf_status e = timed(WF_KERNEL_TRACE, trace)) return e;
+                        if (wf_status e = timed(WF_KERNEL_SHADE, shade)) return e;
+                        if (wf_status e = timed(WF_KERNEL_SHADOW, shadow)) return e;
+                        if (wf_status e = timed(WF_KERNEL_FINALIZE, finalize)) return e;
+                    }
+                }
+                k_advance<<<1, 1, 0, st>>>(r->counters, r->tile);
+            }
+            if (!count) WF_CUDA(cudaMemcpy(after, &r->counters->extension_rays, sizeof(after), cudaMemcpyDeviceToHost));
+        }
+        TallyTotals t[2];
+        WF_CUDA(cudaMemcpy(t, r->tally, sizeof(t), cudaMemcpyDeviceToHost));
+        out->closest_nodes = t[0].v[0];
+        out->closest_triangles = t[0].v[1];
+        out->closest_spheres = t[0].v[2];
+        out->closest_instances = t[0].v[3];
+        out->any_nodes = t[1].v[0];
+        out->any_triangles = t[1].v[1];
+        out->any_spheres = t[1].v[2];
+        out->any_instances = t[1].v[3];
+    }
+    if (r->config.mode == WF_MODE_PERSISTENT)
+        WF_CUDA(cudaMemcpy(after, &r->counters->extension_rays, sizeof(after), cudaMemcpyDeviceToHost));
+    out->extension_rays = after[0] - before[0];
+    out->shadow_rays = after[1] - before[1];
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    WF_CUDA(cudaStreamSynchronize(st));
     return WF_OK;
 }
 

@@ -37,6 +37,12 @@ struct Counters {
     uint32_t persistent_work[kMaxBounces + 1];
 };
 
+// Traversal work totals of one profiling pass: node visits, triangle tests,
+// sphere tests, instance entries.
+struct TallyTotals {
+    unsigned long long v[4];
+};
+
 struct PathSoA {
     float4* origin;     // xyz, prev_pdf
     float4* direction;  // xyz, eta_scale
@@ -94,6 +100,7 @@ struct wf_renderer {
     std::mutex write_mutex;
     uint32_t latest_written = 0;
     uint32_t last_tile_width = 0, last_tile_height = 0;
+    wf::TallyTotals* tally = nullptr;  // [0] closest hit, [1] any hit (profiling pass)
 };
 
 namespace wf {
@@ -103,6 +110,7 @@ wf_status renderer_destroy(wf_renderer* r);
 wf_status renderer_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_start,
                           uint32_t sample_count, uint32_t clear);
 wf_status renderer_render_frame(wf_renderer* r, uint32_t sample_count);
+wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out);
 wf_status trace_closest_batch(const wf_scene* scene, const wf_ray* rays, uint32_t count, wf_hit* hits,
                               cudaStream_t stream);
 wf_status trace_any_batch(const wf_scene* scene, const wf_ray* rays, const float* max_distance, uint32_t count,

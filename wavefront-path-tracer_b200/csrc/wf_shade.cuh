@@ -491,7 +491,8 @@ struct InlineSink {
     // Returns a handle: 1 = occluded, 0 = visible.
     WF_DEV int request(V3 o, V3 d, float t_max) {
         ++requests;
-        return trace_any(*scene, o, d, t_max) ? 1 : 0;
+        NoTally tally;
+        return trace_any(*scene, o, d, t_max, tally) ? 1 : 0;
     }
     WF_DEV bool may_be_visible(int handle) const { return handle == kUnconditional || handle == 0; }
     WF_DEV void term(V3 c, int handle) {

@@ -20,6 +20,24 @@ namespace wf {
 
 constexpr int kStackSize = 64;  // leaf depth <= kMaxBvhDepth (60) < 64
 
+// Traversal work tallies.  NoTally compiles away; CountTally records the
+// node visits (one visit = one 64-byte node = two child boxes), triangle,
+// sphere and instance tests a traversal performs, for the algorithmic-byte
+// accounting of the profiling pass.
+struct NoTally {
+    WF_DEV void node() {}
+    WF_DEV void triangle() {}
+    WF_DEV void sphere() {}
+    WF_DEV void instance() {}
+};
+struct CountTally {
+    uint32_t nodes = 0, triangles = 0, spheres = 0, instances = 0;
+    WF_DEV void node() { ++nodes; }
+    WF_DEV void triangle() { ++triangles; }
+    WF_DEV void sphere() { ++spheres; }
+    WF_DEV void instance() { ++instances; }
+};
+
 struct TraceState {
     float t;          // closestT
     float u, v;
@@ -122,8 +140,9 @@ struct Stack {
 // Closest hit in one BVH over triangles (BLAS with a local ray, or the direct
 // list with the world ray).  intersectNexusBvh2, device_traversal.cuh:239-313.
 // kind/inst label accepted hits; override replaces the triangle material.
+template <typename Tally>
 WF_DEV void bvh_closest(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, TraceState& h,
-                        uint32_t kind, uint32_t inst, uint32_t material_override) {
+                        uint32_t kind, uint32_t inst, uint32_t material_override, Tally& tally) {
     V3 inv = inverse_direction(d);
     float near_t;
     if (bvh.root == kNoRoot || !slab_box(o, inv, bvh.box, h.t, near_t)) return;
@@ -133,6 +152,7 @@ WF_DEV void bvh_closest(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, Tra
     for (;;) {
         if (ref < 0) {
             uint32_t ti = uint32_t(~ref);
+            tally.triangle();
             TriVerts tri = load_triangle(s, ti);
             float t, u, v;
             if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < h.t) {
@@ -146,6 +166,7 @@ WF_DEV void bvh_closest(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, Tra
                 }
             }
         } else {
+            tally.node();
             const BvhNode* node = &s.nodes[ref];
             float4 lxy = __ldg(&node->lxy);
             float4 rxy = __ldg(&node->rxy);
@@ -177,8 +198,9 @@ WF_DEV void bvh_closest(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, Tra
 }
 
 // Any hit with t < t_max in one triangle BVH.
+template <typename Tally>
 WF_DEV bool bvh_any(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, float t_max,
-                    uint32_t material_override) {
+                    uint32_t material_override, Tally& tally) {
     V3 inv = inverse_direction(d);
     float near_t;
     if (bvh.root == kNoRoot || !slab_box(o, inv, bvh.box, t_max, near_t)) return false;
@@ -188,6 +210,7 @@ WF_DEV bool bvh_any(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, float t
     for (;;) {
         if (ref < 0) {
             uint32_t ti = uint32_t(~ref);
+            tally.triangle();
             TriVerts tri = load_triangle(s, ti);
             float t, u, v;
             if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < t_max) {
@@ -195,6 +218,7 @@ WF_DEV bool bvh_any(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, float t
                 if (!alpha_rejects(s, m)) return true;
             }
         } else {
+            tally.node();
             const BvhNode* node = &s.nodes[ref];
             float4 lxy = __ldg(&node->lxy);
             float4 rxy = __ldg(&node->rxy);
@@ -240,10 +264,12 @@ WF_DEV Instance load_instance(const DeviceScene& s, uint32_t i) {
 
 // Linear scan of a mesh in original triangle order (intersectMeshInstance
 // with useBvh = false, device_traversal.cuh:814-821).
+template <typename Tally>
 WF_DEV void mesh_linear_closest(const DeviceScene& s, const Blas& b, V3 o, V3 d, TraceState& h,
-                                uint32_t inst, uint32_t material_override) {
+                                uint32_t inst, uint32_t material_override, Tally& tally) {
     for (uint32_t i = 0; i < b.count; ++i) {
         uint32_t ti = s.mesh_linear[b.first_linear + i];
+        tally.triangle();
         TriVerts tri = load_triangle(s, ti);
         float t, u, v;
         if (!intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
@@ -259,27 +285,32 @@ WF_DEV void mesh_linear_closest(const DeviceScene& s, const Blas& b, V3 o, V3 d,
 
 // intersectMeshInstance, device_traversal.cuh:802-834 (attribute transforms
 // are deferred to finish_hit).
-WF_DEV void instance_closest(const DeviceScene& s, uint32_t inst, V3 o, V3 d, TraceState& h, bool use_bvh) {
+template <typename Tally>
+WF_DEV void instance_closest(const DeviceScene& s, uint32_t inst, V3 o, V3 d, TraceState& h, bool use_bvh, Tally& tally) {
+    tally.instance();
     Instance in = load_instance(s, inst);
     Blas b = s.blases[in.blas];
     V3 lo = to_local_vector(in, o - instance_translation(in));
     V3 ld = to_local_vector(in, d);
     float previous = h.t;
     if (use_bvh && b.bvh.root != kNoRoot)
-        bvh_closest(s, b.bvh, lo, ld, h, kHitMesh, inst, in.material_override);
+        bvh_closest(s, b.bvh, lo, ld, h, kHitMesh, inst, in.material_override, tally);
     else
-        mesh_linear_closest(s, b, lo, ld, h, inst, in.material_override);
+        mesh_linear_closest(s, b, lo, ld, h, inst, in.material_override, tally);
     if (h.t >= previous) return;
     h.sphere = kInvalid;
 }
 
-WF_DEV bool instance_any(const DeviceScene& s, uint32_t inst, V3 o, V3 d, float t_max, bool use_bvh) {
+template <typename Tally>
+WF_DEV bool instance_any(const DeviceScene& s, uint32_t inst, V3 o, V3 d, float t_max, bool use_bvh, Tally& tally) {
+    tally.instance();
     Instance in = load_instance(s, inst);
     Blas b = s.blases[in.blas];
     V3 lo = to_local_vector(in, o - instance_translation(in));
     V3 ld = to_local_vector(in, d);
-    if (use_bvh && b.bvh.root != kNoRoot) return bvh_any(s, b.bvh, lo, ld, t_max, in.material_override);
+    if (use_bvh && b.bvh.root != kNoRoot) return bvh_any(s, b.bvh, lo, ld, t_max, in.material_override, tally);
     for (uint32_t i = 0; i < b.count; ++i) {
+        tally.triangle();
         TriVerts tri = load_triangle(s, s.mesh_linear[b.first_linear + i]);
         float t, u, v;
         if (!intersect_triangle(lo, ld, tri.v0, tri.v1, tri.v2, t, u, v) || t >= t_max) continue;
@@ -290,8 +321,10 @@ WF_DEV bool instance_any(const DeviceScene& s, uint32_t inst, V3 o, V3 d, float 
 }
 
 // intersectSphereHit, device_traversal.cuh:789-800.
-WF_DEV void sphere_closest(const DeviceScene& s, uint32_t index, V3 o, V3 d, TraceState& h) {
+template <typename Tally>
+WF_DEV void sphere_closest(const DeviceScene& s, uint32_t index, V3 o, V3 d, TraceState& h, Tally& tally) {
     float t;
+    tally.sphere();
     if (!intersect_sphere(o, d, __ldg(&s.spheres[index]), t) || t > h.t) return;
     if (t == h.t && index >= h.sphere) return;
     h.t = t;
@@ -300,7 +333,8 @@ WF_DEV void sphere_closest(const DeviceScene& s, uint32_t index, V3 o, V3 d, Tra
 }
 
 // intersectSceneTlas, device_traversal.cuh:836-878.
-WF_DEV void tlas_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h) {
+template <typename Tally>
+WF_DEV void tlas_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h, Tally& tally) {
     if (s.tlas.root == kNoRoot) return;
     V3 inv = inverse_direction(d);
     float near_t;
@@ -312,10 +346,11 @@ WF_DEV void tlas_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h) {
         if (ref < 0) {
             uint32_t leaf = __ldg(&s.tlas_leaves[~ref]);
             if (leaf & 0x80000000u)
-                sphere_closest(s, leaf & 0x7fffffffu, o, d, h);
+                sphere_closest(s, leaf & 0x7fffffffu, o, d, h, tally);
             else
-                instance_closest(s, leaf, o, d, h, true);
+                instance_closest(s, leaf, o, d, h, true, tally);
         } else {
+            tally.node();
             const BvhNode* node = &s.nodes[ref];
             float4 lxy = __ldg(&node->lxy);
             float4 rxy = __ldg(&node->rxy);
@@ -346,7 +381,8 @@ WF_DEV void tlas_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h) {
     }
 }
 
-WF_DEV bool tlas_any(const DeviceScene& s, V3 o, V3 d, float t_max) {
+template <typename Tally>
+WF_DEV bool tlas_any(const DeviceScene& s, V3 o, V3 d, float t_max, Tally& tally) {
     if (s.tlas.root == kNoRoot) return false;
     V3 inv = inverse_direction(d);
     float near_t;
@@ -359,11 +395,13 @@ WF_DEV bool tlas_any(const DeviceScene& s, V3 o, V3 d, float t_max) {
             uint32_t leaf = __ldg(&s.tlas_leaves[~ref]);
             if (leaf & 0x80000000u) {
                 float t;
+                tally.sphere();
                 if (intersect_sphere(o, d, __ldg(&s.spheres[leaf & 0x7fffffffu]), t) && t < t_max) return true;
-            } else if (instance_any(s, leaf, o, d, t_max, true)) {
+            } else if (instance_any(s, leaf, o, d, t_max, true, tally)) {
                 return true;
             }
         } else {
+            tally.node();
             const BvhNode* node = &s.nodes[ref];
             float4 lxy = __ldg(&node->lxy);
             float4 rxy = __ldg(&node->rxy);
@@ -387,12 +425,14 @@ WF_DEV bool tlas_any(const DeviceScene& s, V3 o, V3 d, float t_max) {
 }
 
 // traceRay, device_traversal.cuh:1115-1150 (visit order and sphere reset rules).
-WF_DEV void trace_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h) {
+template <typename Tally>
+WF_DEV void trace_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h, Tally& tally) {
     trace_state_init(h, 1e30f);
-    for (uint32_t i = 0; i < s.direct_sphere_count; ++i) sphere_closest(s, s.direct_spheres[i], o, d, h);
-    for (uint32_t i = 0; i < s.direct_instance_count; ++i) instance_closest(s, s.direct_instances[i], o, d, h, false);
+    for (uint32_t i = 0; i < s.direct_sphere_count; ++i) sphere_closest(s, s.direct_spheres[i], o, d, h, tally);
+    for (uint32_t i = 0; i < s.direct_instance_count; ++i) instance_closest(s, s.direct_instances[i], o, d, h, false, tally);
     for (uint32_t i = 0; i < s.static_count; ++i) {
         uint32_t ti = s.static_first + i;
+        tally.triangle();
         TriVerts tri = load_triangle(s, ti);
         float t, u, v;
         if (!intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
@@ -404,14 +444,15 @@ WF_DEV void trace_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h) {
         h.inst = kInvalid;
         h.sphere = kInvalid;
     }
-    tlas_closest(s, o, d, h);
+    tlas_closest(s, o, d, h, tally);
     if (s.direct_count > 0) {
         float previous = h.t;
         if (s.direct_bvh.root != kNoRoot) {
-            bvh_closest(s, s.direct_bvh, o, d, h, kHitTriangle, kInvalid, kInvalid);
+            bvh_closest(s, s.direct_bvh, o, d, h, kHitTriangle, kInvalid, kInvalid, tally);
         } else {
             for (uint32_t i = 0; i < s.direct_count; ++i) {
                 uint32_t ti = s.direct_first + i;
+                tally.triangle();
                 TriVerts tri = load_triangle(s, ti);
                 float t, u, v;
                 if (!intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
@@ -429,24 +470,28 @@ WF_DEV void trace_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h) {
 
 // isOccluded, device_traversal.cuh:1035-1113.  A pure disjunction of
 // independent tests, so an early return at the first hit gives the same bit.
-WF_DEV bool trace_any(const DeviceScene& s, V3 o, V3 d, float t_max) {
+template <typename Tally>
+WF_DEV bool trace_any(const DeviceScene& s, V3 o, V3 d, float t_max, Tally& tally) {
     for (uint32_t i = 0; i < s.direct_sphere_count; ++i) {
         float t;
+        tally.sphere();
         if (intersect_sphere(o, d, __ldg(&s.spheres[s.direct_spheres[i]]), t) && t < t_max) return true;
     }
     for (uint32_t i = 0; i < s.direct_instance_count; ++i)
-        if (instance_any(s, s.direct_instances[i], o, d, t_max, false)) return true;
+        if (instance_any(s, s.direct_instances[i], o, d, t_max, false, tally)) return true;
     for (uint32_t i = 0; i < s.static_count; ++i) {
+        tally.triangle();
         TriVerts tri = load_triangle(s, s.static_first + i);
         float t, u, v;
         if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < t_max &&
             !alpha_rejects(s, tri.material))
             return true;
     }
-    if (tlas_any(s, o, d, t_max)) return true;
+    if (tlas_any(s, o, d, t_max, tally)) return true;
     if (s.direct_count > 0) {
-        if (s.direct_bvh.root != kNoRoot) return bvh_any(s, s.direct_bvh, o, d, t_max, kInvalid);
+        if (s.direct_bvh.root != kNoRoot) return bvh_any(s, s.direct_bvh, o, d, t_max, kInvalid, tally);
         for (uint32_t i = 0; i < s.direct_count; ++i) {
+            tally.triangle();
             TriVerts tri = load_triangle(s, s.direct_first + i);
             float t, u, v;
             if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < t_max &&

@@ -109,6 +109,18 @@ class RenderConfig(C.Structure):
     ]
 
 
+KERNEL_NAMES = ["raygen", "trace", "shade", "shadow", "finalize", "persistent"]
+
+
+class KernelProfile(C.Structure):
+    _fields_ = [("launches", C.c_uint32 * 6), ("milliseconds", C.c_float * 6),
+                ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("closest_nodes", C.c_uint64), ("closest_triangles", C.c_uint64),
+                ("closest_spheres", C.c_uint64), ("closest_instances", C.c_uint64),
+                ("any_nodes", C.c_uint64), ("any_triangles", C.c_uint64),
+                ("any_spheres", C.c_uint64), ("any_instances", C.c_uint64)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("paths", C.c_uint64)]
 
@@ -140,6 +152,7 @@ def declare(lib):
         "wf_synchronize": (S, [P]),
         "wf_queue_counts": (S, [P, P, U32]),
         "wf_render_stats_get": (S, [P, C.POINTER(RenderStats), U32]),
+        "wf_profile_sample": (S, [P, C.POINTER(KernelProfile)]),
         "wf_photon_stats": (S, [P, C.POINTER(U32), C.POINTER(U32)]),
         "wf_photons_download": (S, [P, P, U32]),
         "wf_checkpoint_save": (S, [P, C.c_char_p, U64]),

@@ -292,6 +292,16 @@ class Renderer:
         check(library().wf_render_stats_get(self.handle, C.byref(s), int(reset)))
         return {"extension_rays": s.extension_rays, "shadow_rays": s.shadow_rays, "paths": s.paths}
 
+    def profile_sample(self):
+        """wf_profile_sample: per-kernel event times and traversal tallies of
+        one extra sample pass (accumulates into the framebuffer)."""
+        p = abi.KernelProfile()
+        check(library().wf_profile_sample(self.handle, C.byref(p)))
+        out = {name: {"launches": p.launches[i], "ms": p.milliseconds[i]} for i, name in enumerate(abi.KERNEL_NAMES)}
+        for f, _ in abi.KernelProfile._fields_[2:]:
+            out[f] = getattr(p, f)
+        return out
+
     def photon_stats(self):
         stored, emitted = C.c_uint32(), C.c_uint32()
         check(library().wf_photon_stats(self.handle, C.byref(stored), C.byref(emitted)))

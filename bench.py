@@ -329,6 +329,7 @@ def main():
                     "d2h_bytes_per_step": pixels * 12},
             "gpu_launches": int(args.steps * (2 + 4 * cfg.max_depth)),
             "roofline": roofline,
+            "profile_pass": {k: (v if not isinstance(v, dict) else v) for k, v in profile.items()},
             "cpu_baseline": cpu,
             "clocks": clock_record,
             "setup_seconds": setup_s,

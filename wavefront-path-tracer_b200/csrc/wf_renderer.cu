@@ -92,6 +92,7 @@ __global__ void k_raygen(RenderParams rp, const TileDev* tile_ptr, Counters* c, 
     if (gid == 0) {
         c->queue_count[0] = n;
         c->paths += n;
+        c->work_trace = 0;
     }
     for (uint32_t lp = gid; lp < n; lp += gridDim.x * blockDim.x) {
         Path path;
@@ -100,6 +101,16 @@ __global__ void k_raygen(RenderParams rp, const TileDev* tile_ptr, Counters* c, 
         ps.radiance[lp] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         queue[lp] = lp;
     }
+}
+
+// Warps pull 32-entry chunks from `counter` until `n` is exhausted (the
+// counter is zeroed by the kernel that runs before).  Balances warps whose
+// rays need very different traversal work.
+WF_DEV bool next_chunk(uint32_t* counter, uint32_t n, uint32_t& base) {
+    uint32_t b = 0;
+    if ((threadIdx.x & 31) == 0) b = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, b, 0);
+    return base < n;
 }
 
 // Sums a thread's tally into per-launch totals (profiling pass only).
@@ -118,11 +129,15 @@ __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const 
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
         c->shadow_count = 0;
+        c->work_shade = 0;
         if (bounce < kMaxBounces) c->profile[bounce] = n;
         c->extension_rays += n;
     }
     Tally tally;
-    for (uint32_t i = gid; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t base;
+    while (next_chunk(&c->work_trace, n, base)) {
+        uint32_t i = base + (threadIdx.x & 31);
+        if (i >= n) continue;
         uint32_t p = queue[i];
         float4 o = ps.origin[p], d = ps.direction[p];
         TraceState h;
@@ -139,8 +154,14 @@ __global__ void k_shade(DeviceScene s, RenderParams rp, PathSoA ps, const uint32
                         uint32_t* next_count) {
     uint32_t n = *count;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid == 0) *next_count = 0;
-    for (uint32_t i = gid; i < n; i += gridDim.x * blockDim.x) {
+    if (gid == 0) {
+        *next_count = 0;
+        c->work_shadow = 0;
+    }
+    uint32_t base;
+    while (next_chunk(&c->work_shade, n, base)) {
+        uint32_t i = base + (threadIdx.x & 31);
+        if (i >= n) continue;
         uint32_t p = queue[i];
         Path path = load_path(ps, p);
         float4 ha = hit_a[i];
@@ -171,7 +192,10 @@ __global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) c->shadow_rays += n;
     Tally tally;
-    for (uint32_t j = gid; j < n; j += gridDim.x * blockDim.x) {
+    uint32_t base;
+    while (next_chunk(&c->work_shadow, n, base)) {
+        uint32_t j = base + (threadIdx.x & 31);
+        if (j >= n) continue;
         float4 o = shadow_origin[j], d = shadow_dir[j];
         result[j] = trace_any(s, f4xyz(o), f4xyz(d), o.w, tally) ? 1 : 0;
     }
@@ -180,11 +204,12 @@ __global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float
 
 __global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* count, const float4* terms,
                            const int4* shade_out, const uint8_t* shadow_result, uint32_t* next, uint32_t* next_count,
-                           uint32_t capacity, float* framebuffer) {
+                           uint32_t capacity, float* framebuffer, uint32_t* work_trace) {
     uint32_t n = *count;
     uint32_t lane = threadIdx.x & 31;
     uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *work_trace = 0;
     for (uint32_t base = warp * 32; base < n; base += warps * 32) {
         uint32_t i = base + lane;
         bool alive = false;
@@ -692,7 +717,7 @@ wf_status capture_graph(wf_renderer* r) {
             s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr);
         k_finalize<<<grid_for(r, cap, r->block_finalize), r->block_finalize, 0, st>>>(
             r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result, r->queue[nxt], next_count,
-            cap, r->framebuffer);
+            cap, r->framebuffer, &r->counters->work_trace);
     }
     k_advance<<<1, 1, 0, st>>>(r->counters, r->tile);
     cudaError_t e = cudaStreamEndCapture(st, &r->graph);
@@ -994,13 +1019,17 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                     auto finalize = [&] {
                         k_finalize<<<grid_for(r, cap, r->block_finalize), r->block_finalize, 0, st>>>(
                             r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result,
-                            r->queue[nxt], next_count, cap, r->framebuffer);
+                            r->queue[nxt], next_count, cap, r->framebuffer, &r->counters->work_trace);
                     };
                     if (count) {
                         trace();
+                        WF_CUDA(cudaGetLastError());
                         shade();
+                        WF_CUDA(cudaGetLastError());
                         shadow();
+                        WF_CUDA(cudaGetLastError());
                         finalize();
+                        WF_CUDA(cudaGetLastError());
                     } else {
                         if (wf_status e = timed(WF_KERNEL_TRACE, trace)) return e;
                         if (wf_status e = timed(WF_KERNEL_SHADE, shade)) return e;

@@ -29,6 +29,10 @@ struct Counters {
     uint32_t error;          // persistent-kernel barrier timeout
     uint32_t barrier_count;
     uint32_t barrier_generation;
+    uint32_t work_trace;   // dynamic work counters (32-entry chunks per warp)
+    uint32_t work_shade;
+    uint32_t work_shadow;
+    uint32_t work_pad;
     unsigned long long extension_rays;
     unsigned long long shadow_rays;
     unsigned long long paths;

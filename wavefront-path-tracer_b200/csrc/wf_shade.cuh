@@ -703,6 +703,17 @@ WF_DEV void add_environment_or_sky(const DeviceScene& s, const RenderParams& rp,
 // cells list their photons in the order the reference's serial insertion
 // produces (descending photon index).
 WF_DEV V3 gather_caustics(const PhotonGridView& g, const ShadeHit& hit, float radius) {
+    // Every stored photon lies inside [minimum, maximum] (the grid drops the
+    // others), so a point farther than the search radius from that box finds
+    // no candidate: the reference then returns zero (nearestCount == 0) after
+    // scanning the clamped border cells.  Return it directly.
+    {
+        float sr = fmaxf(radius * 4.0f, 0.1f) * 1.001f;  // margin keeps the test strict after rounding
+        float dx = fmaxf(fmaxf(g.minimum.x - hit.position.x, hit.position.x - g.maximum.x), 0.0f);
+        float dy = fmaxf(fmaxf(g.minimum.y - hit.position.y, hit.position.y - g.maximum.y), 0.0f);
+        float dz = fmaxf(fmaxf(g.minimum.z - hit.position.z, hit.position.z - g.maximum.z), 0.0f);
+        if (dx > sr || dy > sr || dz > sr) return V3{0, 0, 0};
+    }
     V3 extent = g.maximum - g.minimum;
     V3 offset = hit.position - g.minimum;
     V3 nrm{offset.x / extent.x, offset.y / extent.y, offset.z / extent.z};
@@ -727,6 +738,22 @@ WF_DEV V3 gather_caustics(const PhotonGridView& g, const ShadeHit& hit, float ra
         for (int y = cy - cell_radius; y <= cy + cell_radius; ++y)
             for (int x = cx - cell_radius; x <= cx + cell_radius; ++x) {
                 if (x < 0 || y < 0 || z < 0 || x >= res || y >= res || z >= res) continue;
+                // A cell whose box (padded by a rounding margin) lies beyond the
+                // search radius holds no photon the distance test accepts, so
+                // skipping it leaves the accepted sequence unchanged.
+                {
+                    float cx0 = g.minimum.x + extent.x * (float(x) / float(res));
+                    float cx1 = g.minimum.x + extent.x * (float(x + 1) / float(res));
+                    float cy0 = g.minimum.y + extent.y * (float(y) / float(res));
+                    float cy1 = g.minimum.y + extent.y * (float(y + 1) / float(res));
+                    float cz0 = g.minimum.z + extent.z * (float(z) / float(res));
+                    float cz1 = g.minimum.z + extent.z * (float(z + 1) / float(res));
+                    float gx = fmaxf(fmaxf(cx0 - hit.position.x, hit.position.x - cx1), 0.0f);
+                    float gy = fmaxf(fmaxf(cy0 - hit.position.y, hit.position.y - cy1), 0.0f);
+                    float gz = fmaxf(fmaxf(cz0 - hit.position.z, hit.position.z - cz1), 0.0f);
+                    float cell_margin = search_radius * 1.001f + 1.0e-4f * (fabsf(extent.x) + fabsf(extent.y) + fabsf(extent.z));
+                    if (gx > cell_margin || gy > cell_margin || gz > cell_margin) continue;
+                }
                 uint32_t cell = (uint32_t(z) * g.resolution + uint32_t(y)) * g.resolution + uint32_t(x);
                 uint32_t begin = g.cell_start[cell], end = begin + g.cell_count[cell];
                 for (uint32_t p = begin; p < end; ++p) {

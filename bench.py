@@ -7,8 +7,10 @@ log-uniform in [1, 50]), 500 instances of a 200,000-triangle displaced
 geodesic sphere, 20 glass spheres, a 2048x1024 HDR sun-and-sky environment
 with MIS, and a 2M-photon caustic map.  Synthetic and seeded (no dataset).
 
-One step = one sample per pixel over the full frame (2,073,600 paths)
-through the captured-graph wavefront.  `value` = Mpaths/s over the timed
+One step = `spp` samples per pixel over the full frame (2,073,600 paths
+per sample) through the streaming wavefront (one captured graph per step
+whose device-side loop regenerates finished paths with their pixel's next
+sample; --mode graph replays the reference's per-sample graph instead).  `value` = Mpaths/s over the timed
 steps with the scene resident in HBM; `e2e` = the same metric through the
 C-ABI task call (RenderTaskRenderer::render semantics: task in from the host,
 unnormalized radiance sums back to pinned host memory every step).
@@ -38,9 +40,17 @@ WORKLOADS = {
     "large_mesh_small": (dict(width=480, height=270, terrain_quads=256, instance_count=50, instance_frequency=30,
                               glass_spheres=6, env_size=(512, 256)),
                          dict(max_depth=12, caustics=1, photon_count=200_000)),
+    # profiling-sized variant of large_mesh (about 1 GB on the device, still
+    # larger than L2): 2.1M-triangle terrain, the same 500 instances
+    "large_mesh_medium": (dict(width=960, height=540, terrain_quads=1024),
+                          dict(max_depth=12, caustics=1, photon_count=500_000)),
     "sphere_field": (dict(width=1280, height=720), dict(max_depth=16)),
     "cornell": (dict(width=256, height=256), dict(max_depth=8, rr_start_depth=3)),
 }
+# Samples per pixel that one step renders (the streaming mode overlaps the
+# tail bounces of these samples).
+SPP_PER_STEP = {"large_mesh": 4, "large_mesh_medium": 1, "large_mesh_small": 4, "sphere_field": 4, "cornell": 16}
+MODES = {"graph": 0, "persistent": 1, "stream": 2}
 HBM_FALLBACK_GBS = 6650.0
 
 
@@ -196,6 +206,8 @@ def main():
     ap.add_argument("--workload", default="large_mesh", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--mode", default="stream", choices=sorted(MODES))
+    ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: per workload)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -220,9 +232,13 @@ def main():
         rkw.setdefault("photon_grid_max", (0, 0, 0))
     stream = torch.cuda.Stream()
     dev_scene = wfpt.DeviceScene(scene)
-    cfg = wfpt.render_config(width, height, **rkw)
+    cfg = wfpt.render_config(width, height, mode=MODES[args.mode], **rkw)
+    spp = args.spp or SPP_PER_STEP[args.workload]
     renderer = wfpt.Renderer(dev_scene, cam, cfg, stream=stream.cuda_stream)
     setup_s = time.perf_counter() - t_setup
+    scene_bytes = dev_scene.info().device_bytes
+    # path state (6 x 16 B), queues, hit records, terms and shadow requests per slot
+    renderer_bytes = width * height * (96 + 8 + 20 + 16 * 8 + 16 + 5 * 33 + 12)
     pixels = width * height
     # Each rank owns the absolute sample range [rank * 2^20, ...).
     base = rank << 20
@@ -233,7 +249,7 @@ def main():
 
     renderer.set_sample_index(base)
     for _ in range(args.warmup):
-        renderer.render_frame(1)
+        renderer.render_frame(spp)
     renderer.synchronize()
     renderer.stats(reset=True)
     barrier()
@@ -242,7 +258,7 @@ def main():
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
     for _ in range(args.steps):
-        renderer.render_frame(1)
+        renderer.render_frame(spp)
     end.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -255,19 +271,19 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     seconds = ms / 1e3
-    value = world * pixels * args.steps / seconds / 1e6
+    value = world * pixels * spp * args.steps / seconds / 1e6
     mrays = (stats["extension_rays"] + stats["shadow_rays"]) / seconds / 1e6
 
     # End to end through the C-ABI task call with host buffers.
     host = torch.empty((height, width, 3), dtype=torch.float32, pin_memory=True)
     lib = wfpt.library()
-    renderer.render_task((0, 0, width, height), base + 999_000, 1)
+    renderer.render_task((0, 0, width, height), base + 999_000, spp)
     barrier()
     torch.cuda.synchronize()
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_start.record(stream)
     for i in range(args.steps):
-        wfpt.check(lib.wf_render(renderer.handle, 0, 0, width, height, base + 1000 + i, 1, 1))
+        wfpt.check(lib.wf_render(renderer.handle, 0, 0, width, height, base + 1000 + i * spp, spp, 1))
         wfpt.check(lib.wf_framebuffer_download(renderer.handle, 0, 0, width, height, host.data_ptr()))
     e_end.record(stream)
     torch.cuda.synchronize()
@@ -276,7 +292,7 @@ def main():
         t = torch.tensor([e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e_ms = float(t.item())
-    e2e_value = world * pixels * args.steps / (e_ms / 1e3) / 1e6
+    e2e_value = world * pixels * spp * args.steps / (e_ms / 1e3) / 1e6
 
     # Kernel-level roofline from one profiled pass (event-timed eager launches).
     profile = renderer.profile_sample()
@@ -317,17 +333,21 @@ def main():
             "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-            "config": {"workload": args.workload, "width": width, "height": height, "spp_per_step": 1,
+            "config": {"workload": args.workload, "width": width, "height": height, "spp_per_step": spp,
                        "max_depth": cfg.max_depth, "rr_start_depth": cfg.rr_start_depth,
                        "triangles": int(scene.triangle_count()), "instances": int(len(scene.instances)),
-                       "photons": int(cfg.photon_count) if cfg.caustics else 0, "mode": "graph",
-                       "l2": "inputs larger than L2 (scene BVH + triangles > 1 GB)",
+                       "photons": int(cfg.photon_count) if cfg.caustics else 0, "mode": args.mode,
+                       "scene_device_bytes": int(scene_bytes),
+                       "l2": ("inputs larger than L2 (scene + path state on the device: "
+                              f"{(scene_bytes + renderer_bytes) / 1e6:.0f} MB, no flush)"
+                              if scene_bytes + renderer_bytes > 126e6 else
+                              "working set fits in the 126 MB L2; no flush between steps"),
                        "parallelism": f"sample-range x{world}"},
             "mrays_per_s": mrays,
             "rays_per_step": (stats["extension_rays"] + stats["shadow_rays"]) / args.steps,
             "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 24,
                     "d2h_bytes_per_step": pixels * 12},
-            "gpu_launches": int(args.steps * (2 + 4 * cfg.max_depth)),
+            "gpu_launches": int(stats["kernel_launches"]),
             "roofline": roofline,
             "profile_pass": {k: (v if not isinstance(v, dict) else v) for k, v in profile.items()},
             "cpu_baseline": cpu,

@@ -229,7 +229,15 @@ typedef struct wf_camera {
     float aspect_ratio;
 } wf_camera;
 
-enum { WF_MODE_GRAPH = 0, WF_MODE_PERSISTENT = 1 };
+/* GRAPH: the reference's captured wavefront, one graph replay per tile and
+ * sample (render_driver.cu:264-352).  PERSISTENT: one cooperative launch per
+ * tile and sample (renderer.cu:55-125).  STREAM: one graph replay per tile
+ * covers the whole sample range; a slot whose path ends starts the same
+ * pixel's next sample in the same loop iteration (a device-side while loop,
+ * so the short tail bounces of many samples share launches).  Each pixel
+ * still adds its samples to the framebuffer one after another in sample
+ * order, so the three modes give bit-identical framebuffers. */
+enum { WF_MODE_GRAPH = 0, WF_MODE_PERSISTENT = 1, WF_MODE_STREAM = 2 };
 enum { WF_RNG_XORSHIFT32 = 0, WF_RNG_PCG32 = 1 };
 enum { WF_DEBUG_NONE = 0, WF_DEBUG_INTERSECTION = 1, WF_DEBUG_SHADING_NORMAL = 2 };
 
@@ -259,6 +267,8 @@ typedef struct wf_render_config {
     uint32_t photon_seed;
     uint32_t spectral;
     uint32_t profile_queues;   /* record per-bounce queue counts */
+    uint32_t refill_threshold; /* trace/shadow kernels: a warp fetches new rays once this many of its
+                                  lanes are idle (1..32; 0 = default 8) */
 } wf_render_config;
 
 /* Defaults of RenderConfig (config.hpp:11-41) at the given resolution. */
@@ -312,6 +322,7 @@ typedef struct wf_render_stats {
     uint64_t extension_rays;
     uint64_t shadow_rays;
     uint64_t paths;
+    uint64_t kernel_launches;  /* render-kernel launches that ran (device-counted) */
 } wf_render_stats;
 /* Ray counters accumulated since creation or the last reset (synchronizes). */
 wf_status wf_render_stats_get(wf_renderer* renderer, wf_render_stats* stats, uint32_t reset);
@@ -319,6 +330,7 @@ wf_status wf_render_stats_get(wf_renderer* renderer, wf_render_stats* stats, uin
 /* Kernel-level profile of one sample pass over the whole frame. */
 enum { WF_KERNEL_RAYGEN = 0, WF_KERNEL_TRACE = 1, WF_KERNEL_SHADE = 2, WF_KERNEL_SHADOW = 3,
        WF_KERNEL_FINALIZE = 4, WF_KERNEL_PERSISTENT = 5, WF_KERNEL_KINDS = 6 };
+enum { WF_PROFILE_BOUNCES = 32 };
 typedef struct wf_kernel_profile {
     uint32_t launches[WF_KERNEL_KINDS];
     float milliseconds[WF_KERNEL_KINDS];   /* summed CUDA-event durations */
@@ -327,6 +339,12 @@ typedef struct wf_kernel_profile {
     /* traversal work of the pass: closest-hit kernel, then shadow kernel */
     uint64_t closest_nodes, closest_triangles, closest_spheres, closest_instances;
     uint64_t any_nodes, any_triangles, any_spheres, any_instances;
+    /* graph mode, per bounce of the timing replay summed over tiles: event
+     * times of trace, shade, shadow and finalize, extension rays traced and
+     * shadow rays requested (bounces >= WF_PROFILE_BOUNCES are not split) */
+    float bounce_milliseconds[4][WF_PROFILE_BOUNCES];
+    uint32_t bounce_extension_rays[WF_PROFILE_BOUNCES];
+    uint32_t bounce_shadow_rays[WF_PROFILE_BOUNCES];
 } wf_kernel_profile;
 /* Renders one more sample over all tiles with every kernel launched eagerly
  * and bracketed by CUDA events on the renderer stream (the timing replay),

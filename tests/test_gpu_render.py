@@ -60,6 +60,43 @@ def test_framebuffer_bit_exact(cuda, name, mode):
     assert got.mean() > 0
 
 
+@pytest.mark.parametrize("name", list(WORKLOADS))
+def test_stream_mode_bit_exact(cuda, name):
+    """Streaming mode (slot regeneration inside a graph WHILE loop) gives the
+    reference's framebuffer sums bit for bit, and the same ray totals as the
+    per-sample graph."""
+    got, _, stats, want, want_counts, _ = render_both(name, abi.MODE_STREAM)
+    diff = np.nonzero(got.view(np.uint32) != want.view(np.uint32))
+    assert diff[0].size == 0, f"{diff[0].size} channels differ"
+    assert stats["extension_rays"] == int(want_counts.sum())
+    _, _, graph_stats, _, _, _ = render_both(name, abi.MODE_GRAPH)
+    for k in ("extension_rays", "shadow_rays", "paths"):
+        assert stats[k] == graph_stats[k], k
+    assert 0 < stats["kernel_launches"] <= graph_stats["kernel_launches"]
+
+
+def test_stream_mode_tiles_and_long_ranges(cuda):
+    """Tile-major frames, split ranges and a 16-sample range in streaming mode
+    match the per-sample graph."""
+    scene, cam = scenes.cornell_box(64, 64)
+    frames = {}
+    for mode in (abi.MODE_GRAPH, abi.MODE_STREAM):
+        cfg = wfpt.render_config(64, 64, max_depth=8, rr_start_depth=3, tile_width=32, tile_height=32, mode=mode)
+        dev = wfpt.DeviceScene(scene)
+        r = wfpt.Renderer(dev, cam, cfg)
+        r.reset()
+        r.render_frame(5)
+        assert r.sample_index() == 5
+        frame = r.download()
+        r.render(0, 32, 32, 32, 7, 2, True)
+        r.render(0, 32, 32, 32, 9, 14, False)
+        split = r.download(0, 32, 32, 32)
+        r.close()
+        frames[mode] = (frame, split)
+    for a, b in zip(frames[abi.MODE_GRAPH], frames[abi.MODE_STREAM]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
 def test_ray_counters(cuda):
     got, counts, stats, want, want_counts, (_, _, _, spp) = render_both("cornell", abi.MODE_GRAPH)
     assert stats["extension_rays"] == int(want_counts.sum())

@@ -310,6 +310,8 @@ wf_status wf_synchronize(wf_renderer* r) {
     uint32_t flags[2] = {0, 0};
     WF_CUDA(cudaMemcpy(flags, &r->counters->overflow, sizeof(flags) / 2, cudaMemcpyDeviceToHost));
     WF_CUDA(cudaMemcpy(&flags[1], &r->counters->error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (flags[1] == wf::kErrorStreamBound)
+        return fail(WF_ERR_TIMEOUT, "streaming loop exceeded samples x max_depth iterations");
     if (flags[1]) return fail(WF_ERR_TIMEOUT, "persistent kernel grid barrier timed out");
     if (flags[0]) return fail(WF_ERR_CAPACITY, "shadow queue or term buffer overflow (flags %u)", flags[0]);
     return WF_OK;
@@ -341,12 +343,13 @@ wf_status wf_queue_counts(wf_renderer* r, uint32_t* counts, uint32_t n) {
 
 wf_status wf_render_stats_get(wf_renderer* r, wf_render_stats* stats, uint32_t reset) {
     if (!r || !stats) return fail(WF_ERR_INVALID_ARG, "null argument");
-    unsigned long long v[3];
+    unsigned long long v[4];
     WF_CUDA(cudaMemcpyAsync(v, &r->counters->extension_rays, sizeof(v), cudaMemcpyDeviceToHost, r->stream));
     WF_CUDA(cudaStreamSynchronize(r->stream));
     stats->extension_rays = v[0];
     stats->shadow_rays = v[1];
     stats->paths = v[2];
+    stats->kernel_launches = v[3];
     if (reset) {
         WF_CUDA(cudaMemsetAsync(&r->counters->extension_rays, 0, sizeof(v), r->stream));
         WF_CUDA(cudaStreamSynchronize(r->stream));

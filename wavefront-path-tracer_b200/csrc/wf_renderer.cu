@@ -16,6 +16,7 @@
 // a bounded grid barrier between bounces.
 #include "wf_renderer.h"
 #include "wf_shade.cuh"
+#include "wf_lane_traverse.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -34,6 +35,12 @@ wf_status cuda_fail(cudaError_t e, const char* what) {
     } while (0)
 
 namespace {
+
+// Device-side launch count of the render kernels (kernels on one stream run
+// in order, so thread 0 of CTA 0 updates it without an atomic).
+WF_DEV void count_launch(Counters* c) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) ++c->kernel_launches;
+}
 
 WF_DEV Path load_path(const PathSoA& ps, uint32_t p) {
     float4 o = ps.origin[p], d = ps.direction[p], t = ps.throughput[p];
@@ -85,6 +92,7 @@ WF_DEV void init_path(const RenderParams& rp, const TileDev& tile, uint32_t samp
 
 __global__ void k_raygen(RenderParams rp, const TileDev* tile_ptr, Counters* c, PathSoA ps, uint32_t* queue,
                          uint32_t capacity) {
+    count_launch(c);
     TileDev tile = *tile_ptr;
     uint32_t n = min(tile.width * tile.height, capacity);
     uint32_t sample = c->sample_index;
@@ -99,6 +107,31 @@ __global__ void k_raygen(RenderParams rp, const TileDev* tile_ptr, Counters* c, 
         init_path(rp, tile, sample, lp, path);
         store_path(ps, lp, path);
         ps.radiance[lp] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        queue[lp] = lp;
+    }
+}
+
+// Streaming mode: every slot (= pixel of the tile) starts the launch's first
+// sample; slot_sample counts the samples a slot has started.
+__global__ void k_raygen_stream(RenderParams rp, const TileDev* tile_ptr, Counters* c, PathSoA ps, uint32_t* queue,
+                                uint32_t capacity) {
+    count_launch(c);
+    TileDev tile = *tile_ptr;
+    uint32_t n = min(tile.width * tile.height, capacity);
+    uint32_t sample = c->sample_index;
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) {
+        c->queue_count[0] = n;
+        c->paths += uint64_t(n) * tile.samples;
+        c->work_trace = 0;
+        c->stream_iterations = 0;
+    }
+    for (uint32_t lp = gid; lp < n; lp += gridDim.x * blockDim.x) {
+        Path path;
+        init_path(rp, tile, sample, lp, path);
+        store_path(ps, lp, path);
+        ps.radiance[lp] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        ps.slot_sample[lp] = 0;
         queue[lp] = lp;
     }
 }
@@ -124,7 +157,8 @@ WF_DEV void flush_tally(const CountTally& t, TallyTotals* totals) {
 
 template <typename Tally>
 __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
-                        uint32_t* hit_inst, Counters* c, uint32_t bounce, TallyTotals* totals) {
+                        uint32_t* hit_inst, Counters* c, uint32_t bounce, TallyTotals* totals, uint32_t refill_at) {
+    count_launch(c);
     uint32_t n = *count;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
@@ -134,16 +168,35 @@ __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const 
         c->extension_rays += n;
     }
     Tally tally;
-    uint32_t base;
-    while (next_chunk(&c->work_trace, n, base)) {
-        uint32_t i = base + (threadIdx.x & 31);
-        if (i >= n) continue;
-        uint32_t p = queue[i];
-        float4 o = ps.origin[p], d = ps.direction[p];
-        TraceState h;
-        trace_closest(s, f4xyz(o), f4xyz(d), h, tally);
-        hit_a[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
-        hit_inst[i] = h.inst;
+    ClosestLane L;
+    L.stage = kStageDone;
+    uint32_t i = 0;
+    bool more = true;
+    for (;;) {
+        bool idle = L.stage == kStageDone;
+        uint32_t slot = refill(&c->work_trace, n, idle, refill_at, more);
+        if (slot != kInvalid) {
+            i = slot;
+            uint32_t p = queue[i];
+            float4 o = ps.origin[p], d = ps.direction[p];
+            closest_begin(L, s, f4xyz(o), f4xyz(d), tally);
+            if (L.stage == kStageDone) {
+                hit_a[i] = make_float4(L.h.t, L.h.u, L.h.v, __uint_as_float(L.h.prim));
+                hit_inst[i] = L.h.inst;
+            }
+        }
+        bool busy = L.stage != kStageDone;
+        if (!__any_sync(0xffffffffu, busy)) {
+            if (!more) break;
+            continue;
+        }
+        if (busy) {
+            closest_step(L, s, tally);
+            if (L.stage == kStageDone) {
+                hit_a[i] = make_float4(L.h.t, L.h.u, L.h.v, __uint_as_float(L.h.prim));
+                hit_inst[i] = L.h.inst;
+            }
+        }
     }
     if constexpr (std::is_same<Tally, CountTally>::value) flush_tally(tally, totals);
 }
@@ -152,6 +205,7 @@ __global__ void k_shade(DeviceScene s, RenderParams rp, PathSoA ps, const uint32
                         const float4* hit_a, const uint32_t* hit_inst, float4* terms, int4* shade_out,
                         float4* shadow_origin, float4* shadow_dir, uint32_t shadow_capacity, Counters* c,
                         uint32_t* next_count) {
+    count_launch(c);
     uint32_t n = *count;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
@@ -187,24 +241,50 @@ __global__ void k_shade(DeviceScene s, RenderParams rp, PathSoA ps, const uint32
 
 template <typename Tally>
 __global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float4* shadow_dir, uint8_t* result,
-                         Counters* c, uint32_t capacity, TallyTotals* totals) {
+                         Counters* c, uint32_t capacity, TallyTotals* totals, uint32_t refill_at) {
+    count_launch(c);
     uint32_t n = min(c->shadow_count, capacity);
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) c->shadow_rays += n;
     Tally tally;
-    uint32_t base;
-    while (next_chunk(&c->work_shadow, n, base)) {
-        uint32_t j = base + (threadIdx.x & 31);
-        if (j >= n) continue;
-        float4 o = shadow_origin[j], d = shadow_dir[j];
-        result[j] = trace_any(s, f4xyz(o), f4xyz(d), o.w, tally) ? 1 : 0;
+    AnyLane L;
+    L.stage = kStageDone;
+    uint32_t j = 0;
+    bool more = true;
+    for (;;) {
+        bool idle = L.stage == kStageDone;
+        uint32_t slot = refill(&c->work_shadow, n, idle, refill_at, more);
+        if (slot != kInvalid) {
+            j = slot;
+            float4 o = shadow_origin[j], d = shadow_dir[j];
+            any_begin(L, s, f4xyz(o), f4xyz(d), o.w, tally);
+            if (L.stage == kStageDone) result[j] = L.hit ? 1 : 0;
+        }
+        bool busy = L.stage != kStageDone;
+        if (!__any_sync(0xffffffffu, busy)) {
+            if (!more) break;
+            continue;
+        }
+        if (busy) {
+            any_step(L, s, tally);
+            if (L.stage == kStageDone) result[j] = L.hit ? 1 : 0;
+        }
     }
     if constexpr (std::is_same<Tally, CountTally>::value) flush_tally(tally, totals);
 }
 
+// Adds each path's accepted terms in emission order, applies the kill rule,
+// adds ended paths to the framebuffer and compacts survivors into `next`
+// (appendWarpCompacted, queue_compaction.cuh:8-29).  With kRegenerate (the
+// streaming mode) an ended path's slot starts its pixel's next sample, which
+// joins `next` like a survivor; the framebuffer add comes first, so every
+// pixel still accumulates its samples in sample order.
+template <bool kRegenerate>
 __global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* count, const float4* terms,
                            const int4* shade_out, const uint8_t* shadow_result, uint32_t* next, uint32_t* next_count,
-                           uint32_t capacity, float* framebuffer, uint32_t* work_trace) {
+                           uint32_t capacity, float* framebuffer, uint32_t* work_trace, RenderParams rp,
+                           const TileDev* tile_ptr, Counters* c) {
+    count_launch(c);
     uint32_t n = *count;
     uint32_t lane = threadIdx.x & 31;
     uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -233,6 +313,18 @@ __global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* co
                 f[0] += rad.x;
                 f[1] += rad.y;
                 f[2] += rad.z;
+                if constexpr (kRegenerate) {
+                    TileDev tile = *tile_ptr;
+                    uint32_t started = ps.slot_sample[p] + 1;
+                    if (started < tile.samples) {
+                        Path path;
+                        init_path(rp, tile, c->sample_index + started, p, path);
+                        store_path(ps, p, path);
+                        ps.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        ps.slot_sample[p] = started;
+                        alive = true;
+                    }
+                }
             }
         }
         unsigned mask = __ballot_sync(0xffffffffu, alive);
@@ -244,8 +336,26 @@ __global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* co
     }
 }
 
+// Streaming loop condition: run the body again while paths remain.  Each
+// body pass advances every live path by two bounces, and a slot runs at most
+// samples * max_depth bounces, so a loop that exceeds that bound records an
+// error and stops instead of spinning.
+__global__ void k_stream_condition(cudaGraphConditionalHandle handle, Counters* c, const TileDev* tile,
+                                   uint32_t max_depth) {
+    count_launch(c);
+    uint32_t it = ++c->stream_iterations;
+    bool live = c->queue_count[0] > 0;
+    uint64_t bound = (uint64_t(tile->samples) * max_depth + 1) / 2 + 1;
+    if (live && it >= bound) {
+        c->error = kErrorStreamBound;
+        live = false;
+    }
+    cudaGraphSetConditional(handle, live ? 1u : 0u);
+}
+
 __global__ void k_advance(Counters* c, const TileDev* tile) {
-    if (tile->advance_sample) ++c->sample_index;
+    count_launch(c);
+    if (tile->advance_sample) c->sample_index += tile->samples;
 }
 
 // Grid barrier with a bounded wait.  All blocks are co-resident (cooperative
@@ -267,7 +377,7 @@ WF_DEV bool grid_barrier(Counters* c, uint32_t blocks) {
             while (*gen == g) {
                 if (*(volatile uint32_t*)&c->error) break;
                 if (clock64() - start > (1ll << 31)) {
-                    atomicExch(&c->error, 1u);
+                    atomicExch(&c->error, kErrorBarrierTimeout);
                     break;
                 }
                 __nanosleep(32);
@@ -282,6 +392,7 @@ WF_DEV bool grid_barrier(Counters* c, uint32_t blocks) {
 __global__ void __launch_bounds__(128) k_persistent(DeviceScene s, RenderParams rp, const TileDev* tile_ptr,
                                                     Counters* c, PathSoA ps, uint32_t* q0, uint32_t* q1,
                                                     uint32_t capacity, float* framebuffer, uint32_t chunk_warps) {
+    count_launch(c);
     TileDev tile = *tile_ptr;
     uint32_t n0 = min(tile.width * tile.height, capacity);
     uint32_t sample = c->sample_index;
@@ -611,6 +722,22 @@ uint32_t grid_for(const wf_renderer* r, uint32_t work, uint32_t block) {
     return std::max(1u, std::min(g, r->grid_cap));
 }
 
+// Bounce kernels fetch work dynamically (per-warp chunks or a grid-stride
+// loop), so one full wave of resident CTAs covers any queue; a larger grid
+// only adds CTAs that find nothing to do.
+uint32_t grid(const wf_renderer* r, int kernel, uint32_t work, uint32_t block) {
+    uint32_t g = grid_for(r, work, block);
+    return r->grid_resident[kernel] ? std::min(g, r->grid_resident[kernel]) : g;
+}
+
+template <typename K>
+cudaError_t resident_grid(wf_renderer* r, int kernel, K* fn, uint32_t block) {
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, int(block), 0);
+    if (e == cudaSuccess) r->grid_resident[kernel] = uint32_t(std::max(per_sm, 1)) * uint32_t(r->sm_count);
+    return e;
+}
+
 wf_status build_photon_map(wf_renderer* r) {
     const wf_render_config& c = r->config;
     const DeviceScene& s = r->scene->view;
@@ -708,16 +835,16 @@ wf_status capture_graph(wf_renderer* r) {
         uint32_t cur = b & 1, nxt = cur ^ 1;
         uint32_t* cur_count = &r->counters->queue_count[cur];
         uint32_t* next_count = &r->counters->queue_count[nxt];
-        k_trace<NoTally><<<grid_for(r, cap, r->block_trace), r->block_trace, 0, st>>>(
-            s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr);
-        k_shade<<<grid_for(r, cap, r->block_shade), r->block_shade, 0, st>>>(
+        k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
+            s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill);
+        k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
             r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count);
-        k_shadow<NoTally><<<grid_for(r, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
-            s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr);
-        k_finalize<<<grid_for(r, cap, r->block_finalize), r->block_finalize, 0, st>>>(
+        k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
+            s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr, r->refill);
+        k_finalize<false><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
             r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result, r->queue[nxt], next_count,
-            cap, r->framebuffer, &r->counters->work_trace);
+            cap, r->framebuffer, &r->counters->work_trace, r->params, r->tile, r->counters);
     }
     k_advance<<<1, 1, 0, st>>>(r->counters, r->tile);
     cudaError_t e = cudaStreamEndCapture(st, &r->graph);
@@ -726,11 +853,71 @@ wf_status capture_graph(wf_renderer* r) {
     return WF_OK;
 }
 
+// Streaming graph: raygen, then a device-side WHILE node whose body runs two
+// bounces (queue 0 -> 1 -> 0) and re-arms itself while queue 0 is non-empty,
+// then the sample-index advance.  Built with cudaStreamBeginCaptureToGraph
+// into the parent graph and the conditional node's body graph.
+wf_status capture_stream_graph(wf_renderer* r) {
+    const DeviceScene& s = r->scene->view;
+    cudaStream_t st = r->stream;
+    uint32_t cap = r->capacity;
+    WF_CUDA(cudaGraphCreate(&r->graph, 0));
+    WF_CUDA(cudaStreamBeginCaptureToGraph(st, r->graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    k_raygen_stream<<<grid_for(r, cap, 256), 256, 0, st>>>(r->params, r->tile, r->counters, r->paths, r->queue[0],
+                                                            cap);
+    cudaGraph_t captured = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &captured);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (stream prologue)");
+    size_t nodes = 0;
+    WF_CUDA(cudaGraphGetNodes(r->graph, nullptr, &nodes));
+    if (nodes != 1) return fail(WF_ERR_CUDA, "unexpected streaming prologue graph (%zu nodes)", nodes);
+    cudaGraphNode_t raygen_node = nullptr;
+    WF_CUDA(cudaGraphGetNodes(r->graph, &raygen_node, &nodes));
+
+    cudaGraphConditionalHandle handle;
+    WF_CUDA(cudaGraphConditionalHandleCreate(&handle, r->graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t loop_node = nullptr;
+    WF_CUDA(cudaGraphAddNode(&loop_node, r->graph, &raygen_node, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+
+    WF_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    for (uint32_t cur = 0; cur < 2; ++cur) {
+        uint32_t nxt = cur ^ 1;
+        uint32_t* cur_count = &r->counters->queue_count[cur];
+        uint32_t* next_count = &r->counters->queue_count[nxt];
+        k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
+            s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, kMaxBounces, nullptr, r->refill);
+        k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
+            s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
+            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count);
+        k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
+            s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr, r->refill);
+        k_finalize<true><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
+            r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result, r->queue[nxt], next_count,
+            cap, r->framebuffer, &r->counters->work_trace, r->params, r->tile, r->counters);
+    }
+    k_stream_condition<<<1, 1, 0, st>>>(handle, r->counters, r->tile, r->config.max_depth);
+    e = cudaStreamEndCapture(st, &captured);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (stream body)");
+
+    WF_CUDA(cudaStreamBeginCaptureToGraph(st, r->graph, &loop_node, nullptr, 1, cudaStreamCaptureModeThreadLocal));
+    k_advance<<<1, 1, 0, st>>>(r->counters, r->tile);
+    e = cudaStreamEndCapture(st, &captured);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (stream epilogue)");
+    WF_CUDA(cudaGraphInstantiate(&r->graph_exec, r->graph, 0));
+    return WF_OK;
+}
+
 wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
     WF_CUDA(cudaMemcpyAsync(r->tile, &tile, sizeof(TileDev), cudaMemcpyHostToDevice, r->stream));
     r->last_tile_width = tile.width;
     r->last_tile_height = tile.height;
-    if (r->config.mode == WF_MODE_GRAPH) {
+    if (r->config.mode != WF_MODE_PERSISTENT) {
         WF_CUDA(cudaGraphLaunch(r->graph_exec, r->stream));
         return WF_OK;
     }
@@ -767,7 +954,7 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
     if (c.max_depth == 0) return fail(WF_ERR_INVALID_ARG, "maximum depth must be greater than zero");
     if (c.max_depth > kMaxBounces) return fail(WF_ERR_INVALID_ARG, "maximum depth above %d", kMaxBounces);
     if (c.block_size > 1024) return fail(WF_ERR_INVALID_ARG, "CUDA block size must be between 1 and 1024");
-    if (c.mode > WF_MODE_PERSISTENT || c.rng > WF_RNG_PCG32 || c.debug > WF_DEBUG_SHADING_NORMAL)
+    if (c.mode > WF_MODE_STREAM || c.rng > WF_RNG_PCG32 || c.debug > WF_DEBUG_SHADING_NORMAL)
         return fail(WF_ERR_INVALID_ARG, "unknown mode, rng strategy or debug view");
     if (c.caustics && c.photon_count == 0)
         return fail(WF_ERR_INVALID_ARG, "Photon count must be greater than zero when caustics are enabled");
@@ -787,6 +974,8 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
     WF_CUDA(cudaDeviceGetAttribute(&r->sm_count, cudaDevAttrMultiProcessorCount, r->device));
     r->grid_cap = uint32_t(r->sm_count) * 64;
     if (c.block_size) r->block_trace = r->block_shade = c.block_size;
+    if (c.refill_threshold > 32) return fail(WF_ERR_INVALID_ARG, "refill threshold must be between 0 and 32");
+    r->refill = c.refill_threshold ? c.refill_threshold : 8u;
     if (stream) {
         r->stream = static_cast<cudaStream_t>(stream);
     } else {
@@ -825,7 +1014,7 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
     WF_CUDA(alloc(rr, &r->framebuffer, size_t(pixels) * 3));
     WF_CUDA(cudaMemsetAsync(r->counters, 0, sizeof(Counters), r->stream));
     WF_CUDA(cudaMemsetAsync(r->framebuffer, 0, sizeof(float) * 3 * size_t(pixels), r->stream));
-    if (c.mode == WF_MODE_GRAPH) {
+    if (c.mode != WF_MODE_PERSISTENT) {
         uint32_t requests_per_path = 5u + scene->view.directional_count;
         uint64_t shadow = uint64_t(cap) * requests_per_path;
         if (shadow > 0xffffffffull) shadow = 0xffffffffull;
@@ -837,6 +1026,11 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
         WF_CUDA(alloc(rr, &r->shadow_origin, r->shadow_capacity));
         WF_CUDA(alloc(rr, &r->shadow_dir, r->shadow_capacity));
         WF_CUDA(alloc(rr, &r->shadow_result, r->shadow_capacity));
+        if (c.mode == WF_MODE_STREAM) WF_CUDA(alloc(rr, &r->paths.slot_sample, cap));
+        WF_CUDA(resident_grid(rr, 0, k_trace<NoTally>, r->block_trace));
+        WF_CUDA(resident_grid(rr, 1, k_shade, r->block_shade));
+        WF_CUDA(resident_grid(rr, 2, k_shadow<NoTally>, r->block_trace));
+        WF_CUDA(resident_grid(rr, 3, k_finalize<true>, r->block_finalize));
     } else {
         int cooperative = 0;
         WF_CUDA(cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, r->device));
@@ -855,6 +1049,8 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
     }
     if (c.mode == WF_MODE_GRAPH) {
         if (wf_status e = capture_graph(rr)) return e;
+    } else if (c.mode == WF_MODE_STREAM) {
+        if (wf_status e = capture_stream_graph(rr)) return e;
     }
     WF_CUDA(cudaStreamSynchronize(r->stream));
     *out = r.release();
@@ -891,6 +1087,10 @@ wf_status renderer_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, ui
     WF_CUDA(cudaMemcpyAsync(&r->counters->sample_index, &sample_start, sizeof(uint32_t), cudaMemcpyHostToDevice,
                             r->stream));
     TileDev tile{x, y, w, h, 1};
+    if (c.mode == WF_MODE_STREAM) {
+        tile.samples = sample_count;
+        return launch_tile(r, tile);
+    }
     for (uint32_t s = 0; s < sample_count; ++s)
         if (wf_status e = launch_tile(r, tile)) return e;
     return WF_OK;
@@ -904,6 +1104,17 @@ wf_status renderer_render_frame(wf_renderer* r, uint32_t sample_count) {
     for (uint32_t y = 0; y < c.height; y += th)
         for (uint32_t x = 0; x < c.width; x += tw)
             tiles.push_back(TileDev{x, y, std::min(tw, c.width - x), std::min(th, c.height - y), 0});
+    if (c.mode == WF_MODE_STREAM) {
+        // Tile-major: each tile takes the whole sample range in one launch;
+        // every pixel belongs to one tile, so its sample order is unchanged.
+        for (size_t t = 0; t < tiles.size(); ++t) {
+            TileDev tile = tiles[t];
+            tile.samples = sample_count;
+            tile.advance_sample = t + 1 == tiles.size() ? 1u : 0u;
+            if (wf_status e = launch_tile(r, tile)) return e;
+        }
+        return WF_OK;
+    }
     for (uint32_t s = 0; s < sample_count; ++s)
         for (size_t t = 0; t < tiles.size(); ++t) {
             TileDev tile = tiles[t];
@@ -933,20 +1144,28 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
     cudaEvent_t e0, e1;
     WF_CUDA(cudaEventCreate(&e0));
     WF_CUDA(cudaEventCreate(&e1));
+    float last_ms = 0.0f;
     auto timed = [&](int kind, auto&& launch) -> wf_status {
         WF_CUDA(cudaEventRecord(e0, st));
         launch();
         WF_CUDA(cudaGetLastError());
         WF_CUDA(cudaEventRecord(e1, st));
         WF_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.0f;
-        WF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        out->milliseconds[kind] += ms;
+        last_ms = 0.0f;
+        WF_CUDA(cudaEventElapsedTime(&last_ms, e0, e1));
+        out->milliseconds[kind] += last_ms;
         out->launches[kind] += 1;
         return WF_OK;
     };
+    // Every read goes through the renderer stream: it may be a non-blocking
+    // stream, which a plain cudaMemcpy on the legacy stream does not wait for.
+    auto read_back = [&](void* dst, const void* src, size_t bytes) -> wf_status {
+        WF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+        WF_CUDA(cudaStreamSynchronize(st));
+        return WF_OK;
+    };
     unsigned long long before[2], after[2];
-    WF_CUDA(cudaMemcpy(before, &r->counters->extension_rays, sizeof(before), cudaMemcpyDeviceToHost));
+    if (wf_status e = read_back(before, &r->counters->extension_rays, sizeof(before))) return e;
     if (r->config.mode == WF_MODE_PERSISTENT) {
         for (const TileDev& tile : tiles) {
             WF_CUDA(cudaMemcpyAsync(r->tile, &tile, sizeof(TileDev), cudaMemcpyHostToDevice, st));
@@ -992,34 +1211,35 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                     uint32_t* next_count = &r->counters->queue_count[nxt];
                     auto trace = [&] {
                         if (count)
-                            k_trace<CountTally><<<grid_for(r, cap, r->block_trace), r->block_trace, 0, st>>>(
+                            k_trace<CountTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
-                                r->tally);
+                                r->tally, r->refill);
                         else
-                            k_trace<NoTally><<<grid_for(r, cap, r->block_trace), r->block_trace, 0, st>>>(
+                            k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
-                                nullptr);
+                                nullptr, r->refill);
                     };
                     auto shade = [&] {
-                        k_shade<<<grid_for(r, cap, r->block_shade), r->block_shade, 0, st>>>(
+                        k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
                             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms,
                             r->shade_out, r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters,
                             next_count);
                     };
                     auto shadow = [&] {
                         if (count)
-                            k_shadow<CountTally><<<grid_for(r, r->shadow_capacity, r->block_trace), r->block_trace,
+                            k_shadow<CountTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace,
                                                    0, st>>>(s, r->shadow_origin, r->shadow_dir, r->shadow_result,
-                                                            r->counters, r->shadow_capacity, r->tally + 1);
+                                                            r->counters, r->shadow_capacity, r->tally + 1, r->refill);
                         else
-                            k_shadow<NoTally><<<grid_for(r, r->shadow_capacity, r->block_trace), r->block_trace, 0,
+                            k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0,
                                                 st>>>(s, r->shadow_origin, r->shadow_dir, r->shadow_result,
-                                                      r->counters, r->shadow_capacity, nullptr);
+                                                      r->counters, r->shadow_capacity, nullptr, r->refill);
                     };
                     auto finalize = [&] {
-                        k_finalize<<<grid_for(r, cap, r->block_finalize), r->block_finalize, 0, st>>>(
+                        k_finalize<false><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
                             r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result,
-                            r->queue[nxt], next_count, cap, r->framebuffer, &r->counters->work_trace);
+                            r->queue[nxt], next_count, cap, r->framebuffer, &r->counters->work_trace, r->params,
+                            r->tile, r->counters);
                     };
                     if (count) {
                         trace();
@@ -1031,18 +1251,33 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                         finalize();
                         WF_CUDA(cudaGetLastError());
                     } else {
-                        if (wf_status e = timed(WF_KERNEL_TRACE, trace)) return e;
-                        if (wf_status e = timed(WF_KERNEL_SHADE, shade)) return e;
-                        if (wf_status e = timed(WF_KERNEL_SHADOW, shadow)) return e;
-                        if (wf_status e = timed(WF_KERNEL_FINALIZE, finalize)) return e;
+                        uint32_t pb = std::min<uint32_t>(b, WF_PROFILE_BOUNCES - 1);
+                        const int kinds[4] = {WF_KERNEL_TRACE, WF_KERNEL_SHADE, WF_KERNEL_SHADOW, WF_KERNEL_FINALIZE};
+                        for (int k = 0; k < 4; ++k) {
+                            wf_status e = k == 0   ? timed(kinds[k], trace)
+                                          : k == 1 ? timed(kinds[k], shade)
+                                          : k == 2 ? timed(kinds[k], shadow)
+                                                   : timed(kinds[k], finalize);
+                            if (e) return e;
+                            out->bounce_milliseconds[k][pb] += last_ms;
+                            if (k == 2) {  // after the shadow kernel: rays traced and shadow rays of this bounce
+                                uint32_t rays[2];
+                                if (wf_status e2 = read_back(&rays[0], cur_count, sizeof(uint32_t))) return e2;
+                                if (wf_status e2 = read_back(&rays[1], &r->counters->shadow_count, sizeof(uint32_t)))
+                                    return e2;
+                                out->bounce_extension_rays[pb] += rays[0];
+                                out->bounce_shadow_rays[pb] += std::min(rays[1], r->shadow_capacity);
+                            }
+                        }
                     }
                 }
                 k_advance<<<1, 1, 0, st>>>(r->counters, r->tile);
             }
-            if (!count) WF_CUDA(cudaMemcpy(after, &r->counters->extension_rays, sizeof(after), cudaMemcpyDeviceToHost));
+            if (!count)
+                if (wf_status e = read_back(after, &r->counters->extension_rays, sizeof(after))) return e;
         }
         TallyTotals t[2];
-        WF_CUDA(cudaMemcpy(t, r->tally, sizeof(t), cudaMemcpyDeviceToHost));
+        if (wf_status e = read_back(t, r->tally, sizeof(t))) return e;
         out->closest_nodes = t[0].v[0];
         out->closest_triangles = t[0].v[1];
         out->closest_spheres = t[0].v[2];
@@ -1053,7 +1288,7 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
         out->any_instances = t[1].v[3];
     }
     if (r->config.mode == WF_MODE_PERSISTENT)
-        WF_CUDA(cudaMemcpy(after, &r->counters->extension_rays, sizeof(after), cudaMemcpyDeviceToHost));
+        if (wf_status e = read_back(after, &r->counters->extension_rays, sizeof(after))) return e;
     out->extension_rays = after[0] - before[0];
     out->shadow_rays = after[1] - before[1];
     cudaEventDestroy(e0);

@@ -16,26 +16,30 @@ namespace wf {
 
 struct TileDev {
     uint32_t x, y, width, height;
-    uint32_t advance_sample;
+    uint32_t advance_sample;  // add `samples` to the sample index after the launch
+    uint32_t samples = 1;     // streaming mode: samples per pixel of this launch
 };
 
 // Device counters of one renderer (one allocation, zeroed at creation).
 constexpr int kMaxBounces = 64;
+constexpr uint32_t kErrorBarrierTimeout = 1;  // a persistent-kernel grid barrier wait gave up
+constexpr uint32_t kErrorStreamBound = 2;     // the streaming loop exceeded samples * max_depth bounces
 struct Counters {
     uint32_t queue_count[2];
     uint32_t shadow_count;
     uint32_t overflow;
     uint32_t sample_index;
-    uint32_t error;          // persistent-kernel barrier timeout
+    uint32_t error;          // kErrorBarrierTimeout / kErrorStreamBound
     uint32_t barrier_count;
     uint32_t barrier_generation;
     uint32_t work_trace;   // dynamic work counters (32-entry chunks per warp)
     uint32_t work_shade;
     uint32_t work_shadow;
-    uint32_t work_pad;
+    uint32_t stream_iterations;  // streaming mode: loop iterations of the current launch
     unsigned long long extension_rays;
     unsigned long long shadow_rays;
     unsigned long long paths;
+    unsigned long long kernel_launches;  // launches of the render kernels (each CTA 0 thread 0 adds one)
     uint32_t profile[kMaxBounces];          // per-bounce queue sizes (latest sample)
     uint32_t persistent_count[kMaxBounces + 1];
     uint32_t persistent_work[kMaxBounces + 1];
@@ -54,6 +58,7 @@ struct PathSoA {
     float4* radiance;   // xyz, -
     uint4* info;        // pixel, depth, medium, flags (1 = specular, 2 = active)
     unsigned long long* rng;
+    uint32_t* slot_sample;  // streaming mode: sample of the slot's path, relative to the launch's first
 };
 
 struct AsyncCheckpointSlot {
@@ -93,9 +98,11 @@ struct wf_renderer {
     float* framebuffer = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    uint32_t grid_resident[4] = {0, 0, 0, 0};  // trace, shade, shadow, finalize: one full wave of CTAs
     uint32_t persistent_blocks = 0;
     uint32_t persistent_block_size = 128;
     uint32_t chunk = 1;
+    uint32_t refill = 8;  // trace/shadow kernels: idle lanes of a warp that trigger a refill
     // photon map
     uint32_t photons_emitted = 0, photons_stored = 0;
     float4* photon_raw = nullptr;  // 4 float4 per photon: pos(.w valid), dir, flux, rng/meta

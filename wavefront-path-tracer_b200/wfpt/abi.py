@@ -19,7 +19,7 @@ MAT_DIFFUSE, MAT_METAL, MAT_DIELECTRIC, MAT_EMISSIVE, MAT_SPECGLOSS = 0, 1, 2, 3
 ACCEL_BVH, ACCEL_DIRECT = 0, 1
 LIGHT_POINT, LIGHT_SPOT, LIGHT_DIRECTIONAL = 0, 1, 2
 NO_MATERIAL = 0xFFFFFFFF
-MODE_GRAPH, MODE_PERSISTENT = 0, 1
+MODE_GRAPH, MODE_PERSISTENT, MODE_STREAM = 0, 1, 2
 RNG_XORSHIFT32, RNG_PCG32 = 0, 1
 DEBUG_NONE, DEBUG_INTERSECTION, DEBUG_SHADING_NORMAL = 0, 1, 2
 HIT_NONE, HIT_MESH, HIT_STATIC_TRIANGLE, HIT_TRIANGLE, HIT_SPHERE = 0, 1, 2, 3, 4
@@ -105,10 +105,11 @@ class RenderConfig(C.Structure):
         ("gather_radius", C.c_float),
         ("photon_grid_min", C.c_float * 3), ("photon_grid_max", C.c_float * 3),
         ("photon_grid_resolution", C.c_uint32), ("photon_seed", C.c_uint32), ("spectral", C.c_uint32),
-        ("profile_queues", C.c_uint32),
+        ("profile_queues", C.c_uint32), ("refill_threshold", C.c_uint32),
     ]
 
 
+PROFILE_BOUNCES = 32
 KERNEL_NAMES = ["raygen", "trace", "shade", "shadow", "finalize", "persistent"]
 
 
@@ -118,11 +119,15 @@ class KernelProfile(C.Structure):
                 ("closest_nodes", C.c_uint64), ("closest_triangles", C.c_uint64),
                 ("closest_spheres", C.c_uint64), ("closest_instances", C.c_uint64),
                 ("any_nodes", C.c_uint64), ("any_triangles", C.c_uint64),
-                ("any_spheres", C.c_uint64), ("any_instances", C.c_uint64)]
+                ("any_spheres", C.c_uint64), ("any_instances", C.c_uint64),
+                ("bounce_milliseconds", (C.c_float * PROFILE_BOUNCES) * 4),
+                ("bounce_extension_rays", C.c_uint32 * PROFILE_BOUNCES),
+                ("bounce_shadow_rays", C.c_uint32 * PROFILE_BOUNCES)]
 
 
 class RenderStats(C.Structure):
-    _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("paths", C.c_uint64)]
+    _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("paths", C.c_uint64),
+                ("kernel_launches", C.c_uint64)]
 
 
 def declare(lib):

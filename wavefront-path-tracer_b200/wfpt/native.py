@@ -290,7 +290,8 @@ class Renderer:
     def stats(self, reset=False):
         s = abi.RenderStats()
         check(library().wf_render_stats_get(self.handle, C.byref(s), int(reset)))
-        return {"extension_rays": s.extension_rays, "shadow_rays": s.shadow_rays, "paths": s.paths}
+        return {"extension_rays": s.extension_rays, "shadow_rays": s.shadow_rays, "paths": s.paths,
+                "kernel_launches": s.kernel_launches}
 
     def profile_sample(self):
         """wf_profile_sample: per-kernel event times and traversal tallies of
@@ -298,8 +299,13 @@ class Renderer:
         p = abi.KernelProfile()
         check(library().wf_profile_sample(self.handle, C.byref(p)))
         out = {name: {"launches": p.launches[i], "ms": p.milliseconds[i]} for i, name in enumerate(abi.KERNEL_NAMES)}
-        for f, _ in abi.KernelProfile._fields_[2:]:
+        for f, _ in abi.KernelProfile._fields_[2:12]:
             out[f] = getattr(p, f)
+        depth = min(self.config.max_depth, abi.PROFILE_BOUNCES)
+        out["bounces"] = [{"extension_rays": p.bounce_extension_rays[b], "shadow_rays": p.bounce_shadow_rays[b],
+                           **{k: p.bounce_milliseconds[i][b] for i, k in enumerate(("trace_ms", "shade_ms",
+                                                                                     "shadow_ms", "finalize_ms"))}}
+                          for b in range(depth)]
         return out
 
     def photon_stats(self):

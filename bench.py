@@ -49,7 +49,12 @@ WORKLOADS = {
 }
 # Samples per pixel that one step renders (the streaming mode overlaps the
 # tail bounces of these samples).
-SPP_PER_STEP = {"large_mesh": 4, "large_mesh_medium": 1, "large_mesh_small": 4, "sphere_field": 4, "cornell": 16}
+SPP_PER_STEP = {"large_mesh": 1, "large_mesh_medium": 1, "large_mesh_small": 4, "sphere_field": 4, "cornell": 16}
+# Schedule per workload: the streaming loop pays where deep paths are cheap
+# (sphere field, Cornell); on the large mesh regenerated camera rays lose
+# the coherence of a pure primary-ray bounce, so it replays the graph.
+DEFAULT_MODE = {"large_mesh": "graph", "large_mesh_medium": "graph", "large_mesh_small": "graph",
+                "sphere_field": "stream", "cornell": "stream"}
 MODES = {"graph": 0, "persistent": 1, "stream": 2}
 HBM_FALLBACK_GBS = 6650.0
 
@@ -206,7 +211,7 @@ def main():
     ap.add_argument("--workload", default="large_mesh", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--mode", default="stream", choices=sorted(MODES))
+    ap.add_argument("--mode", default=None, choices=sorted(MODES), help="default: per workload")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: per workload)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -232,6 +237,7 @@ def main():
         rkw.setdefault("photon_grid_max", (0, 0, 0))
     stream = torch.cuda.Stream()
     dev_scene = wfpt.DeviceScene(scene)
+    args.mode = args.mode or DEFAULT_MODE[args.workload]
     cfg = wfpt.render_config(width, height, mode=MODES[args.mode], **rkw)
     spp = args.spp or SPP_PER_STEP[args.workload]
     renderer = wfpt.Renderer(dev_scene, cam, cfg, stream=stream.cuda_stream)

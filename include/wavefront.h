@@ -329,7 +329,7 @@ wf_status wf_render_stats_get(wf_renderer* renderer, wf_render_stats* stats, uin
 
 /* Kernel-level profile of one sample pass over the whole frame. */
 enum { WF_KERNEL_RAYGEN = 0, WF_KERNEL_TRACE = 1, WF_KERNEL_SHADE = 2, WF_KERNEL_SHADOW = 3,
-       WF_KERNEL_FINALIZE = 4, WF_KERNEL_PERSISTENT = 5, WF_KERNEL_KINDS = 6 };
+       WF_KERNEL_FINALIZE = 4, WF_KERNEL_PERSISTENT = 5, WF_KERNEL_GATHER = 6, WF_KERNEL_KINDS = 7 };
 enum { WF_PROFILE_BOUNCES = 32 };
 typedef struct wf_kernel_profile {
     uint32_t launches[WF_KERNEL_KINDS];
@@ -340,9 +340,10 @@ typedef struct wf_kernel_profile {
     uint64_t closest_nodes, closest_triangles, closest_spheres, closest_instances;
     uint64_t any_nodes, any_triangles, any_spheres, any_instances;
     /* graph mode, per bounce of the timing replay summed over tiles: event
-     * times of trace, shade, shadow and finalize, extension rays traced and
-     * shadow rays requested (bounces >= WF_PROFILE_BOUNCES are not split) */
-    float bounce_milliseconds[4][WF_PROFILE_BOUNCES];
+     * times of trace, shade, shadow, finalize and caustic gather, extension
+     * rays traced and shadow rays requested (bounces >= WF_PROFILE_BOUNCES
+     * are not split) */
+    float bounce_milliseconds[5][WF_PROFILE_BOUNCES];
     uint32_t bounce_extension_rays[WF_PROFILE_BOUNCES];
     uint32_t bounce_shadow_rays[WF_PROFILE_BOUNCES];
 } wf_kernel_profile;

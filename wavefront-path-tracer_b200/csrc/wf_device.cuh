@@ -238,6 +238,18 @@ struct Camera {
     float tan_half_fov;  // tanf(verticalFov * 0.5f), camera.cuh:19
 };
 
+// Caustic gather requests of one bounce (filled in by the gather kernel): the
+// term slot, the shading point and the two factors of
+// throughput * (albedo * caustic).
+struct GatherQueue {
+    float4* position;    // xyz, global term index
+    float4* normal;      // xyz, 1 = indirect (depth > 0)
+    float4* throughput;  // xyz
+    float4* albedo;      // xyz
+    uint32_t* count;
+    uint32_t capacity;
+};
+
 struct PhotonGridView {
     const float4* position;   // sorted by cell; .w unused
     const float4* direction;

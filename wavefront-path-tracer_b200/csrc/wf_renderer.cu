@@ -163,6 +163,7 @@ __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const 
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
         c->shadow_count = 0;
+        c->gather_count = 0;
         c->work_shade = 0;
         if (bounce < kMaxBounces) c->profile[bounce] = n;
         c->extension_rays += n;
@@ -204,13 +205,14 @@ __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const 
 __global__ void k_shade(DeviceScene s, RenderParams rp, PathSoA ps, const uint32_t* queue, const uint32_t* count,
                         const float4* hit_a, const uint32_t* hit_inst, float4* terms, int4* shade_out,
                         float4* shadow_origin, float4* shadow_dir, uint32_t shadow_capacity, Counters* c,
-                        uint32_t* next_count) {
+                        uint32_t* next_count, GatherQueue gathers) {
     count_launch(c);
     uint32_t n = *count;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
         *next_count = 0;
         c->work_shadow = 0;
+        c->work_gather = 0;
     }
     uint32_t base;
     while (next_chunk(&c->work_shade, n, base)) {
@@ -232,10 +234,32 @@ __global__ void k_shade(DeviceScene s, RenderParams rp, PathSoA ps, const uint32
         sink.nterms = 0;
         sink.kill = kUnconditional;
         sink.overflow = &c->overflow;
+        sink.gathers = gathers;
         bool alive = shade_path(s, rp, path, did_hit, sh, sink);
         if (sink.nterms > kMaxTerms) atomicOr(&c->overflow, 2u);
         store_path(ps, p, path);
         shade_out[i] = make_int4(min(sink.nterms, kMaxTerms), sink.kill, alive ? 1 : 0, 0);
+    }
+}
+
+// Caustic gathers queued by k_shade (gatherCaustics, photon_mapping.cu:91-163),
+// written into the term slots their paths reserved.
+__global__ void k_gather(RenderParams rp, GatherQueue q, float4* terms, Counters* c) {
+    count_launch(c);
+    uint32_t n = min(*q.count, q.capacity);
+    uint32_t base;
+    while (next_chunk(&c->work_gather, n, base)) {
+        uint32_t r = base + (threadIdx.x & 31);
+        if (r >= n) continue;
+        float4 pos = q.position[r], nrm = q.normal[r], thr = q.throughput[r], alb = q.albedo[r];
+        ShadeHit hit{};
+        hit.position = f4xyz(pos);
+        hit.normal = f4xyz(nrm);
+        V3 caustic = gather_caustics(rp.photons, hit, rp.gather_radius);
+        Path depth_only{};
+        depth_only.depth = nrm.w != 0.0f ? 1u : 0u;
+        V3 col = clamp_contribution(depth_only, hadamard(f4xyz(thr), hadamard(f4xyz(alb), caustic)), rp.clamp, false);
+        terms[__float_as_uint(pos.w)] = make_float4(col.x, col.y, col.z, __int_as_float(kUnconditional));
     }
 }
 
@@ -839,7 +863,10 @@ wf_status capture_graph(wf_renderer* r) {
             s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill);
         k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
-            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count);
+            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers);
+        if (r->params.photons.enabled)
+            k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers, r->terms,
+                                                                                   r->counters);
         k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
             s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr, r->refill);
         k_finalize<false><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
@@ -894,7 +921,10 @@ wf_status capture_stream_graph(wf_renderer* r) {
             s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, kMaxBounces, nullptr, r->refill);
         k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
-            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count);
+            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers);
+        if (r->params.photons.enabled)
+            k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers, r->terms,
+                                                                                   r->counters);
         k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
             s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr, r->refill);
         k_finalize<true><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
@@ -1027,6 +1057,15 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
         WF_CUDA(alloc(rr, &r->shadow_dir, r->shadow_capacity));
         WF_CUDA(alloc(rr, &r->shadow_result, r->shadow_capacity));
         if (c.mode == WF_MODE_STREAM) WF_CUDA(alloc(rr, &r->paths.slot_sample, cap));
+        if (c.caustics) {
+            WF_CUDA(alloc(rr, &r->gathers.position, cap));
+            WF_CUDA(alloc(rr, &r->gathers.normal, cap));
+            WF_CUDA(alloc(rr, &r->gathers.throughput, cap));
+            WF_CUDA(alloc(rr, &r->gathers.albedo, cap));
+            r->gathers.count = &r->counters->gather_count;
+            r->gathers.capacity = cap;
+            WF_CUDA(resident_grid(rr, 4, k_gather, r->block_gather));
+        }
         WF_CUDA(resident_grid(rr, 0, k_trace<NoTally>, r->block_trace));
         WF_CUDA(resident_grid(rr, 1, k_shade, r->block_shade));
         WF_CUDA(resident_grid(rr, 2, k_shadow<NoTally>, r->block_trace));
@@ -1223,8 +1262,13 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                         k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
                             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms,
                             r->shade_out, r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters,
-                            next_count);
+                            next_count, r->gathers);
                     };
+                    auto gather = [&] {
+                        k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers,
+                                                                                               r->terms, r->counters);
+                    };
+                    bool gathers = r->params.photons.enabled != 0;
                     auto shadow = [&] {
                         if (count)
                             k_shadow<CountTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace,
@@ -1246,18 +1290,24 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                         WF_CUDA(cudaGetLastError());
                         shade();
                         WF_CUDA(cudaGetLastError());
+                        if (gathers) gather();
                         shadow();
                         WF_CUDA(cudaGetLastError());
                         finalize();
                         WF_CUDA(cudaGetLastError());
                     } else {
                         uint32_t pb = std::min<uint32_t>(b, WF_PROFILE_BOUNCES - 1);
-                        const int kinds[4] = {WF_KERNEL_TRACE, WF_KERNEL_SHADE, WF_KERNEL_SHADOW, WF_KERNEL_FINALIZE};
-                        for (int k = 0; k < 4; ++k) {
+                        const int kinds[5] = {WF_KERNEL_TRACE, WF_KERNEL_SHADE, WF_KERNEL_SHADOW, WF_KERNEL_FINALIZE,
+                                              WF_KERNEL_GATHER};
+                        const int order[5] = {0, 1, 4, 2, 3};  // trace, shade, gather, shadow, finalize
+                        for (int step = 0; step < 5; ++step) {
+                            int k = order[step];
+                            if (k == 4 && !gathers) continue;
                             wf_status e = k == 0   ? timed(kinds[k], trace)
                                           : k == 1 ? timed(kinds[k], shade)
                                           : k == 2 ? timed(kinds[k], shadow)
-                                                   : timed(kinds[k], finalize);
+                                          : k == 3 ? timed(kinds[k], finalize)
+                                                   : timed(kinds[k], gather);
                             if (e) return e;
                             out->bounce_milliseconds[k][pb] += last_ms;
                             if (k == 2) {  // after the shadow kernel: rays traced and shadow rays of this bounce

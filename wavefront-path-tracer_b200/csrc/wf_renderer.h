@@ -36,6 +36,8 @@ struct Counters {
     uint32_t work_shade;
     uint32_t work_shadow;
     uint32_t stream_iterations;  // streaming mode: loop iterations of the current launch
+    uint32_t gather_count;       // caustic gather requests of the current bounce
+    uint32_t work_gather;
     unsigned long long extension_rays;
     unsigned long long shadow_rays;
     unsigned long long paths;
@@ -79,7 +81,7 @@ struct wf_renderer {
     int device = 0;
     int sm_count = 148;
     uint32_t capacity = 0;
-    uint32_t block_trace = 128, block_shade = 128, block_finalize = 256;
+    uint32_t block_trace = 128, block_shade = 128, block_finalize = 256, block_gather = 128;
     uint32_t grid_cap = 0;
     std::vector<void*> allocations;
     uint64_t device_bytes = 0;
@@ -98,7 +100,8 @@ struct wf_renderer {
     float* framebuffer = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
-    uint32_t grid_resident[4] = {0, 0, 0, 0};  // trace, shade, shadow, finalize: one full wave of CTAs
+    uint32_t grid_resident[5] = {0, 0, 0, 0, 0};  // trace, shade, shadow, finalize, gather: one wave of CTAs
+    wf::GatherQueue gathers{};                      // caustic gather requests (graph and streaming modes)
     uint32_t persistent_blocks = 0;
     uint32_t persistent_block_size = 128;
     uint32_t chunk = 1;

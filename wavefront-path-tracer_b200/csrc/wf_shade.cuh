@@ -484,6 +484,7 @@ constexpr int kUnconditional = -1;
 // in the order the reference adds them, and the test (if any) whose
 // unoccluded result ends the path (a terminal branch that escaped).
 struct InlineSink {
+    static constexpr bool kDeferredGather = false;  // caustic gathers run inline
     const DeviceScene* scene;
     V3 radiance;
     bool killed;
@@ -507,6 +508,8 @@ struct InlineSink {
 };
 
 struct DeferredSink {
+    static constexpr bool kDeferredGather = true;  // caustic gathers go to GatherQueue
+    GatherQueue gathers;
     // shadow queue
     float4* shadow_origin;   // origin xyz, t_max
     float4* shadow_dir;      // direction xyz, owner bits
@@ -541,6 +544,30 @@ struct DeferredSink {
     }
     WF_DEV void kill_if_visible(int handle) { kill = handle; }
     WF_DEV void apply_kill(Path&) const {}
+    // Reserves this path's next term for a caustic gather and queues it.
+    WF_DEV void gather(const Path& path, const ShadeHit& shaded, V3 albedo) {
+        int k = nterms;
+        term(V3{0.0f, 0.0f, 0.0f}, kUnconditional);
+        if (k >= kMaxTerms) return;  // overflow is reported by the caller
+        unsigned mask = __activemask();
+        int lane = threadIdx.x & 31;
+        int leader = __ffs(mask) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(gathers.count, uint32_t(__popc(mask)));
+        base = __shfl_sync(mask, base, leader);
+        uint32_t slot = base + __popc(mask & ((1u << lane) - 1u));
+        if (slot >= gathers.capacity) {
+            atomicOr(overflow, 4u);
+            return;
+        }
+        uint32_t index = owner * kMaxTerms + uint32_t(k);
+        gathers.position[slot] = make_float4(shaded.position.x, shaded.position.y, shaded.position.z,
+                                             __uint_as_float(index));
+        gathers.normal[slot] = make_float4(shaded.normal.x, shaded.normal.y, shaded.normal.z,
+                                           path.depth > 0 ? 1.0f : 0.0f);
+        gathers.throughput[slot] = make_float4(path.throughput.x, path.throughput.y, path.throughput.z, 0.0f);
+        gathers.albedo[slot] = make_float4(albedo.x, albedo.y, albedo.z, 0.0f);
+    }
 };
 
 // ------------------------------------------------------- next events
@@ -758,11 +785,12 @@ WF_DEV V3 gather_caustics(const PhotonGridView& g, const ShadeHit& hit, float ra
                 uint32_t begin = g.cell_start[cell], end = begin + g.cell_count[cell];
                 for (uint32_t p = begin; p < end; ++p) {
                     float4 pp = __ldg(&g.position[p]);
-                    float4 pd = __ldg(&g.direction[p]);
                     V3 po = V3{pp.x, pp.y, pp.z} - hit.position;
                     float dsq = dot(po, po);
+                    if (dsq > search_sq) continue;  // the direction is read only for photons in range
+                    float4 pd = __ldg(&g.direction[p]);
                     float cosine = dot(hit.normal, V3{pd.x, pd.y, pd.z});
-                    if (dsq > search_sq || cosine <= 0.0f) continue;
+                    if (cosine <= 0.0f) continue;
                     if (count < kMaxNearest) {
                         nearest_d[count] = dsq;
                         nearest_i[count] = p;
@@ -1021,31 +1049,33 @@ WF_DEV bool shade_path(const DeviceScene& s, const RenderParams& rp, Path& path,
     uint32_t type = m.type == kDiffuse && m.metallic > 0.5f ? uint32_t(kMetal) : m.type;
     float roughness = material_roughness(m);
     V3 direction{0, 0, 0};
-    if (m.flags & kMatGltfPbr) {
+    // Every non-delta surface samples the triangle lights, the punctual lights
+    // and the environment before its continuation (the same order in each
+    // material branch of shadePaths); one call site keeps the kernel small.
+    bool gltf = (m.flags & kMatGltfPbr) != 0;
+    if (gltf || type == kDiffuse || type == kSpecGloss || (type == kMetal && roughness > 0.0f)) {
         sample_direct_light(s, rp, path, hit, shaded, m, sink);
         sample_direct_punctual(s, rp, path, hit, shaded, m, sink);
         sample_direct_environment(s, rp, path, hit, shaded, m, sink);
+    }
+    if (gltf) {
         direction = continue_gltf(s, rp, path, hit, shaded, m, sink);
     } else if (type == kDiffuse) {
-        sample_direct_light(s, rp, path, hit, shaded, m, sink);
-        sample_direct_punctual(s, rp, path, hit, shaded, m, sink);
-        sample_direct_environment(s, rp, path, hit, shaded, m, sink);
         if (rp.photons.enabled) {
-            V3 caustic = gather_caustics(rp.photons, shaded, rp.gather_radius);
-            sink.term(clamp_contribution(path, hadamard(path.throughput, hadamard(albedo, caustic)), rp.clamp, false),
-                      kUnconditional);
+            if constexpr (Sink::kDeferredGather) {
+                sink.gather(path, shaded, albedo);
+            } else {
+                V3 caustic = gather_caustics(rp.photons, shaded, rp.gather_radius);
+                sink.term(clamp_contribution(path, hadamard(path.throughput, hadamard(albedo, caustic)), rp.clamp,
+                                             false),
+                          kUnconditional);
+            }
         }
         direction = continue_diffuse(s, rp, path, hit, shaded, m);
     } else if (type == kSpecGloss) {
-        sample_direct_light(s, rp, path, hit, shaded, m, sink);
-        sample_direct_punctual(s, rp, path, hit, shaded, m, sink);
-        sample_direct_environment(s, rp, path, hit, shaded, m, sink);
         direction = continue_glossy(s, rp, path, hit, shaded, m);
     } else if (type == kMetal) {
         if (roughness > 0.0f) {
-            sample_direct_light(s, rp, path, hit, shaded, m, sink);
-            sample_direct_punctual(s, rp, path, hit, shaded, m, sink);
-            sample_direct_environment(s, rp, path, hit, shaded, m, sink);
             direction = continue_glossy(s, rp, path, hit, shaded, m);
         } else {
             path.throughput = hadamard(path.throughput, albedo);

@@ -110,17 +110,17 @@ class RenderConfig(C.Structure):
 
 
 PROFILE_BOUNCES = 32
-KERNEL_NAMES = ["raygen", "trace", "shade", "shadow", "finalize", "persistent"]
+KERNEL_NAMES = ["raygen", "trace", "shade", "shadow", "finalize", "persistent", "gather"]
 
 
 class KernelProfile(C.Structure):
-    _fields_ = [("launches", C.c_uint32 * 6), ("milliseconds", C.c_float * 6),
+    _fields_ = [("launches", C.c_uint32 * 7), ("milliseconds", C.c_float * 7),
                 ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("closest_nodes", C.c_uint64), ("closest_triangles", C.c_uint64),
                 ("closest_spheres", C.c_uint64), ("closest_instances", C.c_uint64),
                 ("any_nodes", C.c_uint64), ("any_triangles", C.c_uint64),
                 ("any_spheres", C.c_uint64), ("any_instances", C.c_uint64),
-                ("bounce_milliseconds", (C.c_float * PROFILE_BOUNCES) * 4),
+                ("bounce_milliseconds", (C.c_float * PROFILE_BOUNCES) * 5),
                 ("bounce_extension_rays", C.c_uint32 * PROFILE_BOUNCES),
                 ("bounce_shadow_rays", C.c_uint32 * PROFILE_BOUNCES)]
 

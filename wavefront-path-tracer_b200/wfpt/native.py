@@ -304,7 +304,8 @@ class Renderer:
         depth = min(self.config.max_depth, abi.PROFILE_BOUNCES)
         out["bounces"] = [{"extension_rays": p.bounce_extension_rays[b], "shadow_rays": p.bounce_shadow_rays[b],
                            **{k: p.bounce_milliseconds[i][b] for i, k in enumerate(("trace_ms", "shade_ms",
-                                                                                     "shadow_ms", "finalize_ms"))}}
+                                                                                     "shadow_ms", "finalize_ms",
+                                                                                     "gather_ms"))}}
                           for b in range(depth)]
         return out
 

@@ -205,7 +205,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="large_mesh", choices=sorted(WORKLOADS))
@@ -246,8 +246,9 @@ def main():
     # path state (6 x 16 B), queues, hit records, terms and shadow requests per slot
     renderer_bytes = width * height * (96 + 8 + 20 + 16 * 8 + 16 + 5 * 33 + 12)
     pixels = width * height
-    # Each rank owns the absolute sample range [rank * 2^20, ...).
-    base = rank << 20
+    # Each rank owns its own absolute sample range (weak scaling).
+    from wfpt import shard
+    base = shard.rank_sample_base(rank)
 
     def barrier():
         if world > 1:
@@ -319,7 +320,7 @@ def main():
     # Multi-GPU merge: one NCCL reduce of the framebuffers to rank 0.
     if world > 1:
         fb = torch.from_numpy(renderer.download()).cuda()
-        dist.reduce(fb, dst=0, op=dist.ReduceOp.SUM)
+        shard.reduce_framebuffer(fb, dst=0)
         if rank == 0:
             assert torch.isfinite(fb).all()
 

@@ -327,6 +327,30 @@ typedef struct wf_render_stats {
 /* Ray counters accumulated since creation or the last reset (synchronizes). */
 wf_status wf_render_stats_get(wf_renderer* renderer, wf_render_stats* stats, uint32_t reset);
 
+/* Persistent-mode render of one tile that allocates no device memory.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc while rendering (a host embedded in another framework's memory
+ * pool, a process whose device-memory budget is fixed at start-up, or code
+ * that must not trigger the implicit synchronization an allocation can
+ * cause).  The caller owns the scene and `framebuffer` (a DEVICE buffer of
+ * config->width * config->height * 3 floats, already zeroed or holding
+ * earlier sums); the call ADDS the unnormalized sums of samples
+ * [sample_start, sample_start + sample_count) of pixels inside the tile,
+ * exactly as wf_render with WF_MODE_PERSISTENT does.  Working memory is one
+ * fixed 6.3 MB device array inside the library that every GPU loading the
+ * library holds until the process exits; tiles above 65,536 pixels return
+ * WF_ERR_CAPACITY and configs with caustics return WF_ERR_UNSUPPORTED.
+ * The first call on each device looks up the array's device address and the
+ * kernel's resident grid (no allocation), so make that first call before any
+ * stream capture.  Every call shares the one array (it is reset at the start
+ * of each call): calls whose GPU work overlaps, from several host threads or
+ * streams, race and give wrong images.  The call returns after the work on
+ * `stream` (cudaStream_t, may be NULL) has finished. */
+wf_status wf_render_tile_static(const wf_scene* scene, const wf_camera* camera,
+                                const wf_render_config* config, uint32_t x, uint32_t y,
+                                uint32_t width, uint32_t height, uint32_t sample_start,
+                                uint32_t sample_count, float* framebuffer, void* stream);
+
 /* Kernel-level profile of one sample pass over the whole frame. */
 enum { WF_KERNEL_RAYGEN = 0, WF_KERNEL_TRACE = 1, WF_KERNEL_SHADE = 2, WF_KERNEL_SHADOW = 3,
        WF_KERNEL_FINALIZE = 4, WF_KERNEL_PERSISTENT = 5, WF_KERNEL_GATHER = 6, WF_KERNEL_KINDS = 7 };

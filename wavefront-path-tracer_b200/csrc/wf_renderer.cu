@@ -1364,3 +1364,170 @@ wf_status trace_any_batch(const wf_scene* scene, const wf_ray* rays, const float
 }
 
 }  // namespace wf
+
+// ---------------------------------------------------------------------------
+// wf_render_tile_static: the persistent-mode tile render with its working
+// memory in a fixed device array instead of cudaMalloc'd buffers.
+//
+// Some hosts cannot allocate device memory at render time: a caller running
+// inside another framework's memory pool, under a strict memory budget
+// that was fixed at start-up, or from a context where cudaMalloc would
+// synchronize the device.  They still own their inputs (the scene) and
+// outputs (the framebuffer); this entry point needs nothing else.  The cost
+// is a file-scope array that every GPU loading this library holds until the
+// process exits, and a cap on the tile size.
+namespace wf {
+namespace {
+
+constexpr uint32_t kStaticMaxPixels = 65536;  // one 256 x 256 tile
+
+// Scratch layout (each part 256-byte aligned): counters, tile, path state
+// (origin, direction, throughput, radiance as float4; info as uint4; RNG
+// state as u64) and the two index queues, kStaticMaxPixels slots each.
+constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+constexpr size_t kStaticCountersOffset = 0;
+constexpr size_t kStaticTileOffset = align256(kStaticCountersOffset + sizeof(Counters));
+constexpr size_t kStaticPathOffset = align256(kStaticTileOffset + sizeof(TileDev));
+constexpr size_t kStaticFloat4Bytes = size_t(kStaticMaxPixels) * sizeof(float4);
+constexpr size_t kStaticInfoOffset = kStaticPathOffset + 4 * kStaticFloat4Bytes;
+constexpr size_t kStaticRngOffset = align256(kStaticInfoOffset + size_t(kStaticMaxPixels) * sizeof(uint4));
+constexpr size_t kStaticQueueOffset = align256(kStaticRngOffset + size_t(kStaticMaxPixels) * sizeof(uint64_t));
+constexpr size_t kStaticBytes = align256(kStaticQueueOffset + 2 * size_t(kStaticMaxPixels) * sizeof(uint32_t));
+
+// 6.3 MB per device.  Host code must not use this name as a device address:
+// the host sees a stand-in object; the device address comes from
+// cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mutex;
+unsigned char* g_static_base[kStaticMaxDevices] = {};
+uint32_t g_static_resident[kStaticMaxDevices] = {};
+
+// Zeroes the counters at the start of a call (the array keeps the previous
+// call's contents) and writes the tile and the first sample index.
+__global__ void k_static_prepare(Counters* c, TileDev* tile_out, TileDev tile, uint32_t sample_start) {
+    uint32_t* words = reinterpret_cast<uint32_t*>(c);
+    for (size_t i = threadIdx.x; i < sizeof(Counters) / sizeof(uint32_t); i += blockDim.x) words[i] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        c->sample_index = sample_start;
+        *tile_out = tile;
+    }
+}
+
+// Per-sample reset of the persistent kernel's queue counters and barrier
+// arrival count (what launch_tile clears with memsets).
+__global__ void k_static_sample_reset(Counters* c) {
+    for (uint32_t i = threadIdx.x; i < 2 * (kMaxBounces + 1); i += blockDim.x) c->persistent_count[i] = 0;
+    if (threadIdx.x == 0) c->barrier_count = 0;
+}
+
+}  // namespace
+}  // namespace wf
+
+extern "C" wf_status wf_render_tile_static(const wf_scene* scene, const wf_camera* camera,
+                                          const wf_render_config* config, uint32_t x, uint32_t y, uint32_t width,
+                                          uint32_t height, uint32_t sample_start, uint32_t sample_count,
+                                          float* framebuffer, void* stream) {
+    using namespace wf;
+    if (!scene || !camera || !config || !framebuffer) return fail(WF_ERR_INVALID_ARG, "null argument");
+    const wf_render_config& c = *config;
+    if (!std::isfinite(c.indirect_clamp) || c.indirect_clamp < 0.0f)
+        return fail(WF_ERR_INVALID_ARG, "Indirect radiance clamp must be finite and nonnegative");
+    if (c.width == 0 || c.height == 0) return fail(WF_ERR_INVALID_ARG, "Render dimensions must be greater than zero");
+    if (c.max_depth == 0) return fail(WF_ERR_INVALID_ARG, "maximum depth must be greater than zero");
+    if (c.max_depth > kMaxBounces) return fail(WF_ERR_INVALID_ARG, "maximum depth above %d", kMaxBounces);
+    if (c.rng > WF_RNG_PCG32 || c.debug > WF_DEBUG_SHADING_NORMAL)
+        return fail(WF_ERR_INVALID_ARG, "unknown rng strategy or debug view");
+    if (c.caustics)
+        return fail(WF_ERR_UNSUPPORTED, "wf_render_tile_static does not build photon maps (caustics must be 0)");
+    if (scene->view.punctual_count - scene->view.directional_count > 0 && scene->view.directional_count > 2)
+        return fail(WF_ERR_UNSUPPORTED, "more than two directional lights");
+    if (width == 0 || height == 0 || x >= c.width || y >= c.height || width > c.width - x || height > c.height - y)
+        return fail(WF_ERR_INVALID_ARG, "Render task tile is outside the framebuffer");
+    if (uint64_t(width) * height > kStaticMaxPixels)
+        return fail(WF_ERR_CAPACITY, "wf_render_tile_static renders at most %u pixels per call (tile is %ux%u)",
+                    kStaticMaxPixels, width, height);
+    if (sample_count == 0) return fail(WF_ERR_INVALID_ARG, "Render task sample range is empty");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+    // Once per device: the device address of the scratch array and the
+    // persistent kernel's resident grid.
+    int device = 0;
+    WF_CUDA(cudaGetDevice(&device));
+    if (device < 0 || device >= kStaticMaxDevices) return fail(WF_ERR_UNSUPPORTED, "device index %d", device);
+    unsigned char* base = nullptr;
+    uint32_t resident = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mutex);
+        if (!g_static_base[device]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+            int cooperative = 0, sms = 0, per_sm = 0;
+            WF_CUDA(cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, device));
+            if (!cooperative) return fail(WF_ERR_UNSUPPORTED, "device does not support cooperative launches");
+            WF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+            WF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent, 128, 0));
+            if (per_sm <= 0) return fail(WF_ERR_UNSUPPORTED, "the persistent kernel cannot be resident");
+            g_static_resident[device] = uint32_t(per_sm) * uint32_t(sms);
+            g_static_base[device] = static_cast<unsigned char*>(p);
+        }
+        base = g_static_base[device];
+        resident = g_static_resident[device];
+    }
+
+    // The same parameters renderer_create derives for a persistent renderer.
+    RenderParams rp{};
+    rp.width = c.width;
+    rp.height = c.height;
+    rp.max_depth = c.max_depth;
+    rp.rr_start = c.rr_start_depth;
+    rp.rng = c.rng;
+    rp.debug = c.debug;
+    rp.clamp = c.indirect_clamp;
+    rp.gather_radius = c.gather_radius;
+    rp.camera.position = V3{camera->position[0], camera->position[1], camera->position[2]};
+    rp.camera.forward = V3{camera->forward[0], camera->forward[1], camera->forward[2]};
+    rp.camera.right = V3{camera->right[0], camera->right[1], camera->right[2]};
+    rp.camera.up = V3{camera->up[0], camera->up[1], camera->up[2]};
+    rp.camera.aspect_ratio = camera->aspect_ratio;
+    rp.camera.tan_half_fov = wfm::tanf(camera->vertical_fov * 0.5f);
+    rp.photons = PhotonGridView{};
+    uint32_t blocks = c.persistent_blocks ? std::max(1u, std::min(c.persistent_blocks, resident)) : resident;
+    uint32_t chunk = c.chunk ? std::max(1u, c.chunk / 32) : 1u;
+
+    Counters* counters = reinterpret_cast<Counters*>(base + kStaticCountersOffset);
+    TileDev* tile_dev = reinterpret_cast<TileDev*>(base + kStaticTileOffset);
+    PathSoA ps{};
+    ps.origin = reinterpret_cast<float4*>(base + kStaticPathOffset);
+    ps.direction = ps.origin + kStaticMaxPixels;
+    ps.throughput = ps.direction + kStaticMaxPixels;
+    ps.radiance = ps.throughput + kStaticMaxPixels;
+    ps.info = reinterpret_cast<uint4*>(base + kStaticInfoOffset);
+    ps.rng = reinterpret_cast<unsigned long long*>(base + kStaticRngOffset);
+    ps.slot_sample = nullptr;
+    uint32_t* q0 = reinterpret_cast<uint32_t*>(base + kStaticQueueOffset);
+    uint32_t* q1 = q0 + kStaticMaxPixels;
+
+    TileDev tile{x, y, width, height, 1};
+    k_static_prepare<<<1, 256, 0, st>>>(counters, tile_dev, tile, sample_start);
+    WF_CUDA(cudaGetLastError());
+    DeviceScene s = scene->view;
+    const TileDev* tp = tile_dev;
+    uint32_t cap = kStaticMaxPixels;
+    void* args[] = {&s, &rp, &tp, &counters, &ps, &q0, &q1, &cap, &framebuffer, &chunk};
+    for (uint32_t i = 0; i < sample_count; ++i) {
+        k_static_sample_reset<<<1, 128, 0, st>>>(counters);
+        WF_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_persistent), dim3(blocks), dim3(128), args, 0,
+                                            st));
+        k_advance<<<1, 1, 0, st>>>(counters, tile_dev);
+        WF_CUDA(cudaGetLastError());
+    }
+    uint32_t error = 0;
+    WF_CUDA(cudaMemcpyAsync(&error, &counters->error, sizeof(error), cudaMemcpyDeviceToHost, st));
+    WF_CUDA(cudaStreamSynchronize(st));
+    if (error) return fail(WF_ERR_TIMEOUT, "persistent kernel grid barrier timed out");
+    return WF_OK;
+}

@@ -149,6 +149,8 @@ def declare(lib):
         "wf_renderer_destroy": (S, [P]),
         "wf_render": (S, [P, U32, U32, U32, U32, U32, U32, U32]),
         "wf_render_frame": (S, [P, U32]),
+        "wf_render_tile_static": (S, [P, C.POINTER(Camera), C.POINTER(RenderConfig), U32, U32, U32, U32, U32, U32, P,
+                                      P]),
         "wf_framebuffer_reset": (S, [P]),
         "wf_set_sample_index": (S, [P, U32]),
         "wf_get_sample_index": (S, [P, C.POINTER(U32)]),

@@ -23,9 +23,12 @@
 #if defined(__CUDACC__)
 #define WF_DEV __device__ __forceinline__
 #define WF_HDI __host__ __device__ __forceinline__
+// Large shading helpers called from several sites: one out-of-line copy.
+#define WF_CALL __device__ __noinline__
 #else
 #define WF_DEV inline
 #define WF_HDI inline
+#define WF_CALL inline
 #endif
 
 namespace wf {

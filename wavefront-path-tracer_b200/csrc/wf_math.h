@@ -23,8 +23,12 @@
 
 #if defined(__CUDACC__)
 #define WF_HD __host__ __device__ __forceinline__
+// The double-precision series are called from many shading sites; one
+// out-of-line copy per kernel keeps the instruction footprint small.
+#define WF_HD_CALL static __host__ __device__ __noinline__
 #else
 #define WF_HD inline
+#define WF_HD_CALL inline
 #endif
 
 namespace wfm {
@@ -85,7 +89,7 @@ WF_HD double cos_kernel(double r) {
     return 1.0 + z * p;
 }
 
-WF_HD double sin(double x) {
+WF_HD_CALL double sin(double x) {
     if (!(x == x) || x == INFINITY || x == -INFINITY) return x - x;
     int q;
     double r = reduce_pio2(x, q);
@@ -97,7 +101,7 @@ WF_HD double sin(double x) {
     }
 }
 
-WF_HD double cos(double x) {
+WF_HD_CALL double cos(double x) {
     if (!(x == x) || x == INFINITY || x == -INFINITY) return x - x;
     int q;
     double r = reduce_pio2(x, q);
@@ -138,7 +142,7 @@ WF_HD double atan_unit(double t) {
 }
 
 // atan2 with the C library's signed-zero and quadrant conventions.
-WF_HD double atan2(double y, double x) {
+WF_HD_CALL double atan2(double y, double x) {
     if (!(x == x) || !(y == y)) return x + y;
     bool xneg = std::signbit(x), yneg = std::signbit(y);
     if (y == 0.0) return xneg ? (yneg ? -kPi : kPi) : y;
@@ -159,7 +163,7 @@ WF_HD double atan2(double y, double x) {
 
 // log(x) = e * ln2 + 2 atanh((m - 1) / (m + 1)), m in [sqrt(1/2), sqrt(2)),
 // atanh series through s^21.
-WF_HD double log(double x) {
+WF_HD_CALL double log(double x) {
     if (!(x == x) || x < 0.0) return (x - x) / (x - x);
     if (x == 0.0) return -INFINITY;
     if (x == INFINITY) return x;
@@ -187,7 +191,7 @@ WF_HD double log(double x) {
 }
 
 // exp(x) = 2^k exp(r), r = x - k ln2, Taylor series of exp(r) through r^17.
-WF_HD double exp(double x) {
+WF_HD_CALL double exp(double x) {
     if (!(x == x)) return x;
     if (x > 709.78) return INFINITY;
     if (x < -745.2) return 0.0;
@@ -220,7 +224,7 @@ WF_HD bool is_odd_integer(double y) {
 }
 
 // pow with the C library's special cases for the arguments the renderer uses.
-WF_HD double pow(double x, double y) {
+WF_HD_CALL double pow(double x, double y) {
     if (y == 0.0 || x == 1.0) return 1.0;
     if (!(x == x) || !(y == y)) return x + y;
     if (x == 0.0) {

@@ -17,6 +17,7 @@
 #include "wf_renderer.h"
 #include "wf_shade.cuh"
 #include "wf_lane_traverse.cuh"
+#include "wf_wavefront.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -35,60 +36,6 @@ wf_status cuda_fail(cudaError_t e, const char* what) {
     } while (0)
 
 namespace {
-
-// Device-side launch count of the render kernels (kernels on one stream run
-// in order, so thread 0 of CTA 0 updates it without an atomic).
-WF_DEV void count_launch(Counters* c) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) ++c->kernel_launches;
-}
-
-WF_DEV Path load_path(const PathSoA& ps, uint32_t p) {
-    float4 o = ps.origin[p], d = ps.direction[p], t = ps.throughput[p];
-    uint4 info = ps.info[p];
-    Path path;
-    path.origin = f4xyz(o);
-    path.prev_pdf = o.w;
-    path.direction = f4xyz(d);
-    path.eta_scale = d.w;
-    path.throughput = f4xyz(t);
-    path.medium_density = t.w;
-    path.pixel = info.x;
-    path.depth = info.y;
-    path.medium = info.z;
-    path.specular = (info.w & 1u) != 0;
-    path.active = (info.w & 2u) != 0;
-    path.rng = ps.rng[p];
-    return path;
-}
-
-WF_DEV void store_path(const PathSoA& ps, uint32_t p, const Path& path) {
-    ps.origin[p] = make_float4(path.origin.x, path.origin.y, path.origin.z, path.prev_pdf);
-    ps.direction[p] = make_float4(path.direction.x, path.direction.y, path.direction.z, path.eta_scale);
-    ps.throughput[p] = make_float4(path.throughput.x, path.throughput.y, path.throughput.z, path.medium_density);
-    ps.info[p] = make_uint4(path.pixel, path.depth, path.medium, (path.specular ? 1u : 0u) | (path.active ? 2u : 0u));
-    ps.rng[p] = path.rng;
-}
-
-// generatePrimaryRays, src/renderer/renderer.cu:10-42.
-WF_DEV void init_path(const RenderParams& rp, const TileDev& tile, uint32_t sample, uint32_t lp, Path& path) {
-    uint32_t x = tile.x + lp % tile.width;
-    uint32_t y = tile.y + lp / tile.width;
-    uint32_t pixel = y * rp.width + x;
-    uint64_t rng = make_rng_state(pixel_rng_key(pixel, sample, rp.rng), rp.rng);
-    float u = (float(x) + random_float(rng, rp.rng)) / float(rp.width);
-    float v = (float(y) + random_float(rng, rp.rng)) / float(rp.height);
-    camera_ray(rp.camera, u, v, path.origin, path.direction);
-    path.throughput = V3{1.0f, 1.0f, 1.0f};
-    path.pixel = pixel;
-    path.depth = 0;
-    path.rng = rng;
-    path.medium = kInvalid;
-    path.medium_density = 1.0f;
-    path.prev_pdf = 0.0f;
-    path.specular = true;
-    path.active = true;
-    path.eta_scale = 1.0f;
-}
 
 __global__ void k_raygen(RenderParams rp, const TileDev* tile_ptr, Counters* c, PathSoA ps, uint32_t* queue,
                          uint32_t capacity) {
@@ -133,25 +80,6 @@ __global__ void k_raygen_stream(RenderParams rp, const TileDev* tile_ptr, Counte
         ps.radiance[lp] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         ps.slot_sample[lp] = 0;
         queue[lp] = lp;
-    }
-}
-
-// Warps pull 32-entry chunks from `counter` until `n` is exhausted (the
-// counter is zeroed by the kernel that runs before).  Balances warps whose
-// rays need very different traversal work.
-WF_DEV bool next_chunk(uint32_t* counter, uint32_t n, uint32_t& base) {
-    uint32_t b = 0;
-    if ((threadIdx.x & 31) == 0) b = atomicAdd(counter, 32u);
-    base = __shfl_sync(0xffffffffu, b, 0);
-    return base < n;
-}
-
-// Sums a thread's tally into per-launch totals (profiling pass only).
-WF_DEV void flush_tally(const CountTally& t, TallyTotals* totals) {
-    unsigned long long v[4] = {t.nodes, t.triangles, t.spheres, t.instances};
-    for (int k = 0; k < 4; ++k) {
-        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
-        if ((threadIdx.x & 31) == 0 && v[k]) atomicAdd(&totals->v[k], v[k]);
     }
 }
 
@@ -202,7 +130,8 @@ __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const 
     if constexpr (std::is_same<Tally, CountTally>::value) flush_tally(tally, totals);
 }
 
-__global__ void k_shade(DeviceScene s, RenderParams rp, PathSoA ps, const uint32_t* queue, const uint32_t* count,
+// 128 registers: 4 CTAs per SM; the few spills cost less than the lost warps.
+__global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ RenderParams rp, PathSoA ps, const uint32_t* queue, const uint32_t* count,
                         const float4* hit_a, const uint32_t* hit_inst, float4* terms, int4* shade_out,
                         float4* shadow_origin, float4* shadow_dir, uint32_t shadow_capacity, Counters* c,
                         uint32_t* next_count, GatherQueue gathers) {
@@ -244,7 +173,7 @@ __global__ void k_shade(DeviceScene s, RenderParams rp, PathSoA ps, const uint32
 
 // Caustic gathers queued by k_shade (gatherCaustics, photon_mapping.cu:91-163),
 // written into the term slots their paths reserved.
-__global__ void k_gather(RenderParams rp, GatherQueue q, float4* terms, Counters* c) {
+__global__ void k_gather(const __grid_constant__ RenderParams rp, GatherQueue q, float4* terms, Counters* c) {
     count_launch(c);
     uint32_t n = min(*q.count, q.capacity);
     uint32_t base;
@@ -413,7 +342,8 @@ WF_DEV bool grid_barrier(Counters* c, uint32_t blocks) {
     return *(volatile uint32_t*)&c->error == 0;
 }
 
-__global__ void __launch_bounds__(128) k_persistent(DeviceScene s, RenderParams rp, const TileDev* tile_ptr,
+__global__ void __launch_bounds__(128) k_persistent(const __grid_constant__ DeviceScene s,
+                                                    const __grid_constant__ RenderParams rp, const TileDev* tile_ptr,
                                                     Counters* c, PathSoA ps, uint32_t* q0, uint32_t* q1,
                                                     uint32_t capacity, float* framebuffer, uint32_t chunk_warps) {
     count_launch(c);
@@ -562,7 +492,7 @@ __global__ void k_any_batch(DeviceScene s, const wf_ray* rays, const float* max_
 // emitPhotons / tracePhotons, src/renderer/photon_mapping.cu:4-74.  Each
 // photon is 4 float4: position (.w = valid), direction (.w = spectral channel),
 // flux, rng state (.xy) and specular bounce count (.z).
-__global__ void k_emit_photons(DeviceScene s, uint32_t count, uint32_t seed, uint32_t strategy, uint32_t spectral,
+__global__ void k_emit_photons(const __grid_constant__ DeviceScene s, uint32_t count, uint32_t seed, uint32_t strategy, uint32_t spectral,
                                float4* photons) {
     uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
     if (index >= count || s.light_count == 0) return;
@@ -598,7 +528,7 @@ __global__ void k_emit_photons(DeviceScene s, uint32_t count, uint32_t seed, uin
     ph[3] = make_float4(__uint_as_float(uint32_t(rng)), __uint_as_float(uint32_t(rng >> 32)), __uint_as_float(0u), 0.0f);
 }
 
-__global__ void k_trace_photons(DeviceScene s, uint32_t count, uint32_t max_depth, uint32_t strategy,
+__global__ void k_trace_photons(const __grid_constant__ DeviceScene s, uint32_t count, uint32_t max_depth, uint32_t strategy,
                                 float4* photons, uint32_t* stored) {
     uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
     if (index >= count || s.light_count == 0) return;

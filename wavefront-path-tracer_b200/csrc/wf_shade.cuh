@@ -145,7 +145,7 @@ struct DielectricInterface {
     bool front_face;
 };
 
-WF_DEV DielectricInterface dielectric_interface(V3 incident, V3 geometric, V3 shading, float ior) {
+WF_CALL DielectricInterface dielectric_interface(V3 incident, V3 geometric, V3 shading, float ior) {
     bool front = dot(incident, geometric) < 0.0f;
     V3 facing = front ? geometric : -geometric;
     if (dot(shading, geometric) < 0.0f) shading = -shading;
@@ -187,7 +187,7 @@ WF_DEV float sg_d(float nh, float alpha) {
 WF_DEV float sg_g1(float cosine, float alpha) {
     return 2.0f * cosine / (cosine + sqrtf(alpha * alpha + (1.0f - alpha * alpha) * cosine * cosine));
 }
-WF_DEV V3 sg_evaluate(const SpecGloss& s, V3 n, V3 outgoing, V3 incoming, float& pdf) {
+WF_CALL V3 sg_evaluate(const SpecGloss& s, V3 n, V3 outgoing, V3 incoming, float& pdf) {
     pdf = 0.0f;
     float nv = dot(n, outgoing), nl = dot(n, incoming);
     V3 sum = outgoing + incoming;
@@ -301,7 +301,7 @@ WF_DEV V3 pbr_sample_reflection(V3 normal, V3 view, float roughness, float u, fl
     V3 half = sg_basis(normal, sine * wfm::cosf(phi), sine * wfm::sinf(phi), cosine);
     return 2.f * dot(view, half) * half - view;
 }
-WF_DEV V3 pbr_evaluate_cos(const GltfPbr& s, V3 view, V3 light, float diffuse_pdf, float& pdf) {
+WF_CALL V3 pbr_evaluate_cos(const GltfPbr& s, V3 view, V3 light, float diffuse_pdf, float& pdf) {
     GltfWeights w = pbr_weights(s, view);
     float nl = fmaxf(0.f, dot(s.normal, light));
     V3 reflection_normal = pbr_specular_normal(s);
@@ -332,7 +332,7 @@ WF_DEV void environment_uv(const Environment& e, V3 world, float& u, float& v) {
     float vv = wfm::atan2f(sqrtf(d.x * d.x + d.z * d.z), d.y) / kPiF;
     v = fminf(1.0f, fmaxf(0.0f, vv));
 }
-WF_DEV float environment_pdf(const Environment& e, V3 direction) {
+WF_CALL float environment_pdf(const Environment& e, V3 direction) {
     if (e.width == 0 || e.height == 0 || e.probabilities == nullptr) return 0.0f;
     float u, v;
     environment_uv(e, direction, u, v);
@@ -344,7 +344,7 @@ WF_DEV float environment_pdf(const Environment& e, V3 direction) {
 // Bilinear lookup: normalized coordinates, wrap in u, clamp in v, weights
 // (1-f, f), rows then columns (the texture of scene.cu:318-328 with the
 // filter arithmetic of the reference's CPU replay, cpu_replay.cpp:14-24).
-WF_DEV V3 environment_texel(const Environment& e, float u, float v) {
+WF_CALL V3 environment_texel(const Environment& e, float u, float v) {
     float tx = u * e.width - .5f, ty = v * e.height - .5f;
     int x = int(floorf(tx)), y = int(floorf(ty));
     float fx = tx - x, fy = ty - y;
@@ -362,7 +362,7 @@ WF_DEV V3 environment_texel(const Environment& e, float u, float v) {
         }
     return V3{rx, ry, rz};
 }
-WF_DEV V3 environment_radiance(const Environment& e, V3 direction) {
+WF_CALL V3 environment_radiance(const Environment& e, V3 direction) {
     float u, v;
     environment_uv(e, direction, u, v);
     return environment_texel(e, u, v) * e.intensity;
@@ -371,7 +371,7 @@ struct EnvSample {
     V3 direction;
     float pdf;
 };
-WF_DEV EnvSample sample_environment(const Environment& e, double candidate, float coin, float longitude,
+WF_CALL EnvSample sample_environment(const Environment& e, double candidate, float coin, float longitude,
                                     float latitude) {
     constexpr double pi = 3.14159265358979323846;
     uint32_t count = e.width * e.height;
@@ -425,7 +425,7 @@ struct ShadeHit {
 };
 
 // evaluateSurface, device_traversal.cuh:427-441.
-WF_DEV V3 evaluate_surface(const DeviceScene& s, const Material& m, const ShadeHit& hit, V3 outgoing, V3 incoming,
+WF_CALL V3 evaluate_surface(const DeviceScene& s, const Material& m, const ShadeHit& hit, V3 outgoing, V3 incoming,
                            float& pdf) {
     if (m.type == kSpecGloss)
         return sg_evaluate(SpecGloss{m.albedo, m.specular, material_roughness(m)}, hit.normal, outgoing, incoming, pdf);
@@ -442,7 +442,7 @@ WF_DEV V3 evaluate_surface(const DeviceScene& s, const Material& m, const ShadeH
 }
 
 // getGltfPbrSurface, device_traversal.cuh:500-516 (untextured).
-WF_DEV GltfPbr gltf_surface(const Material& m, const ShadeHit& hit, const ShadeHit& shaded) {
+WF_CALL GltfPbr gltf_surface(const Material& m, const ShadeHit& hit, const ShadeHit& shaded) {
     float weight = m.specular_weight;
     V3 color = m.specular_color;
     float f0 = (m.ior - 1.f) / (m.ior + 1.f);
@@ -465,7 +465,7 @@ WF_DEV GltfPbr gltf_surface(const Material& m, const ShadeHit& hit, const ShadeH
 }
 
 // evaluateSurfaceCos, device_traversal.cuh:519-527.
-WF_DEV V3 evaluate_surface_cos(const DeviceScene& s, const Material& m, const ShadeHit& hit, const ShadeHit& shaded,
+WF_CALL V3 evaluate_surface_cos(const DeviceScene& s, const Material& m, const ShadeHit& hit, const ShadeHit& shaded,
                                V3 view, V3 light, float& pdf) {
     if (m.flags & kMatGltfPbr) {
         GltfPbr g = gltf_surface(m, hit, shaded);

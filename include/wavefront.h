@@ -385,6 +385,50 @@ wf_status wf_photon_stats(wf_renderer* renderer, uint32_t* stored, uint32_t* emi
  * flux sum, valid flag (host memory, count = emitted). */
 wf_status wf_photons_download(wf_renderer* renderer, float* records, uint32_t count);
 
+/* ------------------------------------------------------------------- batch */
+/* Many independent render jobs (own scene, camera, resolution, depth and
+ * sample range) in one captured graph.  No counterpart in the reference,
+ * which renders one job per RenderDriver.  A pool of path slots works
+ * through (job, pixel) units; a slot renders all of its unit's samples in
+ * sample order before it takes the next unit, so each job's framebuffer is
+ * bit-identical to a wf_render of that job's sample range.  Caustics are
+ * not supported in a batch (WF_ERR_UNSUPPORTED). */
+typedef struct wf_batch wf_batch;
+typedef struct wf_batch_job {
+    const wf_scene* scene;
+    wf_camera camera;
+    wf_render_config config;   /* width/height = the job's image; mode and tile fields are ignored */
+    uint32_t sample_start;     /* absolute first sample */
+    uint32_t sample_count;
+} wf_batch_job;
+typedef struct wf_batch_config {
+    uint32_t slot_capacity;    /* paths in flight; 0 = min(total pixels, 4M) */
+    uint32_t block_size;       /* trace/shade/shadow CTA size; 0 = 128 */
+    uint32_t refill_threshold; /* as in wf_render_config; 0 = 8 */
+    uint32_t longest_first;    /* 1 = start the jobs with the most samples x depth per pixel first */
+} wf_batch_config;
+void wf_batch_config_default(wf_batch_config* config);
+wf_status wf_batch_create(const wf_batch_job* jobs, uint32_t job_count, const wf_batch_config* config,
+                          void* stream, wf_batch** out);
+/* Renders every job's sample range once (one graph launch; asynchronous on
+ * the batch stream), adding to the job framebuffers. */
+wf_status wf_batch_run(wf_batch* batch);
+wf_status wf_batch_synchronize(wf_batch* batch);
+wf_status wf_batch_reset(wf_batch* batch);   /* zero every job framebuffer */
+/* Job framebuffer, width * height * 3 floats (host copy; synchronizes). */
+wf_status wf_batch_download(wf_batch* batch, uint32_t job, float* rgb);
+wf_status wf_batch_framebuffer_device(wf_batch* batch, uint32_t job, float** rgb);
+wf_status wf_batch_stats(wf_batch* batch, wf_render_stats* stats, uint32_t reset);
+wf_status wf_batch_destroy(wf_batch* batch);
+
+/* Autotuner: renders the batch once per candidate (slot capacity x block
+ * size x refill threshold; zero-terminated lists, NULL = defaults), times
+ * each run with CUDA events and writes the fastest configuration to *best.
+ * times_ms (optional) receives one entry per candidate in list order. */
+wf_status wf_batch_autotune(const wf_batch_job* jobs, uint32_t job_count, const uint32_t* slot_capacities,
+                            const uint32_t* block_sizes, const uint32_t* refill_thresholds, void* stream,
+                            wf_batch_config* best, float* times_ms, uint32_t times_capacity);
+
 /* -------------------------------------------------------------- checkpoint */
 /* Checkpoint file: header {magic "PTCHKPT1", version 3, width, height,
  * sampleIndex, fingerprint} + width*height Vec3 (render_checkpoint.cpp:17-63).

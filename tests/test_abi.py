@@ -5,11 +5,13 @@ import re
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 import wfpt
 from wfpt import abi
 
-HEADER = Path(__file__).resolve().parents[1] / "include" / "wavefront.h"
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "wavefront.h"
 
 
 def declared_functions():
@@ -39,6 +41,27 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(abi.SceneDesc) == 128
     assert ctypes.sizeof(abi.RenderConfig) == 116
     assert ctypes.sizeof(abi.Camera) == 56
+
+
+def test_struct_sizes_compiled_from_header(tmp_path):
+    # sizeof of every ctypes mirror against a C compiler reading the header.
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    pairs = {"wf_camera": abi.Camera, "wf_render_config": abi.RenderConfig, "wf_scene_desc": abi.SceneDesc,
+             "wf_kernel_profile": abi.KernelProfile, "wf_render_stats": abi.RenderStats,
+             "wf_batch_job": abi.BatchJob, "wf_batch_config": abi.BatchConfig, "wf_scene_info": abi.SceneInfo,
+             "wf_environment": abi.Environment}
+    src = tmp_path / "sizes.c"
+    body = "".join(f'    printf("%zu\\n", sizeof({name}));\n' for name in pairs)
+    src.write_text('#include <stdio.h>\n#include "wavefront.h"\nint main(void) {\n' + body + "    return 0;\n}\n")
+    exe = tmp_path / "sizes"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    sizes = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    for (name, struct), size in zip(pairs.items(), sizes):
+        assert ctypes.sizeof(struct) == size, name
 
 
 def test_defaults_and_errors_without_gpu():

@@ -1,0 +1,690 @@
+// Job batch: many independent renders (own scene, camera, resolution, depth,
+// sample range) in one captured CUDA graph.
+//
+// Work is a list of (job, pixel) units.  A pool of path slots runs the
+// wavefront stages of the single-scene renderer (lane-refill closest hit,
+// shading with deferred shadow rays, lane-refill occlusion, ordered term
+// accumulation and compaction) inside a device-side WHILE loop.  A slot
+// renders every sample of its unit in sample order, and only then takes
+// the next unit from a device counter, so every pixel adds its samples to
+// its job's framebuffer one after another exactly as a per-job wf_render
+// does: the framebuffers are bit-identical.  Jobs with few pixels or few
+// samples no longer pay per-launch and per-bounce overheads of their own,
+// and the slots of finished jobs immediately work on the others.
+#include "wf_wavefront.cuh"
+#include "wf_lane_traverse.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+namespace wf {
+
+struct BatchJob {
+    DeviceScene scene;
+    RenderParams rp;
+    unsigned long long fb_offset;  // first float of the job framebuffer
+    uint32_t unit_begin;           // first unit (pixel 0) of the job
+    uint32_t pixels;
+    uint32_t sample_start, sample_count;
+};
+
+// Device view of a batch (kernel parameter).
+struct BatchView {
+    const BatchJob* jobs;
+    const uint32_t* unit_job;  // job of each unit
+    uint32_t units;
+    uint32_t* slot_job;
+    uint32_t* slot_unit;
+    uint32_t* slot_sample;     // sample of the slot's path, relative to its job's sample_start
+    float* framebuffer;
+};
+
+}  // namespace wf
+
+struct wf_batch {
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0, sm_count = 148;
+    std::vector<void*> allocations;
+    std::vector<wf_batch_job> jobs;
+    std::vector<unsigned long long> fb_offsets;
+    size_t fb_floats = 0;
+    wf::BatchView view{};
+    wf::BatchJob* jobs_dev = nullptr;
+    uint32_t* unit_job = nullptr;
+    wf::PathSoA paths{};
+    uint32_t* queue[2] = {nullptr, nullptr};
+    float4* hit_a = nullptr;
+    uint32_t* hit_inst = nullptr;
+    float4* terms = nullptr;
+    int4* shade_out = nullptr;
+    float4* shadow_origin = nullptr;
+    float4* shadow_dir = nullptr;
+    uint8_t* shadow_result = nullptr;
+    uint32_t shadow_capacity = 0;
+    wf::Counters* counters = nullptr;
+    uint32_t capacity = 0, units = 0, block = 128, refill = 8, max_depth = 1, max_samples = 1;
+    uint32_t grid_resident[4] = {0, 0, 0, 0};
+    unsigned long long total_paths = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace wf {
+namespace {
+
+#define WF_BATCH_CUDA(call)                                       \
+    do {                                                          \
+        cudaError_t wf_e_ = (call);                               \
+        if (wf_e_ != cudaSuccess) return cuda_fail(wf_e_, #call); \
+    } while (0)
+
+// Starts sample `rel` of `unit` in `slot`.
+WF_DEV void batch_start(const BatchView& b, const PathSoA& ps, uint32_t slot, uint32_t unit, uint32_t rel) {
+    uint32_t job = b.unit_job[unit];
+    const BatchJob& J = b.jobs[job];
+    TileDev tile{0, 0, J.rp.width, J.rp.height, 0};
+    Path path;
+    init_path(J.rp, tile, J.sample_start + rel, unit - J.unit_begin, path);
+    store_path(ps, slot, path);
+    ps.radiance[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    b.slot_job[slot] = job;
+    b.slot_unit[slot] = unit;
+    b.slot_sample[slot] = rel;
+}
+
+__global__ void k_batch_raygen(BatchView b, Counters* c, PathSoA ps, uint32_t* queue, uint32_t capacity,
+                               unsigned long long total_paths) {
+    count_launch(c);
+    uint32_t n = min(capacity, b.units);
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) {
+        c->queue_count[0] = n;
+        c->next_unit = n;
+        c->paths += total_paths;
+        c->work_trace = 0;
+        c->stream_iterations = 0;
+    }
+    for (uint32_t slot = gid; slot < n; slot += gridDim.x * blockDim.x) {
+        batch_start(b, ps, slot, slot, 0);
+        queue[slot] = slot;
+    }
+}
+
+template <typename Tally>
+__global__ void k_batch_trace(BatchView b, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
+                              uint32_t* hit_inst, Counters* c, uint32_t refill_at) {
+    count_launch(c);
+    uint32_t n = *count;
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) {
+        c->shadow_count = 0;
+        c->gather_count = 0;
+        c->work_shade = 0;
+        c->extension_rays += n;
+    }
+    Tally tally;
+    ClosestLane L;
+    L.stage = kStageDone;
+    const DeviceScene* sp = nullptr;
+    uint32_t i = 0;
+    bool more = true;
+    for (;;) {
+        bool idle = L.stage == kStageDone;
+        uint32_t slot = refill(&c->work_trace, n, idle, refill_at, more);
+        if (slot != kInvalid) {
+            i = slot;
+            uint32_t p = queue[i];
+            sp = &b.jobs[b.slot_job[p]].scene;
+            float4 o = ps.origin[p], d = ps.direction[p];
+            closest_begin(L, *sp, f4xyz(o), f4xyz(d), tally);
+            if (L.stage == kStageDone) {
+                hit_a[i] = make_float4(L.h.t, L.h.u, L.h.v, __uint_as_float(L.h.prim));
+                hit_inst[i] = L.h.inst;
+            }
+        }
+        bool busy = L.stage != kStageDone;
+        if (!__any_sync(0xffffffffu, busy)) {
+            if (!more) break;
+            continue;
+        }
+        if (busy) {
+            closest_step(L, *sp, tally);
+            if (L.stage == kStageDone) {
+                hit_a[i] = make_float4(L.h.t, L.h.u, L.h.v, __uint_as_float(L.h.prim));
+                hit_inst[i] = L.h.inst;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128, 4) k_batch_shade(BatchView b, PathSoA ps, const uint32_t* queue,
+                                                        const uint32_t* count, const float4* hit_a,
+                                                        const uint32_t* hit_inst, float4* terms, int4* shade_out,
+                                                        float4* shadow_origin, float4* shadow_dir,
+                                                        uint32_t shadow_capacity, Counters* c, uint32_t* next_count) {
+    count_launch(c);
+    uint32_t n = *count;
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) {
+        *next_count = 0;
+        c->work_shadow = 0;
+        c->work_gather = 0;
+    }
+    uint32_t base;
+    while (next_chunk(&c->work_shade, n, base)) {
+        uint32_t i = base + (threadIdx.x & 31);
+        if (i >= n) continue;
+        uint32_t p = queue[i];
+        uint32_t job = b.slot_job[p];
+        const BatchJob& J = b.jobs[job];
+        Path path = load_path(ps, p);
+        float4 ha = hit_a[i];
+        SurfaceHit sh;
+        bool did_hit = finish_hit(J.scene, path.origin, path.direction, ha.x, ha.y, ha.z, __float_as_uint(ha.w),
+                                  hit_inst[i], sh);
+        DeferredSink sink{};
+        sink.shadow_origin = shadow_origin;
+        sink.shadow_dir = shadow_dir;
+        sink.shadow_count = &c->shadow_count;
+        sink.shadow_capacity = shadow_capacity;
+        sink.terms = terms + size_t(i) * kMaxTerms;
+        sink.owner = i;
+        sink.tag = job;
+        sink.nterms = 0;
+        sink.kill = kUnconditional;
+        sink.overflow = &c->overflow;
+        bool alive = shade_path(J.scene, J.rp, path, did_hit, sh, sink);
+        if (sink.nterms > kMaxTerms) atomicOr(&c->overflow, 2u);
+        store_path(ps, p, path);
+        shade_out[i] = make_int4(min(sink.nterms, kMaxTerms), sink.kill, alive ? 1 : 0, 0);
+    }
+}
+
+template <typename Tally>
+__global__ void k_batch_shadow(BatchView b, const float4* shadow_origin, const float4* shadow_dir, uint8_t* result,
+                               Counters* c, uint32_t capacity, uint32_t refill_at) {
+    count_launch(c);
+    uint32_t n = min(c->shadow_count, capacity);
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) c->shadow_rays += n;
+    Tally tally;
+    AnyLane L;
+    L.stage = kStageDone;
+    const DeviceScene* sp = nullptr;
+    uint32_t j = 0;
+    bool more = true;
+    for (;;) {
+        bool idle = L.stage == kStageDone;
+        uint32_t slot = refill(&c->work_shadow, n, idle, refill_at, more);
+        if (slot != kInvalid) {
+            j = slot;
+            float4 o = shadow_origin[j], d = shadow_dir[j];
+            sp = &b.jobs[__float_as_uint(d.w)].scene;
+            any_begin(L, *sp, f4xyz(o), f4xyz(d), o.w, tally);
+            if (L.stage == kStageDone) result[j] = L.hit ? 1 : 0;
+        }
+        bool busy = L.stage != kStageDone;
+        if (!__any_sync(0xffffffffu, busy)) {
+            if (!more) break;
+            continue;
+        }
+        if (busy) {
+            any_step(L, *sp, tally);
+            if (L.stage == kStageDone) result[j] = L.hit ? 1 : 0;
+        }
+    }
+}
+
+// Term accumulation, kill rule and compaction as in the single-scene
+// finalize; an ended path adds to its job framebuffer, then its slot starts
+// the unit's next sample or, when the unit is done, the next unit.
+__global__ void k_batch_finalize(BatchView b, PathSoA ps, const uint32_t* queue, const uint32_t* count,
+                                 const float4* terms, const int4* shade_out, const uint8_t* shadow_result,
+                                 uint32_t* next, uint32_t* next_count, uint32_t capacity, Counters* c) {
+    count_launch(c);
+    uint32_t n = *count;
+    uint32_t lane = threadIdx.x & 31;
+    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) c->work_trace = 0;
+    for (uint32_t base = warp * 32; base < n; base += warps * 32) {
+        uint32_t i = base + lane;
+        bool alive = false, need_unit = false;
+        uint32_t p = 0;
+        if (i < n) {
+            p = queue[i];
+            int4 so = shade_out[i];
+            float4 r = ps.radiance[p];
+            V3 rad = f4xyz(r);
+            for (int k = 0; k < so.x; ++k) {
+                float4 t = terms[size_t(i) * kMaxTerms + k];
+                int h = __float_as_int(t.w);
+                if (h < 0 || !shadow_result[h]) rad += f4xyz(t);
+            }
+            alive = so.z != 0 && !(so.y >= 0 && !shadow_result[so.y]);
+            if (alive) {
+                ps.radiance[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+            } else {
+                const BatchJob& J = b.jobs[b.slot_job[p]];
+                float* f = b.framebuffer + J.fb_offset + 3 * size_t(ps.info[p].x);
+                f[0] += rad.x;
+                f[1] += rad.y;
+                f[2] += rad.z;
+                uint32_t started = b.slot_sample[p] + 1;
+                if (started < J.sample_count) {
+                    batch_start(b, ps, p, b.slot_unit[p], started);
+                    alive = true;
+                } else {
+                    need_unit = true;
+                }
+            }
+        }
+        unsigned want = __ballot_sync(0xffffffffu, need_unit);
+        if (want) {
+            uint32_t first = 0;
+            if (lane == 0) first = atomicAdd(&c->next_unit, uint32_t(__popc(want)));
+            first = __shfl_sync(0xffffffffu, first, 0);
+            if (need_unit) {
+                uint32_t unit = first + __popc(want & ((1u << lane) - 1u));
+                if (unit < b.units) {
+                    batch_start(b, ps, p, unit, 0);
+                    alive = true;
+                }
+            }
+        }
+        unsigned mask = __ballot_sync(0xffffffffu, alive);
+        uint32_t out = 0;
+        if (lane == 0 && mask) out = atomicAdd(next_count, uint32_t(__popc(mask)));
+        out = __shfl_sync(0xffffffffu, out, 0);
+        uint32_t rank = __popc(mask & ((1u << lane) - 1u));
+        if (alive && out + rank < capacity) next[out + rank] = p;
+    }
+}
+
+// Loop condition with a hard bound (every slot runs at most
+// units * max_samples * max_depth bounces in total).
+__global__ void k_batch_condition(cudaGraphConditionalHandle handle, Counters* c, unsigned long long bound) {
+    count_launch(c);
+    uint32_t it = ++c->stream_iterations;
+    bool live = c->queue_count[0] > 0;
+    if (live && it >= bound) {
+        c->error = kErrorStreamBound;
+        live = false;
+    }
+    cudaGraphSetConditional(handle, live ? 1u : 0u);
+}
+
+template <typename T>
+cudaError_t batch_alloc(wf_batch* b, T** p, size_t count) {
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * std::max<size_t>(count, 1));
+    if (e == cudaSuccess) b->allocations.push_back(*p);
+    return e;
+}
+
+uint32_t batch_grid(const wf_batch* b, int kernel, uint32_t work, uint32_t block) {
+    uint32_t g = std::max(1u, (work + block - 1) / block);
+    return b->grid_resident[kernel] ? std::min(g, b->grid_resident[kernel]) : g;
+}
+
+template <typename K>
+cudaError_t batch_resident(wf_batch* b, int kernel, K* fn, uint32_t block) {
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, int(block), 0);
+    if (e == cudaSuccess) b->grid_resident[kernel] = uint32_t(std::max(per_sm, 1)) * uint32_t(b->sm_count);
+    return e;
+}
+
+wf_status capture_batch(wf_batch* b) {
+    cudaStream_t st = b->stream;
+    uint32_t cap = b->capacity;
+    WF_BATCH_CUDA(cudaGraphCreate(&b->graph, 0));
+    WF_BATCH_CUDA(cudaStreamBeginCaptureToGraph(st, b->graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    k_batch_raygen<<<std::max(1u, std::min((cap + 255) / 256, uint32_t(b->sm_count) * 16)), 256, 0, st>>>(
+        b->view, b->counters, b->paths, b->queue[0], cap, b->total_paths);
+    cudaGraph_t captured = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &captured);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (batch prologue)");
+    size_t nodes = 0;
+    WF_BATCH_CUDA(cudaGraphGetNodes(b->graph, nullptr, &nodes));
+    if (nodes != 1) return fail(WF_ERR_CUDA, "unexpected batch prologue graph (%zu nodes)", nodes);
+    cudaGraphNode_t raygen_node = nullptr;
+    WF_BATCH_CUDA(cudaGraphGetNodes(b->graph, &raygen_node, &nodes));
+
+    cudaGraphConditionalHandle handle;
+    WF_BATCH_CUDA(cudaGraphConditionalHandleCreate(&handle, b->graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t loop_node = nullptr;
+    WF_BATCH_CUDA(cudaGraphAddNode(&loop_node, b->graph, &raygen_node, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+
+    WF_BATCH_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    for (uint32_t cur = 0; cur < 2; ++cur) {
+        uint32_t nxt = cur ^ 1;
+        uint32_t* cur_count = &b->counters->queue_count[cur];
+        uint32_t* next_count = &b->counters->queue_count[nxt];
+        k_batch_trace<NoTally><<<batch_grid(b, 0, cap, b->block), b->block, 0, st>>>(
+            b->view, b->paths, b->queue[cur], cur_count, b->hit_a, b->hit_inst, b->counters, b->refill);
+        k_batch_shade<<<batch_grid(b, 1, cap, 128), 128, 0, st>>>(
+            b->view, b->paths, b->queue[cur], cur_count, b->hit_a, b->hit_inst, b->terms, b->shade_out,
+            b->shadow_origin, b->shadow_dir, b->shadow_capacity, b->counters, next_count);
+        k_batch_shadow<NoTally><<<batch_grid(b, 2, b->shadow_capacity, b->block), b->block, 0, st>>>(
+            b->view, b->shadow_origin, b->shadow_dir, b->shadow_result, b->counters, b->shadow_capacity, b->refill);
+        k_batch_finalize<<<batch_grid(b, 3, cap, 256), 256, 0, st>>>(
+            b->view, b->paths, b->queue[cur], cur_count, b->terms, b->shade_out, b->shadow_result, b->queue[nxt],
+            next_count, cap, b->counters);
+    }
+    unsigned long long bound = (unsigned long long)b->units * b->max_samples * b->max_depth / 2 + 2;
+    k_batch_condition<<<1, 1, 0, st>>>(handle, b->counters, bound);
+    e = cudaStreamEndCapture(st, &captured);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (batch body)");
+    WF_BATCH_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    return WF_OK;
+}
+
+wf_status validate_job(const wf_batch_job& j, uint32_t index) {
+    const wf_render_config& c = j.config;
+    if (!j.scene) return fail(WF_ERR_INVALID_ARG, "batch job %u: null scene", index);
+    if (!std::isfinite(c.indirect_clamp) || c.indirect_clamp < 0.0f)
+        return fail(WF_ERR_INVALID_ARG, "batch job %u: indirect radiance clamp must be finite and nonnegative", index);
+    if (c.width == 0 || c.height == 0) return fail(WF_ERR_INVALID_ARG, "batch job %u: empty image", index);
+    if (c.max_depth == 0 || c.max_depth > kMaxBounces)
+        return fail(WF_ERR_INVALID_ARG, "batch job %u: maximum depth must be in [1, %d]", index, kMaxBounces);
+    if (c.rng > WF_RNG_PCG32 || c.debug > WF_DEBUG_SHADING_NORMAL)
+        return fail(WF_ERR_INVALID_ARG, "batch job %u: unknown rng strategy or debug view", index);
+    if (c.caustics) return fail(WF_ERR_UNSUPPORTED, "batch job %u: caustics are not supported in a batch", index);
+    if (j.sample_count == 0) return fail(WF_ERR_INVALID_ARG, "batch job %u: empty sample range", index);
+    const DeviceScene& v = j.scene->view;
+    if (v.punctual_count - v.directional_count > 0 && v.directional_count > 2)
+        return fail(WF_ERR_UNSUPPORTED, "batch job %u: more than two directional lights", index);
+    return WF_OK;
+}
+
+RenderParams job_params(const wf_batch_job& j) {
+    const wf_render_config& c = j.config;
+    const wf_camera* camera = &j.camera;
+    RenderParams rp{};
+    rp.width = c.width;
+    rp.height = c.height;
+    rp.max_depth = c.max_depth;
+    rp.rr_start = c.rr_start_depth;
+    rp.rng = c.rng;
+    rp.debug = c.debug;
+    rp.clamp = c.indirect_clamp;
+    rp.gather_radius = c.gather_radius;
+    rp.camera.position = V3{camera->position[0], camera->position[1], camera->position[2]};
+    rp.camera.forward = V3{camera->forward[0], camera->forward[1], camera->forward[2]};
+    rp.camera.right = V3{camera->right[0], camera->right[1], camera->right[2]};
+    rp.camera.up = V3{camera->up[0], camera->up[1], camera->up[2]};
+    rp.camera.aspect_ratio = camera->aspect_ratio;
+    rp.camera.tan_half_fov = wfm::tanf(camera->vertical_fov * 0.5f);
+    rp.photons = PhotonGridView{};
+    return rp;
+}
+
+wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_config* cfg, void* stream,
+                       wf_batch** out) {
+    if (!jobs || !out || count == 0) return fail(WF_ERR_INVALID_ARG, "empty batch");
+    *out = nullptr;
+    wf_batch_config config;
+    wf_batch_config_default(&config);
+    if (cfg) config = *cfg;
+    if (config.block_size > 1024 || (config.block_size && config.block_size % 32))
+        return fail(WF_ERR_INVALID_ARG, "batch block size must be a multiple of 32 up to 1024");
+    if (config.refill_threshold > 32) return fail(WF_ERR_INVALID_ARG, "refill threshold must be between 0 and 32");
+    for (uint32_t i = 0; i < count; ++i)
+        if (wf_status e = validate_job(jobs[i], i)) return e;
+
+    auto b = std::make_unique<wf_batch>();
+    wf_batch* bp = b.get();
+    b->jobs.assign(jobs, jobs + count);
+    b->block = config.block_size ? config.block_size : 128u;
+    b->refill = config.refill_threshold ? config.refill_threshold : 8u;
+
+    // Unit order: job by job, in the given order or longest per-pixel work first.
+    std::vector<uint32_t> order(count);
+    std::iota(order.begin(), order.end(), 0u);
+    if (config.longest_first)
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) {
+            return uint64_t(jobs[a].sample_count) * jobs[a].config.max_depth >
+                   uint64_t(jobs[c].sample_count) * jobs[c].config.max_depth;
+        });
+    std::vector<BatchJob> host(count);
+    std::vector<uint32_t> unit_job;
+    uint64_t units = 0, fb = 0, max_directional = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const wf_batch_job& j = jobs[i];
+        uint64_t pixels = uint64_t(j.config.width) * j.config.height;
+        host[i].scene = j.scene->view;
+        host[i].rp = job_params(j);
+        host[i].fb_offset = fb;
+        host[i].pixels = uint32_t(pixels);
+        host[i].sample_start = j.sample_start;
+        host[i].sample_count = j.sample_count;
+        b->fb_offsets.push_back(fb);
+        fb += 3 * pixels;
+        b->total_paths += pixels * j.sample_count;
+        b->max_depth = std::max(b->max_depth, j.config.max_depth);
+        b->max_samples = std::max(b->max_samples, j.sample_count);
+        max_directional = std::max<uint64_t>(max_directional, j.scene->view.directional_count);
+    }
+    for (uint32_t job : order) {
+        uint64_t pixels = host[job].pixels;
+        host[job].unit_begin = uint32_t(units);
+        units += pixels;
+        if (units > 0xffffffffull) return fail(WF_ERR_INVALID_ARG, "batch has more than 2^32 pixels");
+        unit_job.insert(unit_job.end(), size_t(pixels), job);
+    }
+    b->units = uint32_t(units);
+    b->fb_floats = fb;
+    uint64_t cap = config.slot_capacity ? config.slot_capacity : std::min<uint64_t>(units, 4u << 20);
+    b->capacity = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(cap, units)));
+
+    WF_BATCH_CUDA(cudaGetDevice(&b->device));
+    WF_BATCH_CUDA(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, b->device));
+    if (stream) {
+        b->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        WF_BATCH_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        b->own_stream = true;
+    }
+    uint32_t c = b->capacity;
+    WF_BATCH_CUDA(batch_alloc(bp, &b->jobs_dev, count));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->unit_job, units));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->view.framebuffer, fb));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->view.slot_job, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->view.slot_unit, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->view.slot_sample, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->paths.origin, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->paths.direction, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->paths.throughput, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->paths.radiance, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->paths.info, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->paths.rng, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->queue[0], c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->queue[1], c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->hit_a, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->hit_inst, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->terms, size_t(c) * kMaxTerms));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->shade_out, c));
+    uint64_t shadow = uint64_t(c) * (5u + max_directional);
+    b->shadow_capacity = uint32_t(std::min<uint64_t>(shadow, 0xffffffffull));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->shadow_origin, b->shadow_capacity));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->shadow_dir, b->shadow_capacity));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->shadow_result, b->shadow_capacity));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->counters, 1));
+    WF_BATCH_CUDA(cudaMemcpyAsync(b->jobs_dev, host.data(), sizeof(BatchJob) * count, cudaMemcpyHostToDevice,
+                                  b->stream));
+    WF_BATCH_CUDA(cudaMemcpyAsync(b->unit_job, unit_job.data(), sizeof(uint32_t) * units, cudaMemcpyHostToDevice,
+                                  b->stream));
+    WF_BATCH_CUDA(cudaMemsetAsync(b->view.framebuffer, 0, sizeof(float) * fb, b->stream));
+    WF_BATCH_CUDA(cudaMemsetAsync(b->counters, 0, sizeof(Counters), b->stream));
+    b->paths.slot_sample = nullptr;
+    b->view.jobs = b->jobs_dev;
+    b->view.unit_job = b->unit_job;
+    b->view.units = b->units;
+    WF_BATCH_CUDA(batch_resident(bp, 0, k_batch_trace<NoTally>, b->block));
+    WF_BATCH_CUDA(batch_resident(bp, 1, k_batch_shade, 128));
+    WF_BATCH_CUDA(batch_resident(bp, 2, k_batch_shadow<NoTally>, b->block));
+    WF_BATCH_CUDA(batch_resident(bp, 3, k_batch_finalize, 256));
+    if (wf_status e = capture_batch(bp)) return e;
+    WF_BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    *out = b.release();
+    return WF_OK;
+}
+
+wf_status batch_destroy(wf_batch* b) {
+    if (!b) return WF_OK;
+    cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (void* p : b->allocations) cudaFree(p);
+    if (b->own_stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return WF_OK;
+}
+
+}  // namespace
+}  // namespace wf
+
+using namespace wf;
+
+extern "C" void wf_batch_config_default(wf_batch_config* config) {
+    if (!config) return;
+    std::memset(config, 0, sizeof(*config));
+    config->longest_first = 1;
+}
+
+extern "C" wf_status wf_batch_create(const wf_batch_job* jobs, uint32_t job_count, const wf_batch_config* config,
+                                     void* stream, wf_batch** out) {
+    wf_batch* b = nullptr;
+    wf_status e = batch_create(jobs, job_count, config, stream, &b);
+    if (e != WF_OK) return e;
+    *out = b;
+    return WF_OK;
+}
+
+extern "C" wf_status wf_batch_run(wf_batch* b) {
+    if (!b) return fail(WF_ERR_INVALID_ARG, "null batch");
+    WF_BATCH_CUDA(cudaGraphLaunch(b->exec, b->stream));
+    return WF_OK;
+}
+
+extern "C" wf_status wf_batch_synchronize(wf_batch* b) {
+    if (!b) return fail(WF_ERR_INVALID_ARG, "null batch");
+    WF_BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    uint32_t flags[2] = {0, 0};
+    WF_BATCH_CUDA(cudaMemcpyAsync(&flags[0], &b->counters->overflow, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  b->stream));
+    WF_BATCH_CUDA(cudaMemcpyAsync(&flags[1], &b->counters->error, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  b->stream));
+    WF_BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    if (flags[1]) return fail(WF_ERR_TIMEOUT, "batch loop exceeded its iteration bound");
+    if (flags[0]) return fail(WF_ERR_CAPACITY, "shadow queue or term buffer overflow (flags %u)", flags[0]);
+    return WF_OK;
+}
+
+extern "C" wf_status wf_batch_reset(wf_batch* b) {
+    if (!b) return fail(WF_ERR_INVALID_ARG, "null batch");
+    WF_BATCH_CUDA(cudaMemsetAsync(b->view.framebuffer, 0, sizeof(float) * b->fb_floats, b->stream));
+    return WF_OK;
+}
+
+extern "C" wf_status wf_batch_download(wf_batch* b, uint32_t job, float* rgb) {
+    if (!b || !rgb) return fail(WF_ERR_INVALID_ARG, "null argument");
+    if (job >= b->jobs.size()) return fail(WF_ERR_INVALID_ARG, "batch job %u out of range", job);
+    const wf_render_config& c = b->jobs[job].config;
+    WF_BATCH_CUDA(cudaMemcpyAsync(rgb, b->view.framebuffer + b->fb_offsets[job],
+                                  sizeof(float) * 3 * size_t(c.width) * c.height, cudaMemcpyDeviceToHost, b->stream));
+    return wf_batch_synchronize(b);
+}
+
+extern "C" wf_status wf_batch_framebuffer_device(wf_batch* b, uint32_t job, float** rgb) {
+    if (!b || !rgb) return fail(WF_ERR_INVALID_ARG, "null argument");
+    if (job >= b->jobs.size()) return fail(WF_ERR_INVALID_ARG, "batch job %u out of range", job);
+    *rgb = b->view.framebuffer + b->fb_offsets[job];
+    return WF_OK;
+}
+
+extern "C" wf_status wf_batch_stats(wf_batch* b, wf_render_stats* stats, uint32_t reset) {
+    if (!b || !stats) return fail(WF_ERR_INVALID_ARG, "null argument");
+    unsigned long long v[4];
+    WF_BATCH_CUDA(cudaMemcpyAsync(v, &b->counters->extension_rays, sizeof(v), cudaMemcpyDeviceToHost, b->stream));
+    WF_BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    stats->extension_rays = v[0];
+    stats->shadow_rays = v[1];
+    stats->paths = v[2];
+    stats->kernel_launches = v[3];
+    if (reset) {
+        WF_BATCH_CUDA(cudaMemsetAsync(&b->counters->extension_rays, 0, sizeof(v), b->stream));
+        WF_BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    }
+    return WF_OK;
+}
+
+extern "C" wf_status wf_batch_destroy(wf_batch* b) { return batch_destroy(b); }
+
+extern "C" wf_status wf_batch_autotune(const wf_batch_job* jobs, uint32_t job_count, const uint32_t* slot_capacities,
+                                       const uint32_t* block_sizes, const uint32_t* refill_thresholds, void* stream,
+                                       wf_batch_config* best, float* times_ms, uint32_t times_capacity) {
+    if (!best) return fail(WF_ERR_INVALID_ARG, "null result");
+    static const uint32_t kCaps[] = {0, 0};
+    static const uint32_t kBlocks[] = {128, 0};
+    static const uint32_t kRefills[] = {8, 0};
+    const uint32_t* caps = slot_capacities ? slot_capacities : kCaps;
+    const uint32_t* blocks = block_sizes ? block_sizes : kBlocks;
+    const uint32_t* refills = refill_thresholds ? refill_thresholds : kRefills;
+    auto list = [](const uint32_t* l, bool zero_ok) {
+        std::vector<uint32_t> v;
+        if (zero_ok && l[0] == 0) return std::vector<uint32_t>{0u};
+        for (; *l; ++l) v.push_back(*l);
+        return v;
+    };
+    std::vector<uint32_t> cap_list = list(caps, true), block_list = list(blocks, false),
+                          refill_list = list(refills, false);
+    if (block_list.empty() || refill_list.empty()) return fail(WF_ERR_INVALID_ARG, "empty candidate list");
+    float best_ms = 0.0f;
+    uint32_t index = 0;
+    bool have = false;
+    for (uint32_t cap : cap_list)
+        for (uint32_t block : block_list)
+            for (uint32_t refill_at : refill_list) {
+                wf_batch_config cfg;
+                wf_batch_config_default(&cfg);
+                cfg.slot_capacity = cap;
+                cfg.block_size = block;
+                cfg.refill_threshold = refill_at;
+                wf_batch* b = nullptr;
+                if (wf_status e = batch_create(jobs, job_count, &cfg, stream, &b)) return e;
+                cudaEvent_t e0 = nullptr, e1 = nullptr;
+                float ms = 0.0f;
+                cudaError_t err = cudaEventCreate(&e0);
+                if (err == cudaSuccess) err = cudaEventCreate(&e1);
+                if (err == cudaSuccess) err = cudaEventRecord(e0, b->stream);
+                if (err == cudaSuccess) err = cudaGraphLaunch(b->exec, b->stream);
+                if (err == cudaSuccess) err = cudaEventRecord(e1, b->stream);
+                if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+                if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+                if (e0) cudaEventDestroy(e0);
+                if (e1) cudaEventDestroy(e1);
+                wf_status sync = err == cudaSuccess ? wf_batch_synchronize(b) : cuda_fail(err, "autotune run");
+                batch_destroy(b);
+                if (sync != WF_OK) return sync;
+                if (times_ms && index < times_capacity) times_ms[index] = ms;
+                ++index;
+                if (!have || ms < best_ms) {
+                    have = true;
+                    best_ms = ms;
+                    *best = cfg;
+                }
+            }
+    return WF_OK;
+}

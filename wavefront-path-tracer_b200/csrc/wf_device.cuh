@@ -24,7 +24,7 @@
 #define WF_DEV __device__ __forceinline__
 #define WF_HDI __host__ __device__ __forceinline__
 // Large shading helpers called from several sites: one out-of-line copy.
-#define WF_CALL __device__ __noinline__
+#define WF_CALL static __device__ __noinline__
 #else
 #define WF_DEV inline
 #define WF_HDI inline

@@ -160,6 +160,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ Device
         sink.shadow_capacity = shadow_capacity;
         sink.terms = terms + size_t(i) * kMaxTerms;
         sink.owner = i;
+        sink.tag = i;
         sink.nterms = 0;
         sink.kill = kUnconditional;
         sink.overflow = &c->overflow;

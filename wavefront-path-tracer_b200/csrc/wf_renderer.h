@@ -38,6 +38,7 @@ struct Counters {
     uint32_t stream_iterations;  // streaming mode: loop iterations of the current launch
     uint32_t gather_count;       // caustic gather requests of the current bounce
     uint32_t work_gather;
+    uint32_t next_unit;          // job batch: next (job, pixel) unit to start
     unsigned long long extension_rays;
     unsigned long long shadow_rays;
     unsigned long long paths;

@@ -518,6 +518,7 @@ struct DeferredSink {
     // terms of this path (queue position)
     float4* terms;           // kMaxTerms per queue entry: rgb, handle bits
     uint32_t owner;
+    uint32_t tag;            // stored with each shadow request (the batch's job index)
     int nterms;
     int kill;
     uint32_t* overflow;
@@ -534,7 +535,7 @@ struct DeferredSink {
             return kUnconditional;
         }
         shadow_origin[slot] = make_float4(o.x, o.y, o.z, t_max);
-        shadow_dir[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(owner));
+        shadow_dir[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(tag));
         return int(slot);
     }
     WF_DEV bool may_be_visible(int) const { return true; }

@@ -109,6 +109,16 @@ class RenderConfig(C.Structure):
     ]
 
 
+class BatchJob(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", Camera), ("config", RenderConfig),
+                ("sample_start", C.c_uint32), ("sample_count", C.c_uint32)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("slot_capacity", C.c_uint32), ("block_size", C.c_uint32), ("refill_threshold", C.c_uint32),
+                ("longest_first", C.c_uint32)]
+
+
 PROFILE_BOUNCES = 32
 KERNEL_NAMES = ["raygen", "trace", "shade", "shadow", "finalize", "persistent", "gather"]
 
@@ -149,6 +159,16 @@ def declare(lib):
         "wf_renderer_destroy": (S, [P]),
         "wf_render": (S, [P, U32, U32, U32, U32, U32, U32, U32]),
         "wf_render_frame": (S, [P, U32]),
+        "wf_batch_config_default": (None, [C.POINTER(BatchConfig)]),
+        "wf_batch_create": (S, [C.POINTER(BatchJob), U32, C.POINTER(BatchConfig), P, C.POINTER(P)]),
+        "wf_batch_run": (S, [P]),
+        "wf_batch_synchronize": (S, [P]),
+        "wf_batch_reset": (S, [P]),
+        "wf_batch_download": (S, [P, U32, P]),
+        "wf_batch_framebuffer_device": (S, [P, U32, C.POINTER(P)]),
+        "wf_batch_stats": (S, [P, C.POINTER(RenderStats), U32]),
+        "wf_batch_destroy": (S, [P]),
+        "wf_batch_autotune": (S, [C.POINTER(BatchJob), U32, P, P, P, P, C.POINTER(BatchConfig), P, U32]),
         "wf_render_tile_static": (S, [P, C.POINTER(Camera), C.POINTER(RenderConfig), U32, U32, U32, U32, U32, U32, P,
                                       P]),
         "wf_framebuffer_reset": (S, [P]),

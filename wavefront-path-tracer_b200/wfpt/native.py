@@ -335,3 +335,86 @@ class Renderer:
         s = C.c_uint32()
         check(library().wf_checkpoint_load(self.handle, os.fsencode(path), fingerprint, C.byref(s)))
         return s.value
+
+
+class Batch:
+    """Many render jobs in one captured graph (wf_batch_*).  `jobs` is a list
+    of dicts: scene (DeviceScene), camera (camera dict), config
+    (render_config), sample_start, sample_count."""
+
+    def __init__(self, jobs, slot_capacity=0, block_size=0, refill_threshold=0, longest_first=True, stream=None,
+                 config=None):
+        arr = (abi.BatchJob * len(jobs))()
+        self.jobs = list(jobs)
+        for i, j in enumerate(jobs):
+            arr[i].scene = j["scene"].handle
+            arr[i].camera = camera_struct(j["camera"])
+            arr[i].config = j["config"]
+            arr[i].sample_start = j.get("sample_start", 0)
+            arr[i].sample_count = j["sample_count"]
+        self._arr = arr
+        if config is None:
+            config = abi.BatchConfig()
+            library().wf_batch_config_default(C.byref(config))
+            config.slot_capacity = slot_capacity
+            config.block_size = block_size
+            config.refill_threshold = refill_threshold
+            config.longest_first = int(longest_first)
+        self.config = config
+        handle = C.c_void_p()
+        check(library().wf_batch_create(arr, len(jobs), C.byref(config), stream, C.byref(handle)))
+        self.handle = handle
+
+    def close(self):
+        if getattr(self, "handle", None):
+            library().wf_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self):
+        check(library().wf_batch_run(self.handle))
+
+    def synchronize(self):
+        check(library().wf_batch_synchronize(self.handle))
+
+    def reset(self):
+        check(library().wf_batch_reset(self.handle))
+
+    def download(self, job):
+        cfg = self.jobs[job]["config"]
+        out = np.empty((cfg.height, cfg.width, 3), np.float32)
+        check(library().wf_batch_download(self.handle, job, out.ctypes.data))
+        return out
+
+    def stats(self, reset=False):
+        s = abi.RenderStats()
+        check(library().wf_batch_stats(self.handle, C.byref(s), int(reset)))
+        return {"extension_rays": s.extension_rays, "shadow_rays": s.shadow_rays, "paths": s.paths,
+                "kernel_launches": s.kernel_launches}
+
+    @staticmethod
+    def autotune(jobs, slot_capacities=(0,), block_sizes=(128,), refill_thresholds=(8,), stream=None):
+        """wf_batch_autotune: times one run per candidate, returns (best
+        BatchConfig, list of candidate times in ms)."""
+        arr = (abi.BatchJob * len(jobs))()
+        for i, j in enumerate(jobs):
+            arr[i].scene = j["scene"].handle
+            arr[i].camera = camera_struct(j["camera"])
+            arr[i].config = j["config"]
+            arr[i].sample_start = j.get("sample_start", 0)
+            arr[i].sample_count = j["sample_count"]
+
+        def zlist(v):
+            a = (C.c_uint32 * (len(v) + 1))(*v, 0)
+            return a
+        caps, blocks, refills = zlist(slot_capacities), zlist(block_sizes), zlist(refill_thresholds)
+        n = max(1, len(slot_capacities)) * len(block_sizes) * len(refill_thresholds)
+        times = (C.c_float * n)()
+        best = abi.BatchConfig()
+        check(library().wf_batch_autotune(arr, len(jobs), caps, blocks, refills, stream, C.byref(best), times, n))
+        return best, list(times)

@@ -429,6 +429,37 @@ wf_status wf_batch_autotune(const wf_batch_job* jobs, uint32_t job_count, const 
                             const uint32_t* block_sizes, const uint32_t* refill_thresholds, void* stream,
                             wf_batch_config* best, float* times_ms, uint32_t times_capacity);
 
+/* ----------------------------------------------------------- differentiable */
+/* Path-replay adjoint renderer (no counterpart in the reference).  Its own
+ * material model: every non-emissive triangle has an Oren-Nayar BRDF with
+ * RGB albedo and roughness (radians) read from caller arrays indexed by the
+ * triangle's index in its mesh or triangle list; emissive materials emit
+ * emission * emission_scale.  Next-event estimation over the triangle
+ * lights, cosine-sampled continuations, no Russian roulette, no clamp.
+ * image = emission_scale / spp * sum of path radiance (RGB floats, full
+ * width x height layout; only the crop is written).  Sampling never depends
+ * on the parameters, so wf_diff_backward returns, for each path, the exact
+ * derivative of its estimate: it replays each path from its RNG key (no
+ * path storage, memory O(pixels)) and ADDS dLoss/dparameter to the double
+ * gradient arrays.  All pointers are device pointers; both calls
+ * synchronize `stream`. */
+typedef struct wf_diff_config {
+    uint32_t width, height;     /* image (camera aspect and pixel RNG index) */
+    uint32_t crop_x, crop_y, crop_width, crop_height;  /* 0 width/height = whole image */
+    uint32_t spp;
+    uint32_t sample_start;      /* absolute first sample */
+    uint32_t max_depth;         /* path vertices */
+    uint32_t rng;               /* WF_RNG_* */
+    uint32_t parameter_count;   /* triangles with parameters (albedo has 3 x this many floats) */
+} wf_diff_config;
+wf_status wf_diff_forward(const wf_scene* scene, const wf_camera* camera, const wf_diff_config* config,
+                          const float* albedo, const float* roughness, float emission_scale, float* image,
+                          void* stream);
+wf_status wf_diff_backward(const wf_scene* scene, const wf_camera* camera, const wf_diff_config* config,
+                           const float* albedo, const float* roughness, float emission_scale,
+                           const float* d_image, double* d_albedo, double* d_roughness,
+                           double* d_emission_scale, void* stream);
+
 /* -------------------------------------------------------------- checkpoint */
 /* Checkpoint file: header {magic "PTCHKPT1", version 3, width, height,
  * sampleIndex, fingerprint} + width*height Vec3 (render_checkpoint.cpp:17-63).

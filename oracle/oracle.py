@@ -177,6 +177,8 @@ def port_lib(det=False):
         lib.oracle_photons.argtypes = [P, P, P]
         lib.oracle_render.restype = I
         lib.oracle_render.argtypes = [P, P, P, U32, U32, U32, U32, U32, U32, P, P, I]
+        lib.oracle_diff.restype = I
+        lib.oracle_diff.argtypes = [P, P, P, P, P, C.c_double, P, P, P, P, P, I]
         _port_libs[key] = lib
     return _port_libs[key]
 
@@ -226,6 +228,28 @@ class PortScene:
         rec = np.zeros((config.photon_count, 8), np.float32)
         stored = self.lib.oracle_photons(self.handle, C.addressof(config), rec.ctypes.data)
         return rec, stored
+
+    def diff(self, camera, config, albedo, roughness, emission_scale, d_image=None, threads=0):
+        """FP64 forward (and, with d_image, adjoint) of the differentiable
+        renderer over config's crop: (image (h, w, 3) float64, d_albedo,
+        d_roughness, d_emission_scale)."""
+        from wfpt.native import camera_struct
+        cam = camera_struct(camera)
+        cw = config.crop_width or config.width
+        ch = config.crop_height or config.height
+        albedo = np.ascontiguousarray(albedo, np.float32)
+        roughness = np.ascontiguousarray(roughness, np.float32)
+        image = np.zeros((ch, cw, 3), np.float64)
+        n = config.parameter_count
+        ga, gr, gs = np.zeros((n, 3)), np.zeros(n), np.zeros(1)
+        dimg = None if d_image is None else np.ascontiguousarray(d_image, np.float32)
+        rc = self.lib.oracle_diff(self.handle, C.addressof(cam), C.addressof(config), albedo.ctypes.data,
+                                  roughness.ctypes.data, float(emission_scale),
+                                  dimg.ctypes.data if dimg is not None else None, image.ctypes.data,
+                                  ga.ctypes.data, gr.ctypes.data, gs.ctypes.data, threads)
+        if rc != 0:
+            raise RuntimeError("a hit triangle's parameter index is not below parameter_count")
+        return image, ga, gr, float(gs[0])
 
     def render(self, camera, config, tile=None, sample_start=0, sample_count=1, threads=0):
         from wfpt.native import camera_struct

@@ -1346,6 +1346,147 @@ struct Handle {
     std::string key;
 };
 
+// ------------------------------------------------- FP64 adjoint (test only)
+// Double-precision restatement of the differentiable renderer of
+// wavefront-path-tracer_b200/csrc/wf_adjoint.cu (Oren-Nayar BRDF per
+// triangle, triangle-light next events, cosine continuations).  Every
+// geometric decision (ray directions, hits, shadow rays, RNG draws) is made
+// in float exactly as on the GPU, so both follow the same paths; BRDF
+// values, path weights, terms and gradients are carried in double.
+struct OrenNayarD {
+    double value, d_sigma;
+};
+static OrenNayarD oren_nayar_d(V n, V wo, V wi, double sigma) {
+    double nx = n.x, ny = n.y, nz = n.z;
+    double ci = std::min(1.0, std::max(0.0, nx * wi.x + ny * wi.y + nz * wi.z));
+    double co = std::min(1.0, std::max(0.0, nx * wo.x + ny * wo.y + nz * wo.z));
+    double si = std::sqrt(std::max(0.0, 1.0 - ci * ci)), so = std::sqrt(std::max(0.0, 1.0 - co * co));
+    double g = 0.0;
+    if (si > 1e-4 && so > 1e-4) {
+        double tix = (wi.x - nx * ci) / si, tiy = (wi.y - ny * ci) / si, tiz = (wi.z - nz * ci) / si;
+        double tox = (wo.x - nx * co) / so, toy = (wo.y - ny * co) / so, toz = (wo.z - nz * co) / so;
+        double cphi = std::max(0.0, tix * tox + tiy * toy + tiz * toz);
+        double sin_alpha = ci < co ? si : so;
+        double tan_beta = ci < co ? so / std::max(co, 1e-4) : si / std::max(ci, 1e-4);
+        g = cphi * sin_alpha * tan_beta;
+    }
+    double s2 = sigma * sigma;
+    double a = 1.0 - 0.5 * s2 / (s2 + 0.33), b = 0.45 * s2 / (s2 + 0.09);
+    double da = -0.33 * sigma / ((s2 + 0.33) * (s2 + 0.33)), db = 0.081 * sigma / ((s2 + 0.09) * (s2 + 0.09));
+    return OrenNayarD{a + b * g, da + db * g};
+}
+
+struct D3 {
+    double x = 0, y = 0, z = 0;
+};
+static D3 d3(V v) { return D3{v.x, v.y, v.z}; }
+static D3 dmul(D3 a, D3 b) { return D3{a.x * b.x, a.y * b.y, a.z * b.z}; }
+static D3 dscale(D3 a, double s) { return D3{a.x * s, a.y * s, a.z * s}; }
+static D3 dadd(D3 a, D3 b) { return D3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+static D3 dsub(D3 a, D3 b) { return D3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+static double ddot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+struct DiffCtx {
+    const Scene& s;
+    const wf_diff_config& c;
+    V cam_p, cam_f, cam_r, cam_u;
+    float aspect, tan_half;
+    const float* albedo;
+    const float* rough;
+};
+
+// kAdjoint = false: returns U (path radiance at emission scale 1).
+// kAdjoint = true: adds delta . dU/dtheta into ga/gr and returns U.
+template <bool kAdjoint>
+static D3 diff_path_d(const DiffCtx& x, uint32_t px, uint32_t py, uint32_t sample, D3 total, D3 delta, double* ga,
+                      double* gr, bool& bad) {
+    const Scene& s = x.s;
+    uint32_t pixel = py * x.c.width + px;
+    Rng rng = seed_rng(pixel_key(pixel, sample, x.c.rng), x.c.rng);
+    float u = (float(px) + rng.next()) / float(x.c.width);
+    float v = (float(py) + rng.next()) / float(x.c.height);
+    float cx = (2.0f * u - 1.0f) * x.aspect * x.tan_half;
+    float cy = (1.0f - 2.0f * v) * x.tan_half;
+    Ray r{x.cam_p, unit(add(add(x.cam_f, mul(x.cam_r, cx)), mul(x.cam_u, cy)))};
+    D3 beta{1, 1, 1}, sum;
+    for (uint32_t depth = 0; depth < x.c.max_depth; ++depth) {
+        Best b = closest(s, r);
+        Hit h;
+        if (!finish(s, r, b, h)) break;
+        const Mat& m = s.mats[h.mat];
+        if (m.type == WF_MAT_EMISSIVE) {
+            if (depth == 0) sum = dadd(sum, dmul(beta, d3(m.emission)));
+            break;
+        }
+        if (b.kind == WF_HIT_SPHERE) break;
+        uint32_t k = b.prim;
+        if (k >= x.c.parameter_count) {
+            bad = true;
+            break;
+        }
+        D3 albedo{x.albedo[3 * k], x.albedo[3 * k + 1], x.albedo[3 * k + 2]};
+        double sigma = x.rough[k];
+        V gn = h.gn, n = h.n;
+        if (dot(n, gn) < 0.0f) n = neg(n);
+        V wo = neg(r.d);
+        D3 nee_free;
+        double nee_dsigma = 0.0;
+        if (!s.lights.empty()) {
+            uint32_t nl = uint32_t(s.lights.size());
+            uint32_t cand = std::min(uint32_t(rng.next() * nl), nl - 1);
+            uint32_t li = rng.next() < s.lights[cand].alias_p ? cand : s.lights[cand].alias;
+            const Light& L = s.lights[li];
+            float ru = std::sqrt(rng.next()), lv = rng.next();
+            V lp = add(add(mul(L.a, 1.0f - ru), mul(L.b, ru * (1.0f - lv))), mul(L.c, ru * lv));
+            V to = sub(lp, h.p);
+            float d2 = len2(to), dist = std::sqrt(d2);
+            V wl = divs(to, dist);
+            float cg = dot(gn, wl), cs = dot(n, wl), cl = dot(L.n, neg(wl));
+            if (cg > 0.0f && cs > 0.0f && cl > 0.0f) {
+                V so = nudge(h.p, gn, wl, h.t), st = nudge(lp, L.n, neg(wl), dist);
+                V seg = sub(st, so);
+                float sd = len(seg);
+                if (sd > T_MIN && !blocked(s, Ray{so, divs(seg, sd)}, sd - T_MIN)) {
+                    OrenNayarD on = oren_nayar_d(n, wo, wl, sigma);
+                    double geo = double(cl) * L.area / (double(d2) * L.pdf);
+                    nee_free = dscale(dmul(beta, d3(s.mats[L.mat].emission)), on.value / M_PI * double(cs) * geo);
+                    nee_dsigma = on.value > 0.0 ? on.d_sigma / on.value : 0.0;
+                    sum = dadd(sum, dmul(albedo, nee_free));
+                }
+            }
+        }
+        float u1 = rng.next(), u2 = rng.next();
+        float rad = std::sqrt(u1), phi = 6.28318530718f * u2;
+        float sx = rad * m_cosf(phi), sy = rad * m_sinf(phi), sz = std::sqrt(1.0f - u1);
+        V helper = std::fabs(n.x) > 0.1f ? mk(0, 1, 0) : mk(1, 0, 0);
+        V t = unit(cross(helper, n));
+        V bt = cross(n, t);
+        V wi = unit(add(add(mul(t, sx), mul(bt, sy)), mul(n, sz)));
+        bool continues = depth + 1 < x.c.max_depth && dot(wi, gn) > 0.0f;
+        OrenNayarD on = continues ? oren_nayar_d(n, wo, wi, sigma) : OrenNayarD{0, 0};
+        if (kAdjoint) {
+            D3 after = dsub(total, sum);
+            D3 g;
+            double gs = 0.0;
+            if (continues) {
+                g = D3{albedo.x > 0 ? after.x / albedo.x : 0, albedo.y > 0 ? after.y / albedo.y : 0,
+                       albedo.z > 0 ? after.z / albedo.z : 0};
+                gs = on.value > 0 ? ddot(delta, after) * (on.d_sigma / on.value) : 0.0;
+            }
+            g = dadd(g, nee_free);
+            gs += ddot(delta, dmul(albedo, nee_free)) * nee_dsigma;
+            ga[3 * k] += delta.x * g.x;
+            ga[3 * k + 1] += delta.y * g.y;
+            ga[3 * k + 2] += delta.z * g.z;
+            gr[k] += gs;
+        }
+        if (!continues) break;
+        beta = dmul(beta, dscale(albedo, on.value));
+        r = Ray{nudge(h.p, gn, wi, h.t), wi};
+    }
+    return sum;
+}
+
 }  // namespace port
 
 using namespace port;
@@ -1490,6 +1631,73 @@ int oracle_render(void* handle, const wf_camera* cam, const wf_render_config* c,
     if (counts)
         for (size_t i = 0; i < live.size(); ++i) counts[i] = live[i].load();
     return 0;
+}
+
+
+// FP64 forward and adjoint of the differentiable renderer over the config's
+// crop.  image (optional): crop_height x crop_width x 3 doubles.  d_image
+// (optional, full width x height x 3 floats): dLoss/dImage; gradients are
+// ADDED to d_albedo (3 per parameter), d_roughness, d_scale.
+int oracle_diff(void* handle, const wf_camera* cam, const wf_diff_config* c, const float* albedo,
+                const float* roughness, double emission_scale, const float* d_image, double* image, double* d_albedo,
+                double* d_roughness, double* d_scale, int threads) {
+    Handle* hd = static_cast<Handle*>(handle);
+    DiffCtx x{*hd->scene, *c, mk3(cam->position), mk3(cam->forward), mk3(cam->right), mk3(cam->up),
+              cam->aspect_ratio, m_tanf(cam->vertical_fov * 0.5f), albedo, roughness};
+    uint32_t cw = c->crop_width ? c->crop_width : c->width, ch = c->crop_height ? c->crop_height : c->height;
+    uint32_t pixels = cw * ch, np = c->parameter_count;
+    if (threads <= 0) threads = int(std::max(1u, std::thread::hardware_concurrency()));
+    std::vector<std::vector<double>> ga(threads), gr(threads);
+    std::vector<double> gs(threads, 0.0);
+    std::atomic<uint32_t> next{0};
+    std::atomic<bool> bad{false};
+    auto work = [&](int w) {
+        if (d_image) {
+            ga[w].assign(size_t(np) * 3, 0.0);
+            gr[w].assign(np, 0.0);
+        }
+        for (;;) {
+            uint32_t i = next.fetch_add(1);
+            if (i >= pixels) break;
+            uint32_t px = c->crop_x + i % cw, py = c->crop_y + i / cw;
+            D3 acc;
+            D3 delta, gpix;
+            if (d_image) {
+                const float* g = d_image + 3 * (size_t(py) * c->width + px);
+                gpix = D3{g[0], g[1], g[2]};
+                delta = dscale(gpix, emission_scale / double(c->spp));
+            }
+            bool b = false;
+            for (uint32_t k = 0; k < c->spp; ++k) {
+                uint32_t sample = c->sample_start + k;
+                D3 total = diff_path_d<false>(x, px, py, sample, D3{}, D3{}, nullptr, nullptr, b);
+                acc = dadd(acc, total);
+                if (d_image) {
+                    diff_path_d<true>(x, px, py, sample, total, delta, ga[w].data(), gr[w].data(), b);
+                    gs[w] += ddot(gpix, total) / double(c->spp);
+                }
+            }
+            if (b) bad = true;
+            if (image) {
+                double* o = image + 3 * size_t(i);
+                double sc = emission_scale / double(c->spp);
+                o[0] = acc.x * sc;
+                o[1] = acc.y * sc;
+                o[2] = acc.z * sc;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 0; w < threads; ++w) pool.emplace_back(work, w);
+    for (auto& t : pool) t.join();
+    if (d_image) {
+        for (int w = 0; w < threads; ++w) {
+            for (size_t j = 0; j < size_t(np) * 3; ++j) d_albedo[j] += ga[w][j];
+            for (size_t j = 0; j < np; ++j) d_roughness[j] += gr[w][j];
+            *d_scale += gs[w];
+        }
+    }
+    return bad ? 1 : 0;
 }
 
 }  // extern "C"

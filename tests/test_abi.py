@@ -53,7 +53,7 @@ def test_struct_sizes_compiled_from_header(tmp_path):
     pairs = {"wf_camera": abi.Camera, "wf_render_config": abi.RenderConfig, "wf_scene_desc": abi.SceneDesc,
              "wf_kernel_profile": abi.KernelProfile, "wf_render_stats": abi.RenderStats,
              "wf_batch_job": abi.BatchJob, "wf_batch_config": abi.BatchConfig, "wf_scene_info": abi.SceneInfo,
-             "wf_environment": abi.Environment}
+             "wf_environment": abi.Environment, "wf_diff_config": abi.DiffConfig}
     src = tmp_path / "sizes.c"
     body = "".join(f'    printf("%zu\\n", sizeof({name}));\n' for name in pairs)
     src.write_text('#include <stdio.h>\n#include "wavefront.h"\nint main(void) {\n' + body + "    return 0;\n}\n")

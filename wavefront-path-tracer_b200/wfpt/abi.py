@@ -119,6 +119,13 @@ class BatchConfig(C.Structure):
                 ("longest_first", C.c_uint32)]
 
 
+class DiffConfig(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("crop_x", C.c_uint32), ("crop_y", C.c_uint32),
+                ("crop_width", C.c_uint32), ("crop_height", C.c_uint32), ("spp", C.c_uint32),
+                ("sample_start", C.c_uint32), ("max_depth", C.c_uint32), ("rng", C.c_uint32),
+                ("parameter_count", C.c_uint32)]
+
+
 PROFILE_BOUNCES = 32
 KERNEL_NAMES = ["raygen", "trace", "shade", "shadow", "finalize", "persistent", "gather"]
 
@@ -159,6 +166,8 @@ def declare(lib):
         "wf_renderer_destroy": (S, [P]),
         "wf_render": (S, [P, U32, U32, U32, U32, U32, U32, U32]),
         "wf_render_frame": (S, [P, U32]),
+        "wf_diff_forward": (S, [P, C.POINTER(Camera), C.POINTER(DiffConfig), P, P, F, P, P]),
+        "wf_diff_backward": (S, [P, C.POINTER(Camera), C.POINTER(DiffConfig), P, P, F, P, P, P, P, P]),
         "wf_batch_config_default": (None, [C.POINTER(BatchConfig)]),
         "wf_batch_create": (S, [C.POINTER(BatchJob), U32, C.POINTER(BatchConfig), P, C.POINTER(P)]),
         "wf_batch_run": (S, [P]),

@@ -372,3 +372,86 @@ def large_mesh(width=1920, height=1080, terrain_quads=2236, instance_count=500, 
     s.black_background = False
     cam = look_at_camera((0.0, 14.0, 38.0), (0.0, 0.0, 0.0), 50.0, width, height)
     return s, cam
+
+
+def batch_jobs(count=64, seed=11, min_triangles=5_000, max_triangles=2_000_000, sizes=(64, 128, 256, 512),
+               spps=(4, 16, 64), max_depth=8):
+    """Uneven render jobs for the batch workload: `count` sphere-field jobs
+    drawn from `seed`, each with its own scene seed and a displaced geodesic
+    mesh of log-uniform size in [min_triangles, max_triangles] (20 f^2
+    triangles for frequency f), a square resolution drawn from `sizes`, a
+    sample count drawn from `spps`, and depth `max_depth`.
+    Returns dicts: scene, camera, width, height, spp, max_depth, triangles."""
+    rng = SceneRng(seed)
+    lo, hi = math.log(min_triangles), math.log(max_triangles)
+    jobs = []
+    for _ in range(count):
+        triangles = math.exp(lo + (hi - lo) * rng.next())
+        frequency = max(16, int(round(math.sqrt(triangles / 20.0))))
+        size = sizes[min(int(rng.next() * len(sizes)), len(sizes) - 1)]
+        spp = spps[min(int(rng.next() * len(spps)), len(spps) - 1)]
+        scene_seed = 1 + int(rng.next() * 1_000_000)
+        scene, cam = sphere_field(size, size, frequency=frequency, seed=scene_seed)
+        jobs.append(dict(scene=scene, camera=cam, width=size, height=size, spp=spp, max_depth=max_depth,
+                         triangles=scene.triangle_count()))
+    return jobs
+
+
+def _grid_quad(p0, eu, ev, n, mat):
+    """Quad p0 + [0,1]^2 (eu, ev) split into n x n cells of two triangles each
+    (same diagonal and winding as quad())."""
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    i, j = i.ravel()[:, None], j.ravel()[:, None]
+    p0, eu, ev = (np.asarray(a, np.float64) for a in (p0, eu, ev))
+    a = p0 + eu * (i / n) + ev * (j / n)
+    b = p0 + eu * ((i + 1) / n) + ev * (j / n)
+    c = p0 + eu * ((i + 1) / n) + ev * ((j + 1) / n)
+    d = p0 + eu * (i / n) + ev * ((j + 1) / n)
+    v0 = np.concatenate([a, a], axis=1).reshape(-1, 3)
+    v1 = np.concatenate([b, c], axis=1).reshape(-1, 3)
+    v2 = np.concatenate([c, d], axis=1).reshape(-1, 3)
+    return triangles(v0.astype(np.float32), v1.astype(np.float32), v2.astype(np.float32), mat)
+
+
+def cornell_inverse(width=512, height=512, cells=32):
+    """Cornell box for inverse rendering: each of the 5 walls split into
+    cells x cells quads (2 * cells^2 triangles; 10,240 walls triangles for
+    cells = 32), the two rotated boxes (24 triangles) and the 2-triangle
+    ceiling light (radiance 15), in one mesh.  The mesh index of a triangle is
+    its parameter index for wf_diff_*: walls first, then boxes, then the
+    light.  Returns (scene, camera, parameter_count, light_triangles)."""
+    s = Scene()
+    grey = s.add_material(material(abi.MAT_DIFFUSE, (0.5, 0.5, 0.5)))
+    light = s.add_material(material(abi.MAT_EMISSIVE, (1.0, 1.0, 1.0), (15.0, 15.0, 15.0)))
+    w, fy, cy, bz, fz = 2.5, -1.0, 3.0, -2.5, 2.5
+    walls = [  # (origin, edge u, edge v) with the windings of cornell_box
+        ((-w, fy, fz), (2 * w, 0, 0), (0, 0, bz - fz)),
+        ((-w, cy, bz), (2 * w, 0, 0), (0, 0, fz - bz)),
+        ((-w, fy, bz), (2 * w, 0, 0), (0, cy - fy, 0)),
+        ((-w, fy, fz), (0, 0, bz - fz), (0, cy - fy, 0)),
+        ((w, fy, bz), (0, 0, fz - bz), (0, cy - fy, 0)),
+    ]
+    tris = [_grid_quad(p, u, v, cells, grey) for p, u, v in walls]
+    tris.append(box((0.85, -0.4, 0.55), (1.2, 1.2, 1.2), -18.0, grey))
+    tris.append(box((-0.8, 0.2, -0.65), (1.2, 2.4, 1.2), 18.0, grey))
+    corner, eu, ev = np.array([-0.75, 2.95, -0.75]), np.array([1.5, 0, 0]), np.array([0, 0, 1.5])
+    tris.append(quad(corner, corner + eu, corner + eu + ev, corner + ev, light))
+    mesh = np.concatenate(tris)
+    s.add_mesh(mesh)
+    s.instances = instance(0)
+    s.black_background = True
+    cam = look_at_camera((0.0, 1.2, 6.5), (0.0, 0.8, -0.6), 42.0, width, height)
+    return s, cam, len(mesh), 2
+
+
+def inverse_parameters(scene, parameter_count, seed, albedo_range=(0.15, 0.85), roughness_range=(0.0, 0.8)):
+    """Smooth seeded parameter fields over a mesh's triangle centroids:
+    RGB albedo and Oren-Nayar roughness (radians) per triangle."""
+    mesh = scene.meshes[0]
+    centroid = (mesh["v0"].astype(np.float64) + mesh["v1"] + mesh["v2"]) / 3.0
+    lo, hi = albedo_range
+    albedo = np.stack([lo + (hi - lo) * 0.5 * (1.0 + value_noise(centroid, seed + c, frequency=0.6))
+                       for c in range(3)], axis=1)
+    rlo, rhi = roughness_range
+    rough = rlo + (rhi - rlo) * 0.5 * (1.0 + value_noise(centroid, seed + 17, frequency=0.6))
+    return albedo[:parameter_count].astype(np.float32), rough[:parameter_count].astype(np.float32)

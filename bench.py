@@ -202,13 +202,233 @@ def run_reference(args):
     return 0
 
 
+def run_inverse(args):
+    """Inverse-rendering step on the subdivided Cornell box (10,240 wall
+    triangles, each with RGB albedo and Oren-Nayar roughness, plus boxes and
+    the light's emission scale): 512x512, 32 spp, depth 6, L2 image loss.
+    One step = forward render + path-replay adjoint.  Reports the adjoint /
+    forward time ratio and the peak device memory of the step."""
+    import numpy as np
+    import torch
+    import wfpt
+    from wfpt import diff, scenes
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0  # one GPU: the parameters are shared by every path
+    width = height = 512
+    spp, depth = 32, 6
+    t0 = time.perf_counter()
+    scene, cam, n, _ = scenes.cornell_inverse(width, height, cells=32)
+    gt_a, gt_r = scenes.inverse_parameters(scene, n, seed=101)
+    a0, r0 = scenes.inverse_parameters(scene, n, seed=202)
+    dev = wfpt.DeviceScene(scene)
+    cfg = diff.diff_config(width, height, spp, depth, n)
+    A = torch.from_numpy(a0).cuda()
+    R = torch.from_numpy(r0).cuda()
+    target = diff.forward(dev, cam, cfg, torch.from_numpy(gt_a).cuda(), torch.from_numpy(gt_r).cuda(), 1.0)
+    setup_s = time.perf_counter() - t0
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    for _ in range(args.warmup):
+        img = diff.forward(dev, cam, cfg, A, R, 1.1)
+        diff.backward(dev, cam, cfg, A, R, 1.1, 2.0 * (img - target))
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats()
+    free0, total = torch.cuda.mem_get_info()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    f_ms = b_ms = 0.0
+    for _ in range(args.steps):
+        a, b, c = ev(), ev(), ev()
+        a.record()
+        img = diff.forward(dev, cam, cfg, A, R, 1.1)
+        b.record()
+        ga, gr, gs = diff.backward(dev, cam, cfg, A, R, 1.1, 2.0 * (img - target))
+        c.record()
+        torch.cuda.synchronize()
+        f_ms += a.elapsed_time(b)
+        b_ms += b.elapsed_time(c)
+    clock_record = clocks.stop()
+    peak_torch = torch.cuda.max_memory_allocated()
+    info = dev.info()
+    f_ms /= args.steps
+    b_ms /= args.steps
+    loss = float(((img.double() - target.double()) ** 2).sum())
+    paths = width * height * spp
+    line = {
+        "metric": "adjoint/forward time", "value": b_ms / f_ms, "unit": "ratio", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": f_ms + b_ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (gradients f64)", "data": "synthetic (seeded generator)",
+        "config": {"workload": "inverse", "width": width, "height": height, "spp": spp, "max_depth": depth,
+                   "triangles": n, "parameters": 4 * n + 1, "wall_triangles": 10240,
+                   "l2": "scene, parameters and images stay on the device; no flush"},
+        "forward_ms": f_ms, "adjoint_ms": b_ms,
+        "forward_mpaths_s": paths / (f_ms / 1e3) / 1e6,
+        "peak_device_bytes": {"torch_tensors": int(peak_torch), "scene": int(info.device_bytes),
+                              "note": "the adjoint stores no paths: images, parameters and gradients only"},
+        "loss": loss,
+        "e2e": None, "gpu_launches": 2 * args.steps, "roofline": None, "clocks": clock_record,
+        "setup_seconds": setup_s,
+    }
+    print(json.dumps(line), flush=True)
+    dev.close()
+    return 0
+
+
+def run_batch(args):
+    """Uneven jobs (64 sphere-field jobs from seed 11: 5k-2M triangles,
+    64^2-512^2 pixels, 4/16/64 spp, depth 8) rendered as one batch graph,
+    against the same jobs rendered one after another by per-job renderers
+    (graph mode, the reference's schedule) on the same GPU.  One step renders
+    every job's full sample count once.  Multi-GPU: jobs are assigned to
+    ranks longest-first by estimated cost; every rank renders its share."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import wfpt
+    from wfpt import scenes, shard
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    t0 = time.perf_counter()
+    specs = scenes.batch_jobs(args.batch_jobs, 11)
+    costs = [j["width"] * j["height"] * j["spp"] * math.log2(max(j["triangles"], 2)) for j in specs]
+    owner = shard.lpt_assign(costs, world)
+    mine = [j for j, r in zip(specs, owner) if r == rank]
+    stream = torch.cuda.Stream()
+    jobs = []
+    for j in mine:
+        cfg = wfpt.render_config(j["width"], j["height"], max_depth=j["max_depth"])
+        jobs.append(dict(scene=wfpt.DeviceScene(j["scene"]), camera=j["camera"], config=cfg, sample_start=0,
+                         sample_count=j["spp"]))
+    setup_s = time.perf_counter() - t0
+    paths = sum(j["config"].width * j["config"].height * j["sample_count"] for j in jobs)
+    total_paths = sum(j["width"] * j["height"] * j["spp"] for j in specs)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(ms):
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return ms
+
+    tune = None
+    if args.no_autotune:
+        batch = wfpt.Batch(jobs, stream=stream.cuda_stream)
+    else:
+        best, times = wfpt.Batch.autotune(jobs, slot_capacities=(1 << 20, 2 << 20, 4 << 20), block_sizes=(128, 256),
+                                          refill_thresholds=(8,), stream=stream.cuda_stream)
+        tune = {"candidates_ms": [round(t, 3) for t in times], "slot_capacity": best.slot_capacity,
+                "block_size": best.block_size, "refill_threshold": best.refill_threshold}
+        batch = wfpt.Batch(jobs, stream=stream.cuda_stream, config=best)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    for _ in range(args.warmup):
+        batch.run()
+    batch.synchronize()
+    batch.stats(reset=True)
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    a, b = ev(), ev()
+    a.record(stream)
+    for _ in range(args.steps):
+        batch.run()
+    b.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clock_record = clocks.stop()
+    batch.synchronize()
+    ms = max_over_ranks(a.elapsed_time(b))
+    stats = batch.stats(reset=True)
+    value = total_paths * args.steps / (ms / 1e3) / 1e6
+
+    # End to end: every step also reads every job framebuffer back to pinned host memory.
+    hosts = [torch.empty((j["config"].height, j["config"].width, 3), dtype=torch.float32, pin_memory=True)
+             for j in jobs]
+    lib = wfpt.library()
+    barrier()
+    torch.cuda.synchronize()
+    a, b = ev(), ev()
+    a.record(stream)
+    for _ in range(args.steps):
+        wfpt.check(lib.wf_batch_reset(batch.handle))
+        batch.run()
+        for k, h in enumerate(hosts):
+            wfpt.check(lib.wf_batch_download(batch.handle, k, h.data_ptr()))
+    b.record(stream)
+    torch.cuda.synchronize()
+    e_ms = max_over_ranks(a.elapsed_time(b))
+    e2e = total_paths * args.steps / (e_ms / 1e3) / 1e6
+
+    # Sequential baseline: one per-job renderer each, rendered one after another.
+    renderers = [wfpt.Renderer(j["scene"], j["camera"], j["config"], stream=stream.cuda_stream) for j in jobs]
+    for r, j in zip(renderers, jobs):
+        r.render(0, 0, j["config"].width, j["config"].height, 0, j["sample_count"], True)
+    torch.cuda.synchronize()
+    barrier()
+    a, b = ev(), ev()
+    a.record(stream)
+    for _ in range(args.steps):
+        for r, j in zip(renderers, jobs):
+            r.render(0, 0, j["config"].width, j["config"].height, 0, j["sample_count"], True)
+    b.record(stream)
+    torch.cuda.synchronize()
+    s_ms = max_over_ranks(a.elapsed_time(b))
+    sequential = total_paths * args.steps / (s_ms / 1e3) / 1e6
+    # parity spot check: the batch's last run equals the per-job renders
+    mismatched = sum(int(not np.array_equal(batch.download(k).view(np.uint32), r.download().view(np.uint32)))
+                     for k, r in enumerate(renderers))
+    for r in renderers:
+        r.close()
+    batch.close()
+    if rank == 0:
+        line = {
+            "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": "batch", "jobs": len(specs), "seed": 11, "paths_per_step": total_paths,
+                       "pixels": sum(j["width"] * j["height"] for j in specs),
+                       "triangles": sum(j["triangles"] for j in specs), "max_depth": 8,
+                       "parallelism": f"jobs x{world} (longest first)",
+                       "l2": "inputs larger than L2 (64 scenes on the device); no flush"},
+            "e2e": {"value": e2e, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": sum(h.numel() * 4 for h in hosts)},
+            "sequential": {"value": sequential, "unit": "Mpaths/s", "ms_per_step": s_ms / args.steps,
+                           "how": "one graph-mode renderer per job, rendered one after another"},
+            "speedup_vs_sequential": value / sequential,
+            "parity_mismatched_jobs": mismatched,
+            "autotune": tune,
+            "gpu_launches": int(stats["kernel_launches"]),
+            "roofline": None,
+            "clocks": clock_record,
+            "setup_seconds": setup_s,
+        }
+        print(json.dumps(line), flush=True)
+    for j in jobs:
+        j["scene"].close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="large_mesh", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="large_mesh", choices=sorted(WORKLOADS) + ["batch", "inverse"])
+    ap.add_argument("--batch-jobs", type=int, default=64, help="batch workload: number of jobs")
+    ap.add_argument("--no-autotune", action="store_true", help="batch workload: default batch configuration")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--mode", default=None, choices=sorted(MODES), help="default: per workload")
@@ -216,6 +436,10 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
+    if args.workload == "inverse":
+        return run_inverse(args)
 
     import numpy as np
     import torch

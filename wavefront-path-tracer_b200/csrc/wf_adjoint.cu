@@ -103,103 +103,140 @@ WF_DEV uint32_t parameter_index(const DeviceScene& s, uint32_t prim) {
     return tri.index_flags & kTriIndexMask;
 }
 
+// Gradient contributions of one vertex, summed over the lanes of a warp
+// that hit the same triangle (all 32 lanes call this together).  One lane
+// per triangle adds the sums with double atomics.
+WF_DEV void flush_vertex(uint32_t key, float4 value, float4* warp_buffer, const DiffGrads& G) {
+    uint32_t lane = threadIdx.x & 31;
+    unsigned peers = __match_any_sync(0xffffffffu, key);
+    warp_buffer[lane] = value;
+    __syncwarp();
+    if (key != kInvalid && lane == uint32_t(__ffs(peers) - 1)) {
+        float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (unsigned m = peers; m; m &= m - 1) {
+            float4 v = warp_buffer[__ffs(m) - 1];
+            sum.x += v.x;
+            sum.y += v.y;
+            sum.z += v.z;
+            sum.w += v.w;
+        }
+        if (sum.x != 0.0f) atomicAdd(&G.albedo[3 * key], double(sum.x));
+        if (sum.y != 0.0f) atomicAdd(&G.albedo[3 * key + 1], double(sum.y));
+        if (sum.z != 0.0f) atomicAdd(&G.albedo[3 * key + 2], double(sum.z));
+        if (sum.w != 0.0f) atomicAdd(&G.roughness[key], double(sum.w));
+    }
+    __syncwarp();
+}
+
 // One path of pixel (px, py), sample `sample`.  kAdjoint = false: returns
 // the path radiance at emission scale 1 (the image multiplies by the scale).
 // kAdjoint = true: `total` is that radiance from the first replay; adds
-// delta * dU/dtheta to the gradients and returns the replayed radiance.
+// delta * dU/dtheta to the gradients and returns the replayed radiance.  In
+// adjoint mode all 32 lanes of the warp call it together (`alive` false for
+// lanes without a path) and run the same number of vertex steps.
 template <bool kAdjoint>
 WF_DEV V3 diff_path(const DeviceScene& s, const DiffParams& P, const DiffSettings& cfg, uint32_t px, uint32_t py,
-                    uint32_t sample, V3 total, V3 delta, const DiffGrads& G, uint32_t* error) {
-    uint32_t pixel = py * cfg.width + px;
-    uint64_t rng = make_rng_state(pixel_rng_key(pixel, sample, cfg.rng), cfg.rng);
-    float u = (float(px) + random_float(rng, cfg.rng)) / float(cfg.width);
-    float v = (float(py) + random_float(rng, cfg.rng)) / float(cfg.height);
-    V3 o, d;
-    camera_ray(cfg.camera, u, v, o, d);
+                    uint32_t sample, bool alive, V3 total, V3 delta, const DiffGrads& G, float4* warp_buffer,
+                    uint32_t* error) {
+    V3 o{0.0f, 0.0f, 0.0f}, d{0.0f, 0.0f, 1.0f};
+    uint64_t rng = 0;
+    if (alive) {
+        uint32_t pixel = py * cfg.width + px;
+        rng = make_rng_state(pixel_rng_key(pixel, sample, cfg.rng), cfg.rng);
+        float u = (float(px) + random_float(rng, cfg.rng)) / float(cfg.width);
+        float v = (float(py) + random_float(rng, cfg.rng)) / float(cfg.height);
+        camera_ray(cfg.camera, u, v, o, d);
+    }
     V3 beta{1.0f, 1.0f, 1.0f};
     V3 sum{0.0f, 0.0f, 0.0f};  // terms so far, at emission scale 1
     NoTally tally;
     for (uint32_t depth = 0; depth < cfg.max_depth; ++depth) {
-        TraceState h;
-        trace_closest(s, o, d, h, tally);
-        SurfaceHit sh;
-        if (!finish_hit(s, o, d, h.t, h.u, h.v, h.prim, h.inst, sh)) break;
-        const Material& m = s.materials[sh.material];
-        if (m.type == kEmissive) {
-            if (depth == 0) sum += hadamard(beta, m.emission);
-            break;
-        }
-        uint32_t kind = hit_kind(h.prim);
-        if (kind == kHitSphere) break;  // spheres carry no parameters: they absorb
-        uint32_t k = parameter_index(s, h.prim);
-        if (k >= cfg.parameters) {
-            atomicOr(error, 1u);
-            break;
-        }
-        V3 albedo{P.albedo[3 * k], P.albedo[3 * k + 1], P.albedo[3 * k + 2]};
-        float sigma = P.roughness[k];
-        V3 gn = sh.geometric_normal;
-        V3 n = sh.normal;
-        if (dot(n, gn) < 0.0f) n = -n;
-        V3 wo = -d;
-        // next event: one triangle light picked by the alias table, one point on it
-        V3 nee_albedo_free{0.0f, 0.0f, 0.0f};  // term without the albedo factor
-        float nee_dsigma = 0.0f;               // d(term)/d(sigma) / term
-        if (s.light_count > 0) {
-            uint32_t candidate = min(uint32_t(random_float(rng, cfg.rng) * s.light_count), s.light_count - 1);
-            const Light* cl = &s.lights[candidate];
-            uint32_t li = random_float(rng, cfg.rng) < cl->alias_probability ? candidate : cl->alias;
-            const Light& light = s.lights[li];
-            float root_u = sqrtf(random_float(rng, cfg.rng));
-            float lv = random_float(rng, cfg.rng);
-            V3 lp = (1.0f - root_u) * light.v0 + root_u * (1.0f - lv) * light.v1 + root_u * lv * light.v2;
-            V3 to_light = lp - sh.position;
-            float dist2 = length_squared(to_light);
-            float dist = sqrtf(dist2);
-            V3 wl = to_light / dist;
-            float cos_g = dot(gn, wl), cos_s = dot(n, wl), cos_l = dot(light.normal, -wl);
-            if (cos_g > 0.0f && cos_s > 0.0f && cos_l > 0.0f) {
-                V3 so = offset_ray_origin(sh.position, gn, wl, sh.t);
-                V3 st = offset_ray_origin(lp, light.normal, -wl, dist);
-                V3 seg = st - so;
-                float sd = length(seg);
-                if (sd > kRayMinDistance && !trace_any(s, so, seg / sd, sd - kRayMinDistance, tally)) {
-                    OrenNayar on = oren_nayar(n, wo, wl, sigma);
-                    float geometry = cos_l * light.area / (dist2 * light.selection_pdf);
-                    const Material& lm = s.materials[light.material];
-                    nee_albedo_free = hadamard(beta, lm.emission) * (on.value * kInvPi * cos_s * geometry);
-                    nee_dsigma = on.value > 0.0f ? on.d_sigma / on.value : 0.0f;
-                    sum += hadamard(albedo, nee_albedo_free);
+        if (!kAdjoint && !alive) break;
+        uint32_t key = kInvalid;
+        float4 contribution = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        do {
+            if (!alive) break;
+            alive = false;  // set again below when the path continues
+            TraceState h;
+            trace_closest(s, o, d, h, tally);
+            SurfaceHit sh;
+            if (!finish_hit(s, o, d, h.t, h.u, h.v, h.prim, h.inst, sh)) break;
+            const Material& m = s.materials[sh.material];
+            if (m.type == kEmissive) {
+                if (depth == 0) sum += hadamard(beta, m.emission);
+                break;
+            }
+            if (hit_kind(h.prim) == kHitSphere) break;  // spheres carry no parameters: they absorb
+            uint32_t k = parameter_index(s, h.prim);
+            if (k >= cfg.parameters) {
+                atomicOr(error, 1u);
+                break;
+            }
+            V3 albedo{P.albedo[3 * k], P.albedo[3 * k + 1], P.albedo[3 * k + 2]};
+            float sigma = P.roughness[k];
+            V3 gn = sh.geometric_normal;
+            V3 n = sh.normal;
+            if (dot(n, gn) < 0.0f) n = -n;
+            V3 wo = -d;
+            // next event: one triangle light picked by the alias table, one point on it
+            V3 nee_albedo_free{0.0f, 0.0f, 0.0f};  // term without the albedo factor
+            float nee_dsigma = 0.0f;               // d(term)/d(sigma) / term
+            if (s.light_count > 0) {
+                uint32_t candidate = min(uint32_t(random_float(rng, cfg.rng) * s.light_count), s.light_count - 1);
+                const Light* cl = &s.lights[candidate];
+                uint32_t li = random_float(rng, cfg.rng) < cl->alias_probability ? candidate : cl->alias;
+                const Light& light = s.lights[li];
+                float root_u = sqrtf(random_float(rng, cfg.rng));
+                float lv = random_float(rng, cfg.rng);
+                V3 lp = (1.0f - root_u) * light.v0 + root_u * (1.0f - lv) * light.v1 + root_u * lv * light.v2;
+                V3 to_light = lp - sh.position;
+                float dist2 = length_squared(to_light);
+                float dist = sqrtf(dist2);
+                V3 wl = to_light / dist;
+                float cos_g = dot(gn, wl), cos_s = dot(n, wl), cos_l = dot(light.normal, -wl);
+                if (cos_g > 0.0f && cos_s > 0.0f && cos_l > 0.0f) {
+                    V3 so = offset_ray_origin(sh.position, gn, wl, sh.t);
+                    V3 st = offset_ray_origin(lp, light.normal, -wl, dist);
+                    V3 seg = st - so;
+                    float sd = length(seg);
+                    if (sd > kRayMinDistance && !trace_any(s, so, seg / sd, sd - kRayMinDistance, tally)) {
+                        OrenNayar on = oren_nayar(n, wo, wl, sigma);
+                        float geometry = cos_l * light.area / (dist2 * light.selection_pdf);
+                        const Material& lm = s.materials[light.material];
+                        nee_albedo_free = hadamard(beta, lm.emission) * (on.value * kInvPi * cos_s * geometry);
+                        nee_dsigma = on.value > 0.0f ? on.d_sigma / on.value : 0.0f;
+                        sum += hadamard(albedo, nee_albedo_free);
+                    }
                 }
             }
-        }
-        // continuation: cosine-weighted about the shading normal
-        float r1 = random_float(rng, cfg.rng), r2 = random_float(rng, cfg.rng);
-        V3 wi = sample_cosine_hemisphere_uv(n, r1, r2);
-        bool continues = depth + 1 < cfg.max_depth && dot(wi, gn) > 0.0f;
-        OrenNayar on = continues ? oren_nayar(n, wo, wi, sigma) : OrenNayar{0.0f, 0.0f};
-        if constexpr (kAdjoint) {
-            // terms after this vertex all carry this vertex's continuation weight
-            V3 after = total - sum;
-            V3 ga{0.0f, 0.0f, 0.0f};
-            float gs = 0.0f;
-            if (continues) {
-                ga = V3{albedo.x > 0.0f ? after.x / albedo.x : 0.0f, albedo.y > 0.0f ? after.y / albedo.y : 0.0f,
-                        albedo.z > 0.0f ? after.z / albedo.z : 0.0f};
-                gs = on.value > 0.0f ? dot(delta, after) * (on.d_sigma / on.value) : 0.0f;
+            // continuation: cosine-weighted about the shading normal
+            float r1 = random_float(rng, cfg.rng), r2 = random_float(rng, cfg.rng);
+            V3 wi = sample_cosine_hemisphere_uv(n, r1, r2);
+            bool continues = depth + 1 < cfg.max_depth && dot(wi, gn) > 0.0f;
+            OrenNayar on = continues ? oren_nayar(n, wo, wi, sigma) : OrenNayar{0.0f, 0.0f};
+            if constexpr (kAdjoint) {
+                // terms after this vertex all carry this vertex's continuation weight
+                V3 after = total - sum;
+                V3 ga{0.0f, 0.0f, 0.0f};
+                float gs = 0.0f;
+                if (continues) {
+                    ga = V3{albedo.x > 0.0f ? after.x / albedo.x : 0.0f, albedo.y > 0.0f ? after.y / albedo.y : 0.0f,
+                            albedo.z > 0.0f ? after.z / albedo.z : 0.0f};
+                    gs = on.value > 0.0f ? dot(delta, after) * (on.d_sigma / on.value) : 0.0f;
+                }
+                ga += nee_albedo_free;
+                gs += dot(delta, hadamard(albedo, nee_albedo_free)) * nee_dsigma;
+                V3 dga = hadamard(delta, ga);
+                key = k;
+                contribution = make_float4(dga.x, dga.y, dga.z, gs);
             }
-            ga += nee_albedo_free;
-            gs += dot(delta, hadamard(albedo, nee_albedo_free)) * nee_dsigma;
-            V3 dga = hadamard(delta, ga);
-            if (dga.x != 0.0f) atomicAdd(&G.albedo[3 * k], double(dga.x));
-            if (dga.y != 0.0f) atomicAdd(&G.albedo[3 * k + 1], double(dga.y));
-            if (dga.z != 0.0f) atomicAdd(&G.albedo[3 * k + 2], double(dga.z));
-            if (gs != 0.0f) atomicAdd(&G.roughness[k], double(gs));
-        }
-        if (!continues) break;
-        beta = hadamard(beta, albedo * on.value);
-        o = offset_ray_origin(sh.position, gn, wi, sh.t);
-        d = wi;
+            if (!continues) break;
+            beta = hadamard(beta, albedo * on.value);
+            o = offset_ray_origin(sh.position, gn, wi, sh.t);
+            d = wi;
+            alive = true;
+        } while (false);
+        if constexpr (kAdjoint) flush_vertex(key, contribution, warp_buffer, G);
     }
     return sum;
 }
@@ -212,7 +249,7 @@ __global__ void k_diff_forward(const __grid_constant__ DeviceScene s, DiffParams
         uint32_t px = cfg.x + i % cfg.w, py = cfg.y + i / cfg.w;
         V3 acc{0.0f, 0.0f, 0.0f};
         for (uint32_t k = 0; k < cfg.spp; ++k)
-            acc += diff_path<false>(s, P, cfg, px, py, cfg.sample_start + k, V3{}, V3{}, none, error);
+            acc += diff_path<false>(s, P, cfg, px, py, cfg.sample_start + k, true, V3{}, V3{}, none, nullptr, error);
         float scale = P.emission_scale / float(cfg.spp);
         float* out = image + 3 * (size_t(py) * cfg.width + px);
         out[0] = acc.x * scale;
@@ -222,27 +259,39 @@ __global__ void k_diff_forward(const __grid_constant__ DeviceScene s, DiffParams
 }
 
 // d_image: dLoss/dImage (image = mean over samples of emission_scale * U).
-__global__ void k_diff_backward(const __grid_constant__ DeviceScene s, DiffParams P, DiffSettings cfg,
-                                const float* d_image, DiffGrads G, uint32_t* error) {
-    uint32_t n = cfg.w * cfg.h;
+// Each warp takes up to 32 samples of one pixel, so the lanes of a warp
+// mostly hit the same triangles and their gradients merge before the
+// atomics (flush_vertex).
+__global__ void __launch_bounds__(128) k_diff_backward(const __grid_constant__ DeviceScene s, DiffParams P,
+                                                       DiffSettings cfg, const float* d_image, DiffGrads G,
+                                                       uint32_t* error) {
+    __shared__ float4 buffers[4][32];
+    float4* warp_buffer = buffers[threadIdx.x >> 5];
+    uint32_t lane = threadIdx.x & 31;
+    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t chunks = (cfg.spp + 31) / 32;
+    uint32_t items = cfg.w * cfg.h * chunks;
     double d_scale = 0.0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    DiffGrads none{};
+    for (uint32_t item = warp; item < items; item += warps) {
+        uint32_t i = item / chunks, chunk = item % chunks;
         uint32_t px = cfg.x + i % cfg.w, py = cfg.y + i / cfg.w;
         const float* g = d_image + 3 * (size_t(py) * cfg.width + px);
         V3 grad_pixel{g[0], g[1], g[2]};
-        if (grad_pixel.x == 0.0f && grad_pixel.y == 0.0f && grad_pixel.z == 0.0f) continue;
+        if (grad_pixel.x == 0.0f && grad_pixel.y == 0.0f && grad_pixel.z == 0.0f) continue;  // uniform per warp
+        uint32_t k = chunk * 32 + lane;
+        bool alive = k < cfg.spp;
+        uint32_t sample = cfg.sample_start + k;
         // the image is scale/spp * sum U: dLoss/dU = dLoss/dImage * scale / spp
         V3 delta = grad_pixel * (P.emission_scale / float(cfg.spp));
-        DiffGrads none{};
-        for (uint32_t k = 0; k < cfg.spp; ++k) {
-            uint32_t sample = cfg.sample_start + k;
-            V3 total = diff_path<false>(s, P, cfg, px, py, sample, V3{}, V3{}, none, error);
-            diff_path<true>(s, P, cfg, px, py, sample, total, delta, G, error);
-            d_scale += double(dot(grad_pixel, total)) / double(cfg.spp);
-        }
+        V3 total{0.0f, 0.0f, 0.0f};
+        if (alive) total = diff_path<false>(s, P, cfg, px, py, sample, true, V3{}, V3{}, none, nullptr, error);
+        diff_path<true>(s, P, cfg, px, py, sample, alive, total, delta, G, warp_buffer, error);
+        if (alive) d_scale += double(dot(grad_pixel, total)) / double(cfg.spp);
     }
     for (int off = 16; off > 0; off >>= 1) d_scale += __shfl_down_sync(0xffffffffu, d_scale, off);
-    if ((threadIdx.x & 31) == 0 && d_scale != 0.0) atomicAdd(G.emission_scale, d_scale);
+    if (lane == 0 && d_scale != 0.0) atomicAdd(G.emission_scale, d_scale);
 }
 
 // Error flag of the differentiable kernels (a parameter index out of range).
@@ -330,7 +379,9 @@ extern "C" wf_status wf_diff_backward(const wf_scene* scene, const wf_camera* ca
     if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemsetAsync");
     DiffParams P{albedo, roughness, emission_scale};
     DiffGrads G{d_albedo, d_roughness, d_emission_scale};
-    k_diff_backward<<<diff_grid(cfg.w * cfg.h), 128, 0, st>>>(scene->view, P, cfg, d_image, G, error);
+    uint32_t items = cfg.w * cfg.h * ((cfg.spp + 31) / 32);  // one warp each
+    k_diff_backward<<<std::max(1u, std::min((items + 3) / 4, 148u * 16u)), 128, 0, st>>>(scene->view, P, cfg, d_image,
+                                                                                          G, error);
     ce = cudaGetLastError();
     if (ce != cudaSuccess) return cuda_fail(ce, "k_diff_backward");
     return diff_finish(error, st);

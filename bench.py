@@ -183,9 +183,10 @@ def run_reference(args):
     cores = os.cpu_count() or 1
     sample_desc = ""
     ref = reference_scene(scene)
+    # every step renders a band of rows sized so the whole run stays near 90 s
+    per_step = max(1.0, min(args.cpu_seconds, 90.0 / max(1, args.warmup + args.steps)))
     for step in range(args.warmup + args.steps):
-        rate, cores, sample_desc, _ = cpu_reference_rate(ref, cam, width, height, rkw,
-                                                          seconds_target=args.cpu_seconds)
+        rate, cores, sample_desc, _ = cpu_reference_rate(ref, cam, width, height, rkw, seconds_target=per_step)
         if step >= args.warmup:
             rates.append(rate)
     value = statistics.median(rates)
@@ -194,7 +195,12 @@ def run_reference(args):
             "ms_per_step": width * height / (value * 1e6) * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
             "config": {"workload": args.workload, "width": width, "height": height,
-                       "max_depth": rkw.get("max_depth")},
+                       "spp_per_step": args.spp or SPP_PER_STEP.get(args.workload, 1),
+                       "max_depth": rkw.get("max_depth"), "rr_start_depth": rkw.get("rr_start_depth", 12),
+                       "triangles": int(scene.triangle_count()), "instances": int(len(scene.instances)),
+                       "photons": int(rkw.get("photon_count", 0)) if rkw.get("caustics") else 0,
+                       "mode": "host-compiled reference (captured-graph chain on host threads)",
+                       "parallelism": "host threads"},
             "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": cores, "kind": "reference",
                              "sample": sample_desc},
             "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

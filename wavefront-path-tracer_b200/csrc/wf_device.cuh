@@ -251,6 +251,8 @@ struct GatherQueue {
     float4* albedo;      // xyz
     uint32_t* count;
     uint32_t capacity;
+    uint32_t* dense;       // requests with many candidate photons (indices into the queue)
+    uint32_t* dense_count;
 };
 
 struct PhotonGridView {

@@ -83,7 +83,11 @@ __global__ void k_raygen_stream(RenderParams rp, const TileDev* tile_ptr, Counte
     }
 }
 
-template <typename Tally>
+// kLanes: lane-refill state machines (incoherent bounces).  Otherwise each
+// warp takes 32 consecutive queue entries and every lane runs its ray to the
+// end (camera rays: neighbouring pixels visit the same nodes in lockstep).
+// The per-ray visit order and arithmetic are the same either way.
+template <typename Tally, bool kLanes = true>
 __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
                         uint32_t* hit_inst, Counters* c, uint32_t bounce, TallyTotals* totals, uint32_t refill_at) {
     count_launch(c);
@@ -92,11 +96,27 @@ __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const 
     if (gid == 0) {
         c->shadow_count = 0;
         c->gather_count = 0;
+        c->dense_count = 0;
         c->work_shade = 0;
         if (bounce < kMaxBounces) c->profile[bounce] = n;
         c->extension_rays += n;
     }
     Tally tally;
+    if constexpr (!kLanes) {
+        uint32_t base;
+        while (next_chunk(&c->work_trace, n, base)) {
+            uint32_t i = base + (threadIdx.x & 31);
+            if (i >= n) continue;
+            uint32_t p = queue[i];
+            float4 o = ps.origin[p], d = ps.direction[p];
+            TraceState h;
+            trace_closest(s, f4xyz(o), f4xyz(d), h, tally);
+            hit_a[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
+            hit_inst[i] = h.inst;
+        }
+        if constexpr (std::is_same<Tally, CountTally>::value) flush_tally(tally, totals);
+        return;
+    }
     ClosestLane L;
     L.stage = kStageDone;
     uint32_t i = 0;
@@ -142,6 +162,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ Device
         *next_count = 0;
         c->work_shadow = 0;
         c->work_gather = 0;
+        c->work_dense = 0;
     }
     uint32_t base;
     while (next_chunk(&c->work_shade, n, base)) {
@@ -173,7 +194,19 @@ __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ Device
 }
 
 // Caustic gathers queued by k_shade (gatherCaustics, photon_mapping.cu:91-163),
-// written into the term slots their paths reserved.
+// written into the term slots their paths reserved.  A request whose cells
+// hold many photons (near a caustic) would scan them serially while the rest
+// of the GPU waits; it goes to k_gather_dense, one warp per request.
+constexpr uint32_t kDenseGather = 256;
+
+WF_DEV void write_gather_term(const RenderParams& rp, const GatherQueue& q, float4* terms, uint32_t r, V3 caustic) {
+    float4 pos = q.position[r], nrm = q.normal[r], thr = q.throughput[r], alb = q.albedo[r];
+    Path depth_only{};
+    depth_only.depth = nrm.w != 0.0f ? 1u : 0u;
+    V3 col = clamp_contribution(depth_only, hadamard(f4xyz(thr), hadamard(f4xyz(alb), caustic)), rp.clamp, false);
+    terms[__float_as_uint(pos.w)] = make_float4(col.x, col.y, col.z, __int_as_float(kUnconditional));
+}
+
 __global__ void k_gather(const __grid_constant__ RenderParams rp, GatherQueue q, float4* terms, Counters* c) {
     count_launch(c);
     uint32_t n = min(*q.count, q.capacity);
@@ -181,15 +214,31 @@ __global__ void k_gather(const __grid_constant__ RenderParams rp, GatherQueue q,
     while (next_chunk(&c->work_gather, n, base)) {
         uint32_t r = base + (threadIdx.x & 31);
         if (r >= n) continue;
-        float4 pos = q.position[r], nrm = q.normal[r], thr = q.throughput[r], alb = q.albedo[r];
+        float4 pos = q.position[r], nrm = q.normal[r];
+        if (gather_cell_photons(rp.photons, f4xyz(pos), rp.gather_radius) > kDenseGather) {
+            q.dense[atomicAdd(q.dense_count, 1u)] = r;
+            continue;
+        }
         ShadeHit hit{};
         hit.position = f4xyz(pos);
         hit.normal = f4xyz(nrm);
-        V3 caustic = gather_caustics(rp.photons, hit, rp.gather_radius);
-        Path depth_only{};
-        depth_only.depth = nrm.w != 0.0f ? 1u : 0u;
-        V3 col = clamp_contribution(depth_only, hadamard(f4xyz(thr), hadamard(f4xyz(alb), caustic)), rp.clamp, false);
-        terms[__float_as_uint(pos.w)] = make_float4(col.x, col.y, col.z, __int_as_float(kUnconditional));
+        write_gather_term(rp, q, terms, r, gather_caustics(rp.photons, hit, rp.gather_radius));
+    }
+}
+
+__global__ void k_gather_dense(const __grid_constant__ RenderParams rp, GatherQueue q, float4* terms, Counters* c) {
+    count_launch(c);
+    uint32_t n = min(*q.dense_count, q.capacity);
+    uint32_t lane = threadIdx.x & 31;
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(&c->work_dense, 1u);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= n) break;
+        uint32_t r = q.dense[k];
+        float4 pos = q.position[r], nrm = q.normal[r];
+        V3 caustic = gather_caustics_warp(rp.photons, f4xyz(pos), f4xyz(nrm), rp.gather_radius);
+        if (lane == 0) write_gather_term(rp, q, terms, r, caustic);
     }
 }
 
@@ -790,14 +839,21 @@ wf_status capture_graph(wf_renderer* r) {
         uint32_t cur = b & 1, nxt = cur ^ 1;
         uint32_t* cur_count = &r->counters->queue_count[cur];
         uint32_t* next_count = &r->counters->queue_count[nxt];
-        k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
-            s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill);
+        if (b == 0)
+            k_trace<NoTally, false><<<grid(r, 5, cap, r->block_trace), r->block_trace, 0, st>>>(
+                s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill);
+        else
+            k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
+                s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill);
         k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
             r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers);
-        if (r->params.photons.enabled)
+        if (r->params.photons.enabled) {
             k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers, r->terms,
                                                                                    r->counters);
+            k_gather_dense<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers,
+                                                                                         r->terms, r->counters);
+        }
         k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
             s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr, r->refill);
         k_finalize<false><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
@@ -853,9 +909,12 @@ wf_status capture_stream_graph(wf_renderer* r) {
         k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
             r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers);
-        if (r->params.photons.enabled)
+        if (r->params.photons.enabled) {
             k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers, r->terms,
                                                                                    r->counters);
+            k_gather_dense<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers,
+                                                                                         r->terms, r->counters);
+        }
         k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
             s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr, r->refill);
         k_finalize<true><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
@@ -995,9 +1054,12 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
             WF_CUDA(alloc(rr, &r->gathers.albedo, cap));
             r->gathers.count = &r->counters->gather_count;
             r->gathers.capacity = cap;
+            WF_CUDA(alloc(rr, &r->gathers.dense, cap));
+            r->gathers.dense_count = &r->counters->dense_count;
             WF_CUDA(resident_grid(rr, 4, k_gather, r->block_gather));
         }
         WF_CUDA(resident_grid(rr, 0, k_trace<NoTally>, r->block_trace));
+        WF_CUDA(resident_grid(rr, 5, k_trace<NoTally, false>, r->block_trace));
         WF_CUDA(resident_grid(rr, 1, k_shade, r->block_shade));
         WF_CUDA(resident_grid(rr, 2, k_shadow<NoTally>, r->block_trace));
         WF_CUDA(resident_grid(rr, 3, k_finalize<true>, r->block_finalize));
@@ -1180,10 +1242,18 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                     uint32_t* cur_count = &r->counters->queue_count[cur];
                     uint32_t* next_count = &r->counters->queue_count[nxt];
                     auto trace = [&] {
-                        if (count)
+                        if (count && b == 0)
+                            k_trace<CountTally, false><<<grid(r, 5, cap, r->block_trace), r->block_trace, 0, st>>>(
+                                s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
+                                r->tally, r->refill);
+                        else if (count)
                             k_trace<CountTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
                                 r->tally, r->refill);
+                        else if (b == 0)
+                            k_trace<NoTally, false><<<grid(r, 5, cap, r->block_trace), r->block_trace, 0, st>>>(
+                                s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
+                                nullptr, r->refill);
                         else
                             k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
@@ -1198,6 +1268,8 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                     auto gather = [&] {
                         k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers,
                                                                                                r->terms, r->counters);
+                        k_gather_dense<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(
+                            r->params, r->gathers, r->terms, r->counters);
                     };
                     bool gathers = r->params.photons.enabled != 0;
                     auto shadow = [&] {

@@ -38,6 +38,8 @@ struct Counters {
     uint32_t stream_iterations;  // streaming mode: loop iterations of the current launch
     uint32_t gather_count;       // caustic gather requests of the current bounce
     uint32_t work_gather;
+    uint32_t dense_count;        // gather requests deferred to the warp-per-request kernel
+    uint32_t work_dense;
     uint32_t next_unit;          // job batch: next (job, pixel) unit to start
     unsigned long long extension_rays;
     unsigned long long shadow_rays;
@@ -101,7 +103,7 @@ struct wf_renderer {
     float* framebuffer = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
-    uint32_t grid_resident[5] = {0, 0, 0, 0, 0};  // trace, shade, shadow, finalize, gather: one wave of CTAs
+    uint32_t grid_resident[6] = {0, 0, 0, 0, 0, 0};  // trace, shade, shadow, finalize, gather, camera-ray trace
     wf::GatherQueue gathers{};                      // caustic gather requests (graph and streaming modes)
     uint32_t persistent_blocks = 0;
     uint32_t persistent_block_size = 128;

@@ -832,6 +832,169 @@ WF_DEV V3 gather_caustics(const PhotonGridView& g, const ShadeHit& hit, float ra
     return result * (3.0f / (3.14159265359f * gather_sq));
 }
 
+// Photons stored in the cells gather_caustics scans for this point (an upper
+// bound on its candidates: the cost of the serial scan).
+WF_DEV uint32_t gather_cell_photons(const PhotonGridView& g, V3 position, float radius) {
+    {
+        float sr = fmaxf(radius * 4.0f, 0.1f) * 1.001f;
+        float dx = fmaxf(fmaxf(g.minimum.x - position.x, position.x - g.maximum.x), 0.0f);
+        float dy = fmaxf(fmaxf(g.minimum.y - position.y, position.y - g.maximum.y), 0.0f);
+        float dz = fmaxf(fmaxf(g.minimum.z - position.z, position.z - g.maximum.z), 0.0f);
+        if (dx > sr || dy > sr || dz > sr) return 0;
+    }
+    V3 extent = g.maximum - g.minimum;
+    V3 offset = position - g.minimum;
+    V3 nrm{offset.x / extent.x, offset.y / extent.y, offset.z / extent.z};
+    int res = int(g.resolution);
+    int cx = min(max(int(nrm.x * g.resolution), 0), res - 1);
+    int cy = min(max(int(nrm.y * g.resolution), 0), res - 1);
+    int cz = min(max(int(nrm.z * g.resolution), 0), res - 1);
+    float search_radius = fmaxf(radius * 4.0f, 0.1f);
+    int cell_radius = max(1, int(ceilf(search_radius * g.resolution / fmaxf(extent.x, 0.0001f))));
+    uint32_t total = 0;
+    for (int z = max(cz - cell_radius, 0); z <= min(cz + cell_radius, res - 1); ++z)
+        for (int y = max(cy - cell_radius, 0); y <= min(cy + cell_radius, res - 1); ++y)
+            for (int x = max(cx - cell_radius, 0); x <= min(cx + cell_radius, res - 1); ++x)
+                total += g.cell_count[(uint32_t(z) * g.resolution + uint32_t(y)) * g.resolution + uint32_t(x)];
+    return total;
+}
+
+// gather_caustics for one shading point, computed by a whole warp (all 32
+// lanes call it with the same arguments).  The lanes filter 32 photons of a
+// cell at a time; the photons that pass are then inserted one after another
+// in scan order, exactly as the serial loop does, into the 64-entry nearest
+// set, whose entries i and i + 32 live in lane i.  The farthest entry (the
+// first index holding the largest distance) is found by a warp argmax, and
+// the result is summed serially in slot order, so the value is the serial
+// one bit for bit.  Every lane returns the result.
+WF_DEV V3 gather_caustics_warp(const PhotonGridView& g, V3 position, V3 normal, float radius) {
+    const uint32_t lane = threadIdx.x & 31;
+    {
+        float sr = fmaxf(radius * 4.0f, 0.1f) * 1.001f;
+        float dx = fmaxf(fmaxf(g.minimum.x - position.x, position.x - g.maximum.x), 0.0f);
+        float dy = fmaxf(fmaxf(g.minimum.y - position.y, position.y - g.maximum.y), 0.0f);
+        float dz = fmaxf(fmaxf(g.minimum.z - position.z, position.z - g.maximum.z), 0.0f);
+        if (dx > sr || dy > sr || dz > sr) return V3{0, 0, 0};
+    }
+    V3 extent = g.maximum - g.minimum;
+    V3 offset = position - g.minimum;
+    V3 nrm{offset.x / extent.x, offset.y / extent.y, offset.z / extent.z};
+    int res = int(g.resolution);
+    int cx = min(max(int(nrm.x * g.resolution), 0), res - 1);
+    int cy = min(max(int(nrm.y * g.resolution), 0), res - 1);
+    int cz = min(max(int(nrm.z * g.resolution), 0), res - 1);
+    constexpr uint32_t kMaxNearest = 64;
+    constexpr uint32_t kMinimumPhotons = 16;
+    float search_radius = fmaxf(radius * 4.0f, 0.1f);
+    int cell_radius = max(1, int(ceilf(search_radius * g.resolution / fmaxf(extent.x, 0.0001f))));
+    float search_sq = search_radius * search_radius;
+    // entries lane and lane + 32 of the nearest set
+    float near_d[2] = {0.0f, 0.0f};
+    uint32_t near_i[2] = {kInvalid, kInvalid};
+    uint32_t count = 0, farthest = 0;
+    float farthest_sq = 0.0f;
+    for (int z = cz - cell_radius; z <= cz + cell_radius; ++z)
+        for (int y = cy - cell_radius; y <= cy + cell_radius; ++y)
+            for (int x = cx - cell_radius; x <= cx + cell_radius; ++x) {
+                if (x < 0 || y < 0 || z < 0 || x >= res || y >= res || z >= res) continue;
+                {
+                    float cx0 = g.minimum.x + extent.x * (float(x) / float(res));
+                    float cx1 = g.minimum.x + extent.x * (float(x + 1) / float(res));
+                    float cy0 = g.minimum.y + extent.y * (float(y) / float(res));
+                    float cy1 = g.minimum.y + extent.y * (float(y + 1) / float(res));
+                    float cz0 = g.minimum.z + extent.z * (float(z) / float(res));
+                    float cz1 = g.minimum.z + extent.z * (float(z + 1) / float(res));
+                    float gx = fmaxf(fmaxf(cx0 - position.x, position.x - cx1), 0.0f);
+                    float gy = fmaxf(fmaxf(cy0 - position.y, position.y - cy1), 0.0f);
+                    float gz = fmaxf(fmaxf(cz0 - position.z, position.z - cz1), 0.0f);
+                    float cell_margin = search_radius * 1.001f + 1.0e-4f * (fabsf(extent.x) + fabsf(extent.y) + fabsf(extent.z));
+                    if (gx > cell_margin || gy > cell_margin || gz > cell_margin) continue;
+                }
+                uint32_t cell = (uint32_t(z) * g.resolution + uint32_t(y)) * g.resolution + uint32_t(x);
+                uint32_t begin = g.cell_start[cell], end = begin + g.cell_count[cell];
+                for (uint32_t base = begin; base < end; base += 32) {
+                    uint32_t p = base + lane;
+                    float dsq = 0.0f;
+                    bool accept = false;
+                    if (p < end) {
+                        float4 pp = __ldg(&g.position[p]);
+                        V3 po = V3{pp.x, pp.y, pp.z} - position;
+                        dsq = dot(po, po);
+                        if (!(dsq > search_sq)) {  // the serial loop's rejection tests, negated
+                            float4 pd = __ldg(&g.direction[p]);
+                            accept = !(dot(normal, V3{pd.x, pd.y, pd.z}) <= 0.0f);
+                        }
+                    }
+                    unsigned accepted = __ballot_sync(0xffffffffu, accept);
+                    while (accepted) {
+                        int j = __ffs(accepted) - 1;
+                        accepted &= accepted - 1;
+                        float d = __shfl_sync(0xffffffffu, dsq, j);
+                        uint32_t index = base + uint32_t(j);
+                        if (count < kMaxNearest) {
+                            if ((count & 31) == lane) {
+                                near_d[count >> 5] = d;
+                                near_i[count >> 5] = index;
+                            }
+                            if (d > farthest_sq) {
+                                farthest_sq = d;
+                                farthest = count;
+                            }
+                            ++count;
+                        } else if (d < farthest_sq) {
+                            if ((farthest & 31) == lane) {
+                                near_d[farthest >> 5] = d;
+                                near_i[farthest >> 5] = index;
+                            }
+                            // first index holding the largest distance
+                            float best = near_d[1] > near_d[0] ? near_d[1] : near_d[0];
+                            uint32_t at = near_d[1] > near_d[0] ? lane + 32 : lane;
+                            for (int off = 16; off > 0; off >>= 1) {
+                                float ob = __shfl_xor_sync(0xffffffffu, best, off);
+                                uint32_t oa = __shfl_xor_sync(0xffffffffu, at, off);
+                                if (ob > best || (ob == best && oa < at)) {
+                                    best = ob;
+                                    at = oa;
+                                }
+                            }
+                            farthest_sq = best;
+                            farthest = at;
+                        }
+                    }
+                }
+            }
+    if (count == 0) return V3{0, 0, 0};
+    float gather_sq = search_sq;
+    if (count >= kMinimumPhotons) {
+        float m = 0.0f;
+        if (lane < count) m = fmaxf(m, near_d[0]);
+        if (lane + 32 < count) m = fmaxf(m, near_d[1]);
+        for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+        gather_sq = fmaxf(m, radius * radius);
+    }
+    float gather_radius = sqrtf(gather_sq);
+    V3 part[2];
+    for (int h = 0; h < 2; ++h) {
+        part[h] = V3{0.0f, 0.0f, 0.0f};
+        if (lane + 32u * h < count) {
+            float4 pd = __ldg(&g.direction[near_i[h]]);
+            float4 pf = __ldg(&g.flux[near_i[h]]);
+            float distance = sqrtf(near_d[h]);
+            float cone = fmaxf(0.0f, 1.0f - distance / gather_radius);
+            part[h] = V3{pf.x, pf.y, pf.z} * (cone * dot(normal, V3{pd.x, pd.y, pd.z}));
+        }
+    }
+    V3 result{0, 0, 0};
+    for (uint32_t i = 0; i < count; ++i) {  // slot order, as the serial sum
+        int src = int(i & 31);
+        V3 c = (i >> 5) ? part[1] : part[0];
+        result.x += __shfl_sync(0xffffffffu, c.x, src);
+        result.y += __shfl_sync(0xffffffffu, c.y, src);
+        result.z += __shfl_sync(0xffffffffu, c.z, src);
+    }
+    return result * (3.0f / (3.14159265359f * gather_sq));
+}
+
 // --------------------------------------------------------- continuations
 // continueDielectricSurface, device_traversal.cuh:589-635.
 template <typename Sink>

@@ -848,14 +848,19 @@ wf_status capture_graph(wf_renderer* r) {
         k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
             r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers);
-        if (r->params.photons.enabled) {
-            k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers, r->terms,
-                                                                                   r->counters);
-            k_gather_dense<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers,
-                                                                                         r->terms, r->counters);
+        bool fork = r->params.photons.enabled != 0;
+        if (fork) {  // gathers on a parallel branch: they and the shadow rays write different buffers
+            WF_CUDA(cudaEventRecord(r->fork_event, st));
+            WF_CUDA(cudaStreamWaitEvent(r->side, r->fork_event, 0));
+            k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, r->side>>>(r->params, r->gathers,
+                                                                                        r->terms, r->counters);
+            k_gather_dense<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, r->side>>>(
+                r->params, r->gathers, r->terms, r->counters);
+            WF_CUDA(cudaEventRecord(r->join_event, r->side));
         }
         k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
             s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr, r->refill);
+        if (fork) WF_CUDA(cudaStreamWaitEvent(st, r->join_event, 0));
         k_finalize<false><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
             r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result, r->queue[nxt], next_count,
             cap, r->framebuffer, &r->counters->work_trace, r->params, r->tile, r->counters);
@@ -909,14 +914,19 @@ wf_status capture_stream_graph(wf_renderer* r) {
         k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
             r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers);
-        if (r->params.photons.enabled) {
-            k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers, r->terms,
-                                                                                   r->counters);
-            k_gather_dense<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers,
-                                                                                         r->terms, r->counters);
+        bool fork = r->params.photons.enabled != 0;
+        if (fork) {  // gathers on a parallel branch: they and the shadow rays write different buffers
+            WF_CUDA(cudaEventRecord(r->fork_event, st));
+            WF_CUDA(cudaStreamWaitEvent(r->side, r->fork_event, 0));
+            k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, r->side>>>(r->params, r->gathers,
+                                                                                        r->terms, r->counters);
+            k_gather_dense<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, r->side>>>(
+                r->params, r->gathers, r->terms, r->counters);
+            WF_CUDA(cudaEventRecord(r->join_event, r->side));
         }
         k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
             s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr, r->refill);
+        if (fork) WF_CUDA(cudaStreamWaitEvent(st, r->join_event, 0));
         k_finalize<true><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
             r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result, r->queue[nxt], next_count,
             cap, r->framebuffer, &r->counters->work_trace, r->params, r->tile, r->counters);
@@ -1079,6 +1089,11 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
     if (c.caustics) {
         if (wf_status e = build_photon_map(rr)) return e;
     }
+    if (c.mode != WF_MODE_PERSISTENT) {
+        WF_CUDA(cudaStreamCreateWithFlags(&r->side, cudaStreamNonBlocking));
+        WF_CUDA(cudaEventCreateWithFlags(&r->fork_event, cudaEventDisableTiming));
+        WF_CUDA(cudaEventCreateWithFlags(&r->join_event, cudaEventDisableTiming));
+    }
     if (c.mode == WF_MODE_GRAPH) {
         if (wf_status e = capture_graph(rr)) return e;
     } else if (c.mode == WF_MODE_STREAM) {
@@ -1099,6 +1114,9 @@ wf_status renderer_destroy(wf_renderer* r) {
     }
     if (r->graph_exec) cudaGraphExecDestroy(r->graph_exec);
     if (r->graph) cudaGraphDestroy(r->graph);
+    if (r->fork_event) cudaEventDestroy(r->fork_event);
+    if (r->join_event) cudaEventDestroy(r->join_event);
+    if (r->side) cudaStreamDestroy(r->side);
     for (void* p : r->allocations) cudaFree(p);
     if (r->own_stream) cudaStreamDestroy(r->stream);
     delete r;

@@ -103,6 +103,9 @@ struct wf_renderer {
     float* framebuffer = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    // capture-time fork of the caustic gathers beside the shadow rays
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_event = nullptr, join_event = nullptr;
     uint32_t grid_resident[6] = {0, 0, 0, 0, 0, 0};  // trace, shade, shadow, finalize, gather, camera-ray trace
     wf::GatherQueue gathers{};                      // caustic gather requests (graph and streaming modes)
     uint32_t persistent_blocks = 0;

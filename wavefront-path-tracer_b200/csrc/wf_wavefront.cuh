@@ -7,10 +7,10 @@
 
 namespace wf {
 
-// Device-side launch count of the render kernels (kernels on one stream run
-// in order, so thread 0 of CTA 0 updates it without an atomic).
+// Device-side launch count of the render kernels (thread 0 of CTA 0 adds
+// one; graph branches can run two kernels at once).
 WF_DEV void count_launch(Counters* c) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) ++c->kernel_launches;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&c->kernel_launches, 1ull);
 }
 
 WF_DEV Path load_path(const PathSoA& ps, uint32_t p) {

@@ -269,6 +269,10 @@ typedef struct wf_render_config {
     uint32_t profile_queues;   /* record per-bounce queue counts */
     uint32_t refill_threshold; /* trace/shadow kernels: a warp fetches new rays once this many of its
                                   lanes are idle (1..32; 0 = default 8) */
+    uint32_t concurrent_tiles; /* graph mode: 2 (or 0 = default) = two wavefronts on two streams, each
+                                  rendering its own rows of every tile, so the long last bounces of one
+                                  overlap the other's work; 1 = one wavefront.  Each pixel stays with one
+                                  wavefront, so the sums are the same either way. */
 } wf_render_config;
 
 /* Defaults of RenderConfig (config.hpp:11-41) at the given resolution. */

@@ -97,6 +97,44 @@ def test_stream_mode_tiles_and_long_ranges(cuda):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
+@pytest.mark.parametrize("tiles", [None, (32, 24)])
+def test_two_wavefronts_match_one(cuda, tiles):
+    """Graph mode with the twin wavefront (default) against one wavefront:
+    identical sums, queue counts, ray counters and sample indices for frames,
+    odd-row tasks and one-row tasks."""
+    scene, cam = scenes.cornell_box(64, 48)
+    results = []
+    for concurrent in (1, 2):
+        fields = dict(max_depth=8, rr_start_depth=3, concurrent_tiles=concurrent)
+        if tiles:
+            fields.update(tile_width=tiles[0], tile_height=tiles[1])
+        cfg = wfpt.render_config(64, 48, **fields)
+        dev = wfpt.DeviceScene(scene)
+        r = wfpt.Renderer(dev, cam, cfg)
+        r.set_sample_index(40)
+        r.render_frame(3)
+        frame = r.download()
+        index = r.sample_index()
+        counts = r.queue_counts()
+        r.render(5, 7, 24, 17, 90, 2, True)
+        r.render(0, 3, 20, 1, 200, 3, True)
+        task = r.download()
+        after = r.sample_index()
+        r.render_frame(1)
+        stats = r.stats()
+        last = r.download()
+        r.close()
+        dev.close()
+        results.append((frame, index, counts, task, after, stats, last))
+    one, two = results
+    for a, b in ((one[0], two[0]), (one[3], two[3]), (one[6], two[6])):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert one[1] == two[1] == 43 and one[4] == two[4] == 203
+    assert np.array_equal(one[2], two[2])
+    for k in ("extension_rays", "shadow_rays", "paths"):
+        assert one[5][k] == two[5][k], k
+
+
 def test_ray_counters(cuda):
     got, counts, stats, want, want_counts, (_, _, _, spp) = render_both("cornell", abi.MODE_GRAPH)
     assert stats["extension_rays"] == int(want_counts.sum())

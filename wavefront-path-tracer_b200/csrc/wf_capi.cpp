@@ -3,7 +3,9 @@
 
 #include <chrono>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
+#include <vector>
 #include <fstream>
 #include <memory>
 
@@ -284,15 +286,20 @@ wf_status wf_framebuffer_reset(wf_renderer* r) {
     if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
     size_t pixels = size_t(r->config.width) * r->config.height;
     WF_CUDA(cudaMemsetAsync(r->framebuffer, 0, sizeof(float) * 3 * pixels, r->stream));
-    WF_CUDA(cudaMemsetAsync(&r->counters->sample_index, 0, sizeof(uint32_t), r->stream));
+    wf_renderer* parts[2];
+    for (int i = 0, n = renderer_parts(r, parts); i < n; ++i)
+        WF_CUDA(cudaMemsetAsync(&parts[i]->counters->sample_index, 0, sizeof(uint32_t), parts[i]->stream));
     return WF_OK;
 }
 
 wf_status wf_set_sample_index(wf_renderer* r, uint32_t sample_index) {
     if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
-    WF_CUDA(cudaMemcpyAsync(&r->counters->sample_index, &sample_index, sizeof(uint32_t), cudaMemcpyHostToDevice,
-                            r->stream));
-    WF_CUDA(cudaStreamSynchronize(r->stream));
+    wf_renderer* parts[2];
+    for (int i = 0, n = renderer_parts(r, parts); i < n; ++i) {
+        WF_CUDA(cudaMemcpyAsync(&parts[i]->counters->sample_index, &sample_index, sizeof(uint32_t),
+                                cudaMemcpyHostToDevice, parts[i]->stream));
+        WF_CUDA(cudaStreamSynchronize(parts[i]->stream));
+    }
     return WF_OK;
 }
 
@@ -306,10 +313,16 @@ wf_status wf_get_sample_index(wf_renderer* r, uint32_t* sample_index) {
 
 wf_status wf_synchronize(wf_renderer* r) {
     if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
-    WF_CUDA(cudaStreamSynchronize(r->stream));
     uint32_t flags[2] = {0, 0};
-    WF_CUDA(cudaMemcpy(flags, &r->counters->overflow, sizeof(flags) / 2, cudaMemcpyDeviceToHost));
-    WF_CUDA(cudaMemcpy(&flags[1], &r->counters->error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    wf_renderer* parts[2];
+    for (int i = 0, n = renderer_parts(r, parts); i < n; ++i) {
+        WF_CUDA(cudaStreamSynchronize(parts[i]->stream));
+        uint32_t f[2] = {0, 0};
+        WF_CUDA(cudaMemcpy(&f[0], &parts[i]->counters->overflow, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        WF_CUDA(cudaMemcpy(&f[1], &parts[i]->counters->error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        flags[0] |= f[0];
+        flags[1] = flags[1] ? flags[1] : f[1];
+    }
     if (flags[1] == wf::kErrorStreamBound)
         return fail(WF_ERR_TIMEOUT, "streaming loop exceeded samples x max_depth iterations");
     if (flags[1]) return fail(WF_ERR_TIMEOUT, "persistent kernel grid barrier timed out");
@@ -336,23 +349,36 @@ wf_status wf_framebuffer_device(wf_renderer* r, float** rgb) {
 wf_status wf_queue_counts(wf_renderer* r, uint32_t* counts, uint32_t n) {
     if (!r || !counts) return fail(WF_ERR_INVALID_ARG, "null argument");
     uint32_t m = std::min(n, r->config.max_depth);
-    WF_CUDA(cudaMemcpyAsync(counts, r->counters->profile, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost, r->stream));
-    WF_CUDA(cudaStreamSynchronize(r->stream));
+    std::vector<uint32_t> part(m);
+    std::fill(counts, counts + m, 0u);
+    wf_renderer* parts[2];
+    for (int i = 0, k = renderer_parts(r, parts); i < k; ++i) {  // the parts that rendered the last tile
+        if (!(r->last_tile_parts & (1u << i))) continue;
+        WF_CUDA(cudaMemcpyAsync(part.data(), parts[i]->counters->profile, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost,
+                                parts[i]->stream));
+        WF_CUDA(cudaStreamSynchronize(parts[i]->stream));
+        for (uint32_t b = 0; b < m; ++b) counts[b] += part[b];
+    }
     return WF_OK;
 }
 
 wf_status wf_render_stats_get(wf_renderer* r, wf_render_stats* stats, uint32_t reset) {
     if (!r || !stats) return fail(WF_ERR_INVALID_ARG, "null argument");
-    unsigned long long v[4];
-    WF_CUDA(cudaMemcpyAsync(v, &r->counters->extension_rays, sizeof(v), cudaMemcpyDeviceToHost, r->stream));
-    WF_CUDA(cudaStreamSynchronize(r->stream));
-    stats->extension_rays = v[0];
-    stats->shadow_rays = v[1];
-    stats->paths = v[2];
-    stats->kernel_launches = v[3];
-    if (reset) {
-        WF_CUDA(cudaMemsetAsync(&r->counters->extension_rays, 0, sizeof(v), r->stream));
-        WF_CUDA(cudaStreamSynchronize(r->stream));
+    std::memset(stats, 0, sizeof(*stats));
+    wf_renderer* parts[2];
+    for (int i = 0, n = renderer_parts(r, parts); i < n; ++i) {
+        unsigned long long v[4];
+        WF_CUDA(cudaMemcpyAsync(v, &parts[i]->counters->extension_rays, sizeof(v), cudaMemcpyDeviceToHost,
+                                parts[i]->stream));
+        WF_CUDA(cudaStreamSynchronize(parts[i]->stream));
+        stats->extension_rays += v[0];
+        stats->shadow_rays += v[1];
+        stats->paths += v[2];
+        stats->kernel_launches += v[3];
+        if (reset) {
+            WF_CUDA(cudaMemsetAsync(&parts[i]->counters->extension_rays, 0, sizeof(v), parts[i]->stream));
+            WF_CUDA(cudaStreamSynchronize(parts[i]->stream));
+        }
     }
     return WF_OK;
 }
@@ -466,6 +492,11 @@ wf_status wf_checkpoint_load(wf_renderer* r, const char* path, uint64_t fingerpr
     WF_CUDA(cudaMemcpyAsync(&r->counters->sample_index, &header.sample_index, sizeof(uint32_t), cudaMemcpyHostToDevice,
                             r->stream));
     WF_CUDA(cudaStreamSynchronize(r->stream));
+    if (r->twin) {
+        WF_CUDA(cudaMemcpyAsync(&r->twin->counters->sample_index, &header.sample_index, sizeof(uint32_t),
+                                cudaMemcpyHostToDevice, r->twin->stream));
+        WF_CUDA(cudaStreamSynchronize(r->twin->stream));
+    }
     *sample_index = header.sample_index;
     return WF_OK;
 }

@@ -973,8 +973,12 @@ wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
 
 }  // namespace
 
-wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const wf_render_config* cfg, void* stream,
-                          wf_renderer** out) {
+namespace {
+// external_framebuffer: render into this buffer instead of allocating one;
+// photon_source: reuse that renderer's photon map instead of building one.
+wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, const wf_render_config* cfg,
+                               void* stream, wf_renderer** out, float* external_framebuffer,
+                               const wf_renderer* photon_source) {
     if (!scene || !camera || !cfg || !out) return fail(WF_ERR_INVALID_ARG, "null argument");
     *out = nullptr;
     const wf_render_config& c = *cfg;
@@ -1041,9 +1045,14 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
     WF_CUDA(alloc(rr, &r->queue[1], cap));
     WF_CUDA(alloc(rr, &r->counters, 1));
     WF_CUDA(alloc(rr, &r->tile, 1));
-    WF_CUDA(alloc(rr, &r->framebuffer, size_t(pixels) * 3));
     WF_CUDA(cudaMemsetAsync(r->counters, 0, sizeof(Counters), r->stream));
-    WF_CUDA(cudaMemsetAsync(r->framebuffer, 0, sizeof(float) * 3 * size_t(pixels), r->stream));
+    if (external_framebuffer) {
+        r->framebuffer = external_framebuffer;
+        r->external_framebuffer = true;
+    } else {
+        WF_CUDA(alloc(rr, &r->framebuffer, size_t(pixels) * 3));
+        WF_CUDA(cudaMemsetAsync(r->framebuffer, 0, sizeof(float) * 3 * size_t(pixels), r->stream));
+    }
     if (c.mode != WF_MODE_PERSISTENT) {
         uint32_t requests_per_path = 5u + scene->view.directional_count;
         uint64_t shadow = uint64_t(cap) * requests_per_path;
@@ -1086,7 +1095,11 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
         r->persistent_blocks = std::max(1u, std::min(wanted, resident));
         r->chunk = c.chunk ? std::max(1u, c.chunk / 32) : 1u;
     }
-    if (c.caustics) {
+    if (c.caustics && photon_source) {
+        r->params.photons = photon_source->params.photons;
+        r->photons_emitted = photon_source->photons_emitted;
+        r->photons_stored = photon_source->photons_stored;
+    } else if (c.caustics) {
         if (wf_status e = build_photon_map(rr)) return e;
     }
     if (c.mode != WF_MODE_PERSISTENT) {
@@ -1103,9 +1116,37 @@ wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const 
     *out = r.release();
     return WF_OK;
 }
+}  // namespace
+
+wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const wf_render_config* cfg, void* stream,
+                          wf_renderer** out) {
+    wf_renderer* r = nullptr;
+    if (wf_status e = renderer_create_impl(scene, camera, cfg, stream, &r, nullptr, nullptr)) return e;
+    if (cfg->mode == WF_MODE_GRAPH && cfg->concurrent_tiles != 1) {
+        wf_render_config twin_config = *cfg;
+        twin_config.concurrent_tiles = 1;
+        wf_renderer* twin = nullptr;
+        wf_status e = renderer_create_impl(scene, camera, &twin_config, nullptr, &twin, r->framebuffer, r);
+        cudaError_t ce = cudaSuccess;
+        if (e == WF_OK) {
+            r->twin = twin;
+            ce = cudaEventCreateWithFlags(&r->twin_fork, cudaEventDisableTiming);
+            if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&r->twin_join, cudaEventDisableTiming);
+        }
+        if (e != WF_OK || ce != cudaSuccess) {
+            renderer_destroy(r);
+            return e != WF_OK ? e : cuda_fail(ce, "cudaEventCreateWithFlags");
+        }
+    }
+    *out = r;
+    return WF_OK;
+}
 
 wf_status renderer_destroy(wf_renderer* r) {
     if (!r) return WF_OK;
+    if (r->twin) renderer_destroy(r->twin);
+    if (r->twin_fork) cudaEventDestroy(r->twin_fork);
+    if (r->twin_join) cudaEventDestroy(r->twin_join);
     cudaStreamSynchronize(r->stream);
     for (auto& slot : r->slots) {
         if (slot->writer.joinable()) slot->writer.join();
@@ -1136,6 +1177,25 @@ wf_status renderer_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, ui
     }
     WF_CUDA(cudaMemcpyAsync(&r->counters->sample_index, &sample_start, sizeof(uint32_t), cudaMemcpyHostToDevice,
                             r->stream));
+    if (r->twin && h >= 2) {
+        // the top rows on this renderer, the bottom rows on the twin's stream
+        wf_renderer* t = r->twin;
+        uint32_t top = (h + 1) / 2;
+        WF_CUDA(cudaEventRecord(r->twin_fork, r->stream));
+        WF_CUDA(cudaStreamWaitEvent(t->stream, r->twin_fork, 0));
+        WF_CUDA(cudaMemcpyAsync(&t->counters->sample_index, &sample_start, sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                t->stream));
+        TileDev a{x, y, w, top, 1}, b{x, y + top, w, h - top, 1};
+        r->last_tile_parts = 3;
+        for (uint32_t s = 0; s < sample_count; ++s) {
+            if (wf_status e = launch_tile(r, a)) return e;
+            if (wf_status e = launch_tile(t, b)) return e;
+        }
+        WF_CUDA(cudaEventRecord(r->twin_join, t->stream));
+        WF_CUDA(cudaStreamWaitEvent(r->stream, r->twin_join, 0));
+        // both sample indices end at sample_start + sample_count
+        return WF_OK;
+    }
     TileDev tile{x, y, w, h, 1};
     if (c.mode == WF_MODE_STREAM) {
         tile.samples = sample_count;
@@ -1143,6 +1203,15 @@ wf_status renderer_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, ui
     }
     for (uint32_t s = 0; s < sample_count; ++s)
         if (wf_status e = launch_tile(r, tile)) return e;
+    r->last_tile_parts = 1;
+    if (r->twin) {  // a one-row task ran here alone: the twin's sample index follows
+        uint32_t end = sample_start + sample_count;
+        WF_CUDA(cudaEventRecord(r->twin_fork, r->stream));
+        WF_CUDA(cudaStreamWaitEvent(r->twin->stream, r->twin_fork, 0));
+        WF_CUDA(cudaMemcpyAsync(&r->twin->counters->sample_index, &end, sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                r->twin->stream));
+        WF_CUDA(cudaStreamSynchronize(r->twin->stream));
+    }
     return WF_OK;
 }
 
@@ -1163,6 +1232,46 @@ wf_status renderer_render_frame(wf_renderer* r, uint32_t sample_count) {
             tile.advance_sample = t + 1 == tiles.size() ? 1u : 0u;
             if (wf_status e = launch_tile(r, tile)) return e;
         }
+        return WF_OK;
+    }
+    if (r->twin) {
+        // Rows of a single frame tile, or whole tiles alternately, go to the
+        // two wavefronts; each advances its own sample index once per sample.
+        wf_renderer* twin = r->twin;
+        std::vector<TileDev> mine, theirs;
+        if (tiles.size() == 1 && tiles[0].height >= 2) {
+            TileDev a = tiles[0], b = tiles[0];
+            a.height = (tiles[0].height + 1) / 2;
+            b.y = tiles[0].y + a.height;
+            b.height = tiles[0].height - a.height;
+            mine.push_back(a);
+            theirs.push_back(b);
+        } else {
+            for (size_t t = 0; t < tiles.size(); ++t) (t % 2 ? theirs : mine).push_back(tiles[t]);
+        }
+        // queue counts report the frame's last tile: both halves, or the part that rendered it
+        r->last_tile_parts = theirs.empty() ? 1u : (mine.size() == 1 && theirs.size() == 1 && tiles.size() == 1)
+                                                        ? 3u
+                                                        : (tiles.size() % 2 ? 1u : 2u);
+        WF_CUDA(cudaEventRecord(r->twin_fork, r->stream));
+        WF_CUDA(cudaStreamWaitEvent(twin->stream, r->twin_fork, 0));
+        for (uint32_t s = 0; s < sample_count; ++s)
+            for (int part = 0; part < 2; ++part) {
+                std::vector<TileDev>& list = part ? theirs : mine;
+                for (size_t t = 0; t < list.size(); ++t) {
+                    TileDev tile = list[t];
+                    tile.advance_sample = t + 1 == list.size() ? 1u : 0u;
+                    if (wf_status e = launch_tile(part ? twin : r, tile)) return e;
+                }
+                if (list.empty() && part) {  // a single one-row frame: keep the twin's sample index in step
+                    TileDev idle{0, 0, 0, 0, 1};
+                    WF_CUDA(cudaMemcpyAsync(twin->tile, &idle, sizeof(TileDev), cudaMemcpyHostToDevice, twin->stream));
+                    k_advance<<<1, 1, 0, twin->stream>>>(twin->counters, twin->tile);
+                    WF_CUDA(cudaGetLastError());
+                }
+            }
+        WF_CUDA(cudaEventRecord(r->twin_join, twin->stream));
+        WF_CUDA(cudaStreamWaitEvent(r->stream, r->twin_join, 0));
         return WF_OK;
     }
     for (uint32_t s = 0; s < sample_count; ++s)
@@ -1365,6 +1474,14 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     WF_CUDA(cudaStreamSynchronize(st));
+    r->last_tile_parts = 1;
+    if (r->twin) {  // the pass ran on this renderer alone: bring the twin's sample index along
+        uint32_t index = 0;
+        if (wf_status e = read_back(&index, &r->counters->sample_index, sizeof(index))) return e;
+        WF_CUDA(cudaMemcpyAsync(&r->twin->counters->sample_index, &index, sizeof(index), cudaMemcpyHostToDevice,
+                                r->twin->stream));
+        WF_CUDA(cudaStreamSynchronize(r->twin->stream));
+    }
     return WF_OK;
 }
 

@@ -121,6 +121,13 @@ struct wf_renderer {
     uint32_t latest_written = 0;
     uint32_t last_tile_width = 0, last_tile_height = 0;
     wf::TallyTotals* tally = nullptr;  // [0] closest hit, [1] any hit (profiling pass)
+    // Graph mode with two wavefronts: the twin has its own buffers, graph and
+    // stream, renders into this renderer's framebuffer and reuses its photon
+    // map; each render call splits its rows between the two.
+    wf_renderer* twin = nullptr;
+    bool external_framebuffer = false;
+    uint32_t last_tile_parts = 1;  // which of {this, twin} rendered the last tile (bit 0, bit 1)
+    cudaEvent_t twin_fork = nullptr, twin_join = nullptr;
 };
 
 namespace wf {
@@ -131,6 +138,12 @@ wf_status renderer_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, ui
                           uint32_t sample_count, uint32_t clear);
 wf_status renderer_render_frame(wf_renderer* r, uint32_t sample_count);
 wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out);
+// The renderers that hold device counters: the renderer and its twin.
+inline int renderer_parts(wf_renderer* r, wf_renderer* parts[2]) {
+    parts[0] = r;
+    parts[1] = r->twin;
+    return r->twin ? 2 : 1;
+}
 wf_status trace_closest_batch(const wf_scene* scene, const wf_ray* rays, uint32_t count, wf_hit* hits,
                               cudaStream_t stream);
 wf_status trace_any_batch(const wf_scene* scene, const wf_ray* rays, const float* max_distance, uint32_t count,

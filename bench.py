@@ -439,6 +439,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--mode", default=None, choices=sorted(MODES), help="default: per workload")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: per workload)")
+    ap.add_argument("--concurrent-tiles", type=int, default=0,
+                    help="graph mode: 1 = one wavefront, 2 = two on two streams (default)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -468,7 +470,7 @@ def main():
     stream = torch.cuda.Stream()
     dev_scene = wfpt.DeviceScene(scene)
     args.mode = args.mode or DEFAULT_MODE[args.workload]
-    cfg = wfpt.render_config(width, height, mode=MODES[args.mode], **rkw)
+    cfg = wfpt.render_config(width, height, mode=MODES[args.mode], concurrent_tiles=args.concurrent_tiles, **rkw)
     spp = args.spp or SPP_PER_STEP[args.workload]
     renderer = wfpt.Renderer(dev_scene, cam, cfg, stream=stream.cuda_stream)
     setup_s = time.perf_counter() - t_setup
@@ -574,6 +576,7 @@ def main():
                        "max_depth": cfg.max_depth, "rr_start_depth": cfg.rr_start_depth,
                        "triangles": int(scene.triangle_count()), "instances": int(len(scene.instances)),
                        "photons": int(cfg.photon_count) if cfg.caustics else 0, "mode": args.mode,
+                       "wavefronts": 1 if args.mode != "graph" or args.concurrent_tiles == 1 else 2,
                        "scene_device_bytes": int(scene_bytes),
                        "l2": ("inputs larger than L2 (scene + path state on the device: "
                               f"{(scene_bytes + renderer_bytes) / 1e6:.0f} MB, no flush)"

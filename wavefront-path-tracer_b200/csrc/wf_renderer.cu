@@ -98,6 +98,7 @@ __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const 
         c->gather_count = 0;
         c->dense_count = 0;
         c->work_shade = 0;
+        for (int k = 0; k < 8; ++k) c->shade_bucket[k] = c->shade_cursor[k] = 0;
         if (bounce < kMaxBounces) c->profile[bounce] = n;
         c->extension_rays += n;
     }
@@ -150,11 +151,84 @@ __global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const 
     if constexpr (std::is_same<Tally, CountTally>::value) flush_tally(tally, totals);
 }
 
+// Shading categories: warps of k_shade take entries of one category at a
+// time, so they run one material branch instead of all of them.  Which warp
+// shades which path does not change any path's arithmetic: the outputs go to
+// the entry's own queue position.
+constexpr uint32_t kShadeCategories = 6;  // miss, emissive, diffuse, metal, dielectric, other
+
+WF_DEV uint32_t shade_category(const DeviceScene& s, float4 ha, uint32_t inst) {
+    uint32_t prim = __float_as_uint(ha.w);
+    uint32_t kind = hit_kind(prim), index = hit_index(prim);
+    if (kind == kHitMiss) return 0;
+    uint32_t m;
+    if (kind == kHitSphere) {
+        m = s.sphere_materials[index];
+    } else {
+        m = __float_as_uint(__ldg(&s.triangles[3 * size_t(index) + 1]).w);
+        if (kind == kHitMesh) {
+            uint32_t over = load_instance(s, inst).material_override;
+            if (over != kInvalid) m = over;
+        }
+    }
+    const Material& mat = s.materials[m];
+    if (mat.flags & kMatGltfPbr) return 5;
+    switch (mat.type) {
+    case kEmissive: return 1;
+    case kDiffuse: return mat.metallic > 0.5f ? 3 : 2;
+    case kMetal: return 3;
+    case kDielectric: return 4;
+    default: return 5;
+    }
+}
+
+__global__ void k_classify(const __grid_constant__ DeviceScene s, const uint32_t* count, const float4* hit_a,
+                           const uint32_t* hit_inst, uint8_t* key, Counters* c) {
+    count_launch(c);
+    __shared__ uint32_t histogram[kShadeCategories];
+    if (threadIdx.x < kShadeCategories) histogram[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t n = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t k = shade_category(s, hit_a[i], hit_inst[i]);
+        key[i] = uint8_t(k);
+        atomicAdd(&histogram[k], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < kShadeCategories && histogram[threadIdx.x])
+        atomicAdd(&c->shade_bucket[threadIdx.x], histogram[threadIdx.x]);
+}
+
+// Counting-sort scatter: within a warp, entries of one category keep their
+// order (ballot rank); warps reserve runs of each bucket with one atomic.
+__global__ void k_scatter(const uint32_t* count, const uint8_t* key, uint32_t* order, Counters* c) {
+    count_launch(c);
+    uint32_t n = *count;
+    uint32_t offset[kShadeCategories];
+    uint32_t run = 0;
+    for (uint32_t k = 0; k < kShadeCategories; ++k) {
+        offset[k] = run;
+        run += c->shade_bucket[k];
+    }
+    uint32_t lane = threadIdx.x & 31;
+    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = warp * 32; base < n; base += warps * 32) {
+        uint32_t i = base + lane;
+        uint32_t k = i < n ? key[i] : kShadeCategories;
+        unsigned peers = __match_any_sync(0xffffffffu, k);
+        uint32_t leader = __ffs(peers) - 1;
+        uint32_t start = 0;
+        if (lane == leader && k < kShadeCategories) start = atomicAdd(&c->shade_cursor[k], uint32_t(__popc(peers)));
+        start = __shfl_sync(0xffffffffu, start, leader);
+        if (k < kShadeCategories) order[offset[k] + start + __popc(peers & ((1u << lane) - 1u))] = i;
+    }
+}
+
 // 128 registers: 4 CTAs per SM; the few spills cost less than the lost warps.
 __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ RenderParams rp, PathSoA ps, const uint32_t* queue, const uint32_t* count,
                         const float4* hit_a, const uint32_t* hit_inst, float4* terms, int4* shade_out,
                         float4* shadow_origin, float4* shadow_dir, uint32_t shadow_capacity, Counters* c,
-                        uint32_t* next_count, GatherQueue gathers) {
+                        uint32_t* next_count, GatherQueue gathers, const uint32_t* order) {
     count_launch(c);
     uint32_t n = *count;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -166,8 +240,9 @@ __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ Device
     }
     uint32_t base;
     while (next_chunk(&c->work_shade, n, base)) {
-        uint32_t i = base + (threadIdx.x & 31);
-        if (i >= n) continue;
+        uint32_t j = base + (threadIdx.x & 31);
+        if (j >= n) continue;
+        uint32_t i = order ? order[j] : j;
         uint32_t p = queue[i];
         Path path = load_path(ps, p);
         float4 ha = hit_a[i];
@@ -845,9 +920,12 @@ wf_status capture_graph(wf_renderer* r) {
         else
             k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill);
+        k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
+                                                          r->counters);
+        k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order, r->counters);
         k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
-            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers);
+            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers, r->shade_order);
         bool fork = r->params.photons.enabled != 0;
         if (fork) {  // gathers on a parallel branch: they and the shadow rays write different buffers
             WF_CUDA(cudaEventRecord(r->fork_event, st));
@@ -911,9 +989,12 @@ wf_status capture_stream_graph(wf_renderer* r) {
         uint32_t* next_count = &r->counters->queue_count[nxt];
         k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
             s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, kMaxBounces, nullptr, r->refill);
+        k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
+                                                          r->counters);
+        k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order, r->counters);
         k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
-            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers);
+            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers, r->shade_order);
         bool fork = r->params.photons.enabled != 0;
         if (fork) {  // gathers on a parallel branch: they and the shadow rays write different buffers
             WF_CUDA(cudaEventRecord(r->fork_event, st));
@@ -1062,6 +1143,8 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
         WF_CUDA(alloc(rr, &r->hit_inst, cap));
         WF_CUDA(alloc(rr, &r->terms, size_t(cap) * kMaxTerms));
         WF_CUDA(alloc(rr, &r->shade_out, cap));
+        WF_CUDA(alloc(rr, &r->shade_key, cap));
+        WF_CUDA(alloc(rr, &r->shade_order, cap));
         WF_CUDA(alloc(rr, &r->shadow_origin, r->shadow_capacity));
         WF_CUDA(alloc(rr, &r->shadow_dir, r->shadow_capacity));
         WF_CUDA(alloc(rr, &r->shadow_result, r->shadow_capacity));
@@ -1386,11 +1469,15 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
                                 nullptr, r->refill);
                     };
-                    auto shade = [&] {
+                    auto shade = [&] {  // with the category sort it feeds on
+                        k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst,
+                                                                          r->shade_key, r->counters);
+                        k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order,
+                                                                         r->counters);
                         k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
                             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms,
                             r->shade_out, r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters,
-                            next_count, r->gathers);
+                            next_count, r->gathers, r->shade_order);
                     };
                     auto gather = [&] {
                         k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers,

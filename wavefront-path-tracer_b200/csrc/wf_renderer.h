@@ -40,6 +40,8 @@ struct Counters {
     uint32_t work_gather;
     uint32_t dense_count;        // gather requests deferred to the warp-per-request kernel
     uint32_t work_dense;
+    uint32_t shade_bucket[8];    // queue entries per shading category (current bounce)
+    uint32_t shade_cursor[8];
     uint32_t next_unit;          // job batch: next (job, pixel) unit to start
     unsigned long long extension_rays;
     unsigned long long shadow_rays;
@@ -107,6 +109,8 @@ struct wf_renderer {
     cudaStream_t side = nullptr;
     cudaEvent_t fork_event = nullptr, join_event = nullptr;
     uint32_t grid_resident[6] = {0, 0, 0, 0, 0, 0};  // trace, shade, shadow, finalize, gather, camera-ray trace
+    uint8_t* shade_key = nullptr;     // shading category of each queue entry
+    uint32_t* shade_order = nullptr;  // queue entries grouped by category (the order k_shade takes them)
     wf::GatherQueue gathers{};                      // caustic gather requests (graph and streaming modes)
     uint32_t persistent_blocks = 0;
     uint32_t persistent_block_size = 128;

@@ -143,5 +143,5 @@ def test_autograd_binding_and_descent(setup):
         with torch.no_grad():
             A.clamp_(0.01, 1.0)
             R.clamp_(0.0, 1.5)
-        losses.append(float(l))
+        losses.append(float(l.detach()))
     assert losses[-1] < 0.7 * losses[0]

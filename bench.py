@@ -71,6 +71,24 @@ def make_scene(name):
     return scene, cam, kw["width"], kw["height"], dict(rkw)
 
 
+def reference_cuda_comparison(workload):
+    """The reference's CUDA renderer (oracle/_ref/libwfref_cuda.so) and this
+    renderer timed the same way on the same tasks, in a child process
+    (oracle/ref_cuda_bench.py; caustics off on both sides)."""
+    script = ROOT / "oracle" / "ref_cuda_bench.py"
+    if not (ROOT / "oracle" / "_ref" / "libwfref_cuda.so").exists():
+        return {"unavailable": "reference CUDA build absent (make -C oracle cuda)"}
+    out = {}
+    for mode in ("graph", "persistent"):
+        run = subprocess.run([sys.executable, str(script), "--workload", workload, "--mode", mode, "--steps", "5"],
+                             capture_output=True, text=True, timeout=1200, cwd=ROOT)
+        if run.returncode != 0:
+            out[mode] = {"failed": (run.stdout + run.stderr)[-300:]}
+            continue
+        out[mode] = json.loads(run.stdout.strip().splitlines()[-1])
+    return out
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -396,6 +414,10 @@ def run_batch(args):
     for r in renderers:
         r.close()
     batch.close()
+    reference_cuda = None
+    if rank == 0 and world == 1 and args.reference_cuda:
+        reference_cuda = reference_cuda_comparison(args.workload)
+
     if rank == 0:
         line = {
             "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
@@ -441,6 +463,9 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: per workload)")
     ap.add_argument("--concurrent-tiles", type=int, default=0,
                     help="graph mode: 1 = one wavefront, 2 = two on two streams (default)")
+    ap.add_argument("--reference-cuda", action="store_true",
+                    help="also time the reference's own CUDA renderer built for sm_100a (make -C oracle cuda) "
+                         "beside this one, both through their task calls, and add it as `reference_cuda`")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -567,6 +592,10 @@ def main():
         except FileNotFoundError as e:
             cpu = {"value": None, "unit": "Mpaths/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
+    reference_cuda = None
+    if rank == 0 and world == 1 and args.reference_cuda:
+        reference_cuda = reference_cuda_comparison(args.workload)
+
     if rank == 0:
         line = {
             "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
@@ -594,6 +623,8 @@ def main():
             "clocks": clock_record,
             "setup_seconds": setup_s,
         }
+        if reference_cuda is not None:
+            line["reference_cuda"] = reference_cuda
         print(json.dumps(line), flush=True)
     renderer.close()
     dev_scene.close()

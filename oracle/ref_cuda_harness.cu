@@ -1,0 +1,196 @@
+// ORACLE / TEST INFRASTRUCTURE ONLY -- never linked into or called by the
+// product.  Only bench.py's --reference-cuda measurement and the script beside
+// it (oracle/ref_cuda_bench.py) load the library built from this file
+// (oracle/_ref/libwfref_cuda.so).
+//
+// The reference's own CUDA renderer on this GPU: its sources (src/scene/scene.cu,
+// src/renderer/renderer.cu, render_driver.cu, render_task.cu, ...) are
+// compiled unmodified for sm_100a by oracle/Makefile (target `cuda`), with the
+// reference's separable compilation and nvcc's default floating-point flags.
+// This file only converts the C-ABI scene description into the reference's
+// HostScene (ref_scene_convert.h), calls the reference's uploadScene and
+// uploadEnvironmentMap, and renders whole-frame tasks through the reference's
+// RenderTaskRenderer::render (src/renderer/render_task.cu:26-114), the call a
+// distributed worker makes: clear the tile, render the sample range with the
+// captured graph or the persistent kernel, download the radiance.
+//
+// NexusBVH is absent, so the BVH2 builds that scene.cu asks for are answered
+// here with the project's binned-SAH builder (the same trees the host build of
+// the reference and the B200 renderer traverse), built on the host and
+// uploaded (shim_cuda/NXB/BVH.h).
+#include "config.hpp"
+#include "renderer/image_output.hpp"
+#include "renderer/render_driver.cuh"
+#include "renderer/render_fingerprint.hpp"
+#include "renderer/render_task.cuh"
+#include "scene/environment.hpp"
+#include "scene/scene_host.hpp"
+
+#include "../wavefront-path-tracer_b200/csrc/bvh_build.h"
+#include "ref_scene_convert.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+// ------------------------------------------------------------ NXB builder
+namespace {
+NXB::BVH2 build_nexus(std::vector<wf::BvhBox>& boxes) {
+    std::vector<wf::BvhBinaryNode> nodes;
+    wf::build_binary_bvh(boxes.data(), uint32_t(boxes.size()), nodes, 0);
+    std::vector<NXB::BVH2::Node> host(nodes.size());
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        const wf::BvhBinaryNode& n = nodes[i];
+        host[i].bounds = NXB::AABB(make_float3(n.box.lo[0], n.box.lo[1], n.box.lo[2]),
+                                   make_float3(n.box.hi[0], n.box.hi[1], n.box.hi[2]));
+        host[i].leftChild = n.left;
+        host[i].rightChild = n.right;
+    }
+    NXB::BVH2 bvh;
+    bvh.nodes_ = NXB::detail::device_copy(host.data(), host.size());
+    bvh.nodeCount_ = uint32_t(host.size());
+    bvh.primCount_ = uint32_t(boxes.size());
+    if (!host.empty()) bvh.bounds_ = host.back().bounds;  // the root is the last node
+    return bvh;
+}
+
+void download(void* dst, const void* src, size_t bytes) {
+    if (bytes && cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw std::runtime_error("NXB shim: cudaMemcpy from the device failed");
+}
+}  // namespace
+
+namespace NXB {
+BVH2 BuildBVH2(const Triangle* triangles, uint32_t count, BuildConfig, BVHBuildMetrics*) {
+    static_assert(sizeof(Triangle) == 9 * sizeof(float), "NXB::Triangle is three float3");
+    std::vector<float> v(size_t(count) * 9);
+    download(v.data(), triangles, sizeof(Triangle) * size_t(count));
+    std::vector<wf::BvhBox> boxes(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        const float* t = &v[size_t(i) * 9];
+        for (int a = 0; a < 3; ++a) {
+            boxes[i].lo[a] = std::min(std::min(t[a], t[3 + a]), t[6 + a]);
+            boxes[i].hi[a] = std::max(std::max(t[a], t[3 + a]), t[6 + a]);
+        }
+    }
+    return build_nexus(boxes);
+}
+BVH2 BuildBVH2(const AABB* aabbs, uint32_t count, BuildConfig, BVHBuildMetrics*) {
+    std::vector<AABB> host(count);
+    download(host.data(), aabbs, sizeof(AABB) * size_t(count));
+    std::vector<wf::BvhBox> boxes(count);
+    for (uint32_t i = 0; i < count; ++i)
+        boxes[i] = wf::BvhBox{{host[i].bMin.x, host[i].bMin.y, host[i].bMin.z},
+                              {host[i].bMax.x, host[i].bMax.y, host[i].bMax.z}};
+    return build_nexus(boxes);
+}
+BVH8 BuildBVH8(const Triangle*, uint32_t, BuildConfig, BVHBuildMetrics*) {
+    throw std::runtime_error("BVH8 is not provided by the NexusBVH shim");
+}
+}  // namespace NXB
+
+// RenderDriver::writeFinalImage (render_driver.cu:403-418) is reached only
+// from RenderDriver::run, which this harness does not call; the PPM writer
+// and its SHA-256 digest (image_output.cpp, OpenSSL) are not linked.
+std::string sha256Framebuffer(const std::vector<Vec3>&) { return std::string(); }
+void writePpm(const char*, const std::vector<Vec3>&, uint32_t, uint32_t) {}
+
+namespace {
+struct CudaRefScene {
+    DeviceScene device;
+};
+}  // namespace
+
+extern "C" {
+
+void* wfcuda_scene_create(const wf_scene_desc* d, const wf_environment* env) {
+    try {
+        HostScene h;
+        wfref::host_scene_from_desc(d, false, h);
+        auto r = std::make_unique<CudaRefScene>();
+        r->device = uploadScene(h);
+        r->device.scene.ignoreDirectLightOcclusion = d->ignore_direct_light_occlusion != 0;
+        if (env && env->width && env->height) {
+            HostEnvironment map;
+            map.width = env->width;
+            map.height = env->height;
+            map.pixels.resize(size_t(env->width) * env->height);
+            for (size_t i = 0; i < map.pixels.size(); ++i)
+                map.pixels[i] = make_float4(env->rgba[4 * i], env->rgba[4 * i + 1], env->rgba[4 * i + 2],
+                                            env->rgba[4 * i + 3]);
+            buildEnvironmentDistribution(map);
+            uploadEnvironmentMap(r->device, map, env->intensity, env->rotation_degrees);
+        }
+        if (cudaDeviceSynchronize() != cudaSuccess) return nullptr;
+        return r.release();
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "wfcuda_scene_create: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+void wfcuda_scene_destroy(void* handle) {
+    CudaRefScene* r = static_cast<CudaRefScene*>(handle);
+    if (!r) return;
+    destroyDeviceScene(r->device);
+    delete r;
+}
+
+// Renders one warm-up task and then `steps` whole-frame tasks of `spp`
+// samples each (absolute samples from sample_start on) through
+// RenderTaskRenderer::render.  task_ms[i] is the wall time of task i, which
+// covers the reference's own clear, launches, stream synchronisation and
+// download; rgb (optional) receives the last task's unnormalised sums.
+// Caustics stay off: the reference builds a photon map only for its Cornell
+// family of presets, with fixed Cornell grid bounds (render_driver.cu:180-214).
+int wfcuda_render(void* handle, const wf_camera* cam, const wf_render_config* c, int persistent,
+                  uint32_t sample_start, uint32_t spp, uint32_t steps, float* rgb, double* task_ms) {
+    try {
+        CudaRefScene* r = static_cast<CudaRefScene*>(handle);
+        if (!r || spp == 0) return 1;
+        Camera camera;
+        camera.position = wfref::v3(cam->position);
+        camera.forward = wfref::v3(cam->forward);
+        camera.right = wfref::v3(cam->right);
+        camera.up = wfref::v3(cam->up);
+        camera.verticalFov = cam->vertical_fov;
+        camera.aspectRatio = cam->aspect_ratio;
+        RenderConfig config;
+        config.width = c->width;
+        config.height = c->height;
+        config.maxDepth = c->max_depth;
+        config.russianRouletteStartDepth = c->rr_start_depth;
+        config.samplesPerPixel = 1u << 30;  // bounds the absolute sample ranges of tasks
+        config.persistentWavefront = persistent != 0;
+        config.indirectRadianceClamp = c->indirect_clamp;
+        config.rngStrategy = RngStrategy(c->rng);
+        config.enableCaustics = false;
+        config.distributedRole = DistributedRole::Worker;  // no local checkpoint writer
+        SceneConfig scene_config;
+        scene_config.preset = ScenePreset::Demo;
+        RenderDriver driver(r->device, camera, config, scene_config);
+        RenderTaskRenderer renderer(driver);
+        RenderTask task;
+        task.jobFingerprint = computeRenderFingerprint(config, scene_config);
+        task.tile = DistributedTile{0, 0, c->width, c->height};
+        for (uint32_t i = 0; i <= steps; ++i) {
+            task.id = RenderTaskId{0, sample_start + i * spp, spp};
+            auto t0 = std::chrono::steady_clock::now();
+            RenderTaskResult result = renderer.render(task);
+            auto t1 = std::chrono::steady_clock::now();
+            if (!result.success) return 2;
+            if (i > 0) task_ms[i - 1] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+            if (i == steps && rgb) std::memcpy(rgb, result.radiance.data(), sizeof(float) * 3 * result.radiance.size());
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "wfcuda_render: %s\n", e.what());
+        return 3;
+    }
+}
+
+}  // extern "C"

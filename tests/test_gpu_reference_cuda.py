@@ -1,0 +1,45 @@
+"""The reference's own CUDA renderer on the same GPU.
+
+oracle/_ref/libwfref_cuda.so is the reference's renderer compiled for sm_100a
+from its own sources (`make -C oracle cuda`; nvcc's default floating-point
+flags, so multiply-adds are contracted there and not here).  Both renderers
+run the same seeded scene, camera and absolute sample range through their
+task calls: the reference's RenderTaskRenderer::render and this renderer's
+wf_render + wf_framebuffer_download.  The two images are the same paths, so
+their relative RMSE (root-mean-square difference over the root-mean-square
+of the reference image) only reflects contraction and elementary-function
+rounding: it must stay below 1 % on the Cornell box (16 spp) and below 2 % on
+the reduced large mesh (4 spp; terrain, 50 instances, glass spheres, HDR
+environment with a 5e4 sun, caustics off on both sides because the reference
+builds photon maps only for its Cornell presets).
+
+The comparison runs in a child process (oracle/ref_cuda_bench.py), so the
+reference's exit-on-error cannot end the test session.  Skipped when the
+library has not been built.
+"""
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+LIB = ROOT / "oracle" / "_ref" / "libwfref_cuda.so"
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not LIB.exists(), reason="reference CUDA build absent (make -C oracle cuda)")]
+
+
+@pytest.mark.parametrize("workload,mode,tolerance", [
+    ("cornell", "graph", 0.01),
+    ("cornell", "persistent", 0.01),
+    ("large_mesh_small", "graph", 0.02),
+])
+def test_image_matches_reference_cuda_renderer(cuda, workload, mode, tolerance):
+    run = subprocess.run([sys.executable, str(ROOT / "oracle" / "ref_cuda_bench.py"), "--workload", workload,
+                          "--mode", mode, "--steps", "1"], capture_output=True, text=True, timeout=900, cwd=ROOT)
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr[-2000:]
+    line = json.loads(run.stdout.strip().splitlines()[-1])
+    assert line["reference_cuda"]["Mpaths/s"] > 0 and line["b200_renderer"]["Mpaths/s"] > 0
+    assert line["image_relative_rmse"] <= tolerance, line

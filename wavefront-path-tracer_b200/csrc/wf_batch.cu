@@ -115,8 +115,9 @@ __global__ void k_batch_raygen(BatchView b, Counters* c, PathSoA ps, uint32_t* q
     }
 }
 
+// At most 72 registers, as k_trace (7 CTAs of 128 per SM instead of 6).
 template <typename Tally>
-__global__ void k_batch_trace(BatchView b, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
+__global__ void __maxnreg__(72) k_batch_trace(BatchView b, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
                               uint32_t* hit_inst, Counters* c, uint32_t refill_at) {
     count_launch(c);
     uint32_t n = *count;

@@ -87,8 +87,11 @@ __global__ void k_raygen_stream(RenderParams rp, const TileDev* tile_ptr, Counte
 // warp takes 32 consecutive queue entries and every lane runs its ray to the
 // end (camera rays: neighbouring pixels visit the same nodes in lockstep).
 // The per-ray visit order and arithmetic are the same either way.
+// At most 72 registers (7 CTAs of 128 per SM): 8 bytes of spill cost less
+// than the warps a 79-register allocation (6 CTAs) leaves out; a 64-register
+// cap spills far more.  __maxnreg__ keeps every block size launchable.
 template <typename Tally, bool kLanes = true>
-__global__ void k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
+__global__ void __maxnreg__(72) k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
                         uint32_t* hit_inst, Counters* c, uint32_t bounce, TallyTotals* totals, uint32_t refill_at) {
     count_launch(c);
     uint32_t n = *count;

@@ -463,6 +463,8 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: per workload)")
     ap.add_argument("--concurrent-tiles", type=int, default=0,
                     help="graph mode: 1 = one wavefront, 2 = two on two streams (default)")
+    ap.add_argument("--bvh-builder", default="host", choices=["host", "gpu"],
+                    help="BVH2 builder of the scene: host binned SAH (default) or GPU PLOC")
     ap.add_argument("--reference-cuda", action="store_true",
                     help="also time the reference's own CUDA renderer built for sm_100a (make -C oracle cuda) "
                          "beside this one, both through their task calls, and add it as `reference_cuda`")
@@ -493,7 +495,9 @@ def main():
         rkw.setdefault("photon_grid_min", (0, 0, 0))  # min == max: grid bounds derived from the photons
         rkw.setdefault("photon_grid_max", (0, 0, 0))
     stream = torch.cuda.Stream()
+    scene.bvh_builder = wfpt.abi.BVH_GPU_PLOC if args.bvh_builder == "gpu" else wfpt.abi.BVH_HOST_SAH
     dev_scene = wfpt.DeviceScene(scene)
+    scene_info = dev_scene.info()
     args.mode = args.mode or DEFAULT_MODE[args.workload]
     cfg = wfpt.render_config(width, height, mode=MODES[args.mode], concurrent_tiles=args.concurrent_tiles, **rkw)
     spp = args.spp or SPP_PER_STEP[args.workload]
@@ -607,6 +611,8 @@ def main():
                        "photons": int(cfg.photon_count) if cfg.caustics else 0, "mode": args.mode,
                        "wavefronts": 1 if args.mode != "graph" or args.concurrent_tiles == 1 else 2,
                        "scene_device_bytes": int(scene_bytes),
+                       "bvh_builder": args.bvh_builder, "bvh_build_ms": round(float(scene_info.bvh_build_ms), 1),
+                       "gpu_bvh_builds": int(scene_info.gpu_bvh_builds),
                        "l2": ("inputs larger than L2 (scene + path state on the device: "
                               f"{(scene_bytes + renderer_bytes) / 1e6:.0f} MB, no flush)"
                               if scene_bytes + renderer_bytes > 126e6 else

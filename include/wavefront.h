@@ -160,7 +160,17 @@ typedef struct wf_scene_desc {
      * addStaticTriangleLights, src/scene/scene_host.cpp:60-106). */
     uint32_t register_triangle_lights;
     uint32_t build_threads; /* 0 = all host threads */
+    /* WF_BVH_HOST_SAH (0, default): binned-SAH BVH2s built on the host.
+     * WF_BVH_GPU_PLOC: BVH2s over >= 4096 primitives built on the GPU by
+     * PLOC (the role of the reference's NexusBVH builder, scene.cu:148-149,
+     * 227-228, 262-264); smaller ones, and any build that fails or exceeds
+     * the 60-level depth bound, use the host builder.  No counterpart field
+     * in the reference. */
+    uint32_t bvh_builder;
+    uint32_t reserved;
 } wf_scene_desc;
+
+enum { WF_BVH_HOST_SAH = 0, WF_BVH_GPU_PLOC = 1 };
 
 typedef struct wf_scene wf_scene;
 
@@ -182,8 +192,20 @@ typedef struct wf_scene_info {
     uint32_t material_count;
     uint64_t device_bytes;
     double build_seconds;
+    uint32_t gpu_bvh_builds;  /* BVH2s the GPU builder produced */
+    float bvh_build_ms;       /* wall time of all BVH2 builds of the scene */
 } wf_scene_info;
 wf_status wf_scene_get_info(const wf_scene* scene, wf_scene_info* info);
+
+/* Builds one binary BVH2 over `count` boxes (6 floats each: lo xyz, hi xyz)
+ * with WF_BVH_HOST_SAH or WF_BVH_GPU_PLOC (on the current device) and writes
+ * its 2*count-1 nodes, 8 words each: box (6 floats), left, right.  A leaf has
+ * left = 0xffffffff and right = its box index; the root is the last node.
+ * `milliseconds` (optional) receives the build's wall time.  No counterpart
+ * in the reference (whose builder, NexusBVH, is absent): it exposes the two
+ * builders behind wf_scene_desc::bvh_builder for validation and timing. */
+wf_status wf_bvh_build(uint32_t builder, const float* boxes, uint32_t count, uint32_t* nodes,
+                       double* milliseconds);
 
 /* ------------------------------------------------------- ray-level queries */
 /* One ray: origin xyz, direction xyz (float). */

@@ -1,0 +1,476 @@
+// GPU BVH2 builder: PLOC (Meister and Bittner, "Parallel Locally-Ordered
+// Clustering for Bounding Volume Hierarchy Construction", IEEE TVCG 2018).
+//
+// The reference builds its BVH2s on the GPU with NexusBVH (an H-PLOC builder
+// in an un-vendored submodule, called at src/scene/scene.cu:148-149,227-228,
+// 262-264).  This is this build's GPU builder for the same role:
+//   1. primitive centroids are quantised to 21 bits per axis and interleaved
+//      into 63-bit Morton keys;
+//   2. a stable LSD radix sort (8-bit digits, hand-written) orders the
+//      primitives along the curve;
+//   3. clusters start as one leaf per primitive in that order; each round,
+//      every cluster finds the neighbour within +-kPlocRadius positions whose
+//      union box has the smallest surface area (symmetric tie-breaks, see
+//      k_nearest), mutual nearest neighbours merge into a new node (the
+//      lower position keeps it), and an exclusive scan compacts the
+//      survivors and numbers the new nodes;
+//   4. rounds repeat until one cluster is left (at most kMaxRounds; the
+//      caller falls back to the host builder beyond that).
+// Every step is deterministic (stable sort, index tie-breaks, scan-ordered
+// node numbering), so a scene always gets the same tree.  The output is the
+// host builder's format (bvh_build.h): 2n-1 nodes, leaves first with
+// left == kInvalidChild and right == primitive, the root last.
+#include "bvh_build.h"
+#include "wf_bvh_gpu.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+namespace wf {
+namespace {
+
+constexpr int kPlocRadius = 16;
+constexpr int kSortThreads = 256;
+constexpr int kSortChunks = 16;  // elements per sort block = threads x chunks
+constexpr int kSortTile = kSortThreads * kSortChunks;
+constexpr int kScanThreads = 1024;
+constexpr int kNearestThreads = 256;
+constexpr int kMaxRounds = 512;
+
+__device__ __forceinline__ float half_area(const BvhBox& b) {
+    float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__device__ __forceinline__ BvhBox merged(const BvhBox& a, const BvhBox& b) {
+    BvhBox r;
+    for (int k = 0; k < 3; ++k) {
+        r.lo[k] = fminf(a.lo[k], b.lo[k]);
+        r.hi[k] = fmaxf(a.hi[k], b.hi[k]);
+    }
+    return r;
+}
+
+// Floats as order-preserving unsigned integers, for atomicMin/atomicMax.
+__device__ __forceinline__ uint32_t ordered(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__host__ __device__ inline float unordered(uint32_t u) {
+    uint32_t v = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+    float f;
+    memcpy(&f, &v, 4);
+    return f;
+}
+
+// Centroid bounds: bounds[0..2] = ordered min, bounds[3..5] = ordered max.
+__global__ void k_centroid_bounds(const BvhBox* prims, uint32_t n, uint32_t* bounds) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        for (int k = 0; k < 3; ++k) {
+            float c = 0.5f * (prims[i].lo[k] + prims[i].hi[k]);
+            lo[k] = fminf(lo[k], c);
+            hi[k] = fmaxf(hi[k], c);
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        for (int off = 16; off > 0; off >>= 1) {
+            lo[k] = fminf(lo[k], __shfl_down_sync(0xffffffffu, lo[k], off));
+            hi[k] = fmaxf(hi[k], __shfl_down_sync(0xffffffffu, hi[k], off));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(&bounds[k], ordered(lo[k]));
+            atomicMax(&bounds[3 + k], ordered(hi[k]));
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned long long spread21(uint32_t v) {
+    unsigned long long x = v & 0x1fffffu;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+
+__global__ void k_morton(const BvhBox* prims, uint32_t n, const uint32_t* bounds, unsigned long long* keys,
+                         uint32_t* values) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t q[3];
+    for (int k = 0; k < 3; ++k) {
+        float lo = unordered(bounds[k]), hi = unordered(bounds[3 + k]);
+        float extent = hi - lo;
+        float c = 0.5f * (prims[i].lo[k] + prims[i].hi[k]);
+        float t = extent > 0.0f ? (c - lo) / extent : 0.0f;
+        t = fminf(fmaxf(t, 0.0f), 1.0f);
+        q[k] = min(uint32_t(t * 2097151.0f), 2097151u);
+    }
+    keys[i] = spread21(q[0]) | spread21(q[1]) << 1 | spread21(q[2]) << 2;
+    values[i] = i;
+}
+
+// ---------------------------------------------------------- radix sort
+// Per-block digit histograms, digit-major: hist[digit * blocks + block].
+__global__ void k_sort_histogram(const unsigned long long* keys, uint32_t n, int shift, uint32_t* hist) {
+    __shared__ uint32_t count[256];
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) count[d] = 0;
+    __syncthreads();
+    uint32_t base = blockIdx.x * kSortTile;
+    for (int c = 0; c < kSortChunks; ++c) {
+        uint32_t i = base + c * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&count[(keys[i] >> shift) & 0xffu], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[size_t(d) * gridDim.x + blockIdx.x] = count[d];
+}
+
+// Stable scatter: within a tile, elements keep their order per digit (warp
+// match ranks, then warps in order, then chunks in order).
+__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const unsigned long long* keys_in,
+                                                               const uint32_t* values_in, uint32_t n, int shift,
+                                                               const uint32_t* offsets,
+                                                               unsigned long long* keys_out,
+                                                               uint32_t* values_out) {
+    constexpr int kWarps = kSortThreads / 32;
+    __shared__ uint32_t running[256];
+    __shared__ uint32_t warp_count[kWarps][256];
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) running[d] = offsets[size_t(d) * gridDim.x + blockIdx.x];
+    for (int k = threadIdx.x; k < kWarps * 256; k += blockDim.x) (&warp_count[0][0])[k] = 0;
+    __syncthreads();
+    uint32_t base = blockIdx.x * kSortTile;
+    for (int c = 0; c < kSortChunks; ++c) {
+        uint32_t i = base + c * kSortThreads + threadIdx.x;
+        bool valid = i < n;
+        unsigned long long key = valid ? keys_in[i] : 0ull;
+        uint32_t value = valid ? values_in[i] : 0u;
+        uint32_t digit = valid ? uint32_t((key >> shift) & 0xffu) : 256u;
+        unsigned peers = __match_any_sync(0xffffffffu, digit);
+        uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+        if (valid && lane == __ffs(peers) - 1) warp_count[warp][digit] = __popc(peers);
+        __syncthreads();
+        for (int d = threadIdx.x; d < 256; d += blockDim.x) {
+            uint32_t run = running[d];
+            for (int w = 0; w < kWarps; ++w) {
+                uint32_t t = warp_count[w][d];
+                warp_count[w][d] = run;
+                run += t;
+            }
+            running[d] = run;
+        }
+        __syncthreads();
+        if (valid) {
+            uint32_t pos = warp_count[warp][digit] + rank;
+            keys_out[pos] = key;
+            values_out[pos] = value;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < kWarps * 256; k += blockDim.x) (&warp_count[0][0])[k] = 0;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ scan
+// Exclusive scan of one kScanThreads-element block; block sums to `sums`.
+__global__ void __launch_bounds__(kScanThreads) k_scan_block(const uint32_t* in, uint32_t* out, uint32_t n,
+                                                             uint32_t* sums) {
+    __shared__ uint32_t warp_sum[kScanThreads / 32];
+    uint32_t i = blockIdx.x * kScanThreads + threadIdx.x;
+    uint32_t v = i < n ? in[i] : 0u;
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+    for (int off = 1; off < 32; off <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_sum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = warp_sum[lane];
+        for (int off = 1; off < 32; off <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, off);
+            if (lane >= off) s += y;
+        }
+        warp_sum[lane] = s;
+    }
+    __syncthreads();
+    uint32_t warp_base = warp ? warp_sum[warp - 1] : 0u;
+    if (i < n) out[i] = warp_base + x - v;
+    if (threadIdx.x == kScanThreads - 1 && sums) sums[blockIdx.x] = warp_base + x;
+}
+
+__global__ void k_scan_add(uint32_t* data, uint32_t n, const uint32_t* block_offsets) {
+    uint32_t i = blockIdx.x * kScanThreads + threadIdx.x;
+    if (i < n && blockIdx.x > 0) data[i] += block_offsets[blockIdx.x];
+}
+
+struct Scratch {
+    std::vector<void*> blocks;
+    cudaError_t error = cudaSuccess;
+    template <typename T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        if (error == cudaSuccess) error = cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1));
+        if (error == cudaSuccess) blocks.push_back(p);
+        return static_cast<T*>(p);
+    }
+    ~Scratch() {
+        for (void* p : blocks) cudaFree(p);
+    }
+};
+
+// Exclusive scan of n values in place-free form (in -> out), any n.
+cudaError_t exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t st, Scratch& scratch) {
+    if (n == 0) return cudaSuccess;
+    uint32_t blocks = (n + kScanThreads - 1) / kScanThreads;
+    uint32_t* sums = blocks > 1 ? scratch.alloc<uint32_t>(blocks) : nullptr;
+    if (scratch.error != cudaSuccess) return scratch.error;
+    k_scan_block<<<blocks, kScanThreads, 0, st>>>(in, out, n, sums);
+    if (blocks == 1) return cudaGetLastError();
+    uint32_t* sum_offsets = scratch.alloc<uint32_t>(blocks);
+    if (scratch.error != cudaSuccess) return scratch.error;
+    if (cudaError_t e = exclusive_scan(sums, sum_offsets, blocks, st, scratch)) return e;
+    k_scan_add<<<blocks, kScanThreads, 0, st>>>(out, n, sum_offsets);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ PLOC
+__global__ void k_leaves(const BvhBox* prims, const uint32_t* order, uint32_t n, BvhBinaryNode* nodes,
+                         uint32_t* clusters, BvhBox* boxes, uint32_t* heights) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    nodes[i] = BvhBinaryNode{prims[i], kInvalidChild, i};
+    uint32_t p = order[i];
+    clusters[i] = p;
+    boxes[i] = prims[p];
+    heights[i] = 0;
+}
+
+// Nearest neighbour of every cluster within +-kPlocRadius: the candidate
+// with the smallest key (union surface area, distance in the curve order,
+// not being the position's pair partner i^1, lower position).  The key is
+// symmetric in the two positions, so the pair with the smallest key over the
+// whole array is mutual and every round merges at least once; clusters with
+// equal boxes pair up as (2k, 2k+1) and halve each round.  Boxes of the
+// block's clusters and the halo are staged in shared memory.
+__global__ void __launch_bounds__(kNearestThreads) k_nearest(const BvhBox* boxes, uint32_t m, uint32_t* nearest) {
+    __shared__ BvhBox tile[kNearestThreads + 2 * kPlocRadius];
+    int first = int(blockIdx.x * kNearestThreads) - kPlocRadius;
+    for (int k = threadIdx.x; k < kNearestThreads + 2 * kPlocRadius; k += blockDim.x) {
+        int j = first + k;
+        if (j >= 0 && j < int(m)) tile[k] = boxes[j];
+    }
+    __syncthreads();
+    int i = int(blockIdx.x * kNearestThreads + threadIdx.x);
+    if (i >= int(m)) return;
+    const BvhBox& mine = tile[threadIdx.x + kPlocRadius];
+    float best = INFINITY;
+    int best_j = -1, best_d = 0, best_other = 0;
+    int lo = max(0, i - kPlocRadius), hi = min(int(m) - 1, i + kPlocRadius);
+    for (int j = lo; j <= hi; ++j) {  // ascending j: equal keys keep the lower position
+        if (j == i) continue;
+        float a = half_area(merged(mine, tile[j - first]));
+        int d = abs(j - i), other = j != (i ^ 1);
+        bool better = best_j < 0 || a < best || (a == best && (d < best_d || (d == best_d && other < best_other)));
+        if (better) {
+            best = a;
+            best_j = j;
+            best_d = d;
+            best_other = other;
+        }
+    }
+    nearest[i] = uint32_t(best_j < 0 ? i : best_j);
+}
+
+// alive: not the upper half of a mutual pair; leader: lower half of one.
+__global__ void k_merge_flags(const uint32_t* nearest, uint32_t m, uint32_t* alive, uint32_t* leader) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    uint32_t j = nearest[i];
+    bool mutual = j != i && nearest[j] == i;
+    alive[i] = mutual && i > j ? 0u : 1u;
+    leader[i] = mutual && i < j ? 1u : 0u;
+}
+
+// Survivors move to their compacted position; each mutual pair becomes a new
+// node whose height (longest path to a leaf) is one more than its taller child.
+__global__ void k_merge(const uint32_t* clusters, const BvhBox* boxes, const uint32_t* heights,
+                        const uint32_t* nearest, uint32_t m, const uint32_t* alive, const uint32_t* alive_at,
+                        const uint32_t* leader, const uint32_t* leader_at, uint32_t node_base, BvhBinaryNode* nodes,
+                        uint32_t* clusters_out, BvhBox* boxes_out, uint32_t* heights_out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || !alive[i]) return;
+    uint32_t dst = alive_at[i];
+    if (leader[i]) {
+        uint32_t j = nearest[i];
+        BvhBox box = merged(boxes[i], boxes[j]);
+        uint32_t node = node_base + leader_at[i];
+        nodes[node] = BvhBinaryNode{box, clusters[i], clusters[j]};
+        clusters_out[dst] = node;
+        boxes_out[dst] = box;
+        heights_out[dst] = 1u + max(heights[i], heights[j]);
+    } else {
+        clusters_out[dst] = clusters[i];
+        boxes_out[dst] = boxes[i];
+        heights_out[dst] = heights[i];
+    }
+}
+
+// Device -> host.  Large copies go through two pinned staging buffers, so
+// the copy of one chunk overlaps the host copy of the previous one (fresh
+// pageable memory would otherwise take the transfer through page faults);
+// small ones are not worth pinning the buffers (~40 ms).
+cudaError_t download(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    constexpr size_t kChunk = size_t(32) << 20;
+    if (bytes == 0) return cudaSuccess;
+    if (bytes < 4 * kChunk) {
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+        return e ? e : cudaStreamSynchronize(st);
+    }
+    void* staging[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 2 && !e; ++k) {
+        e = cudaMallocHost(&staging[k], kChunk);
+        if (!e) e = cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming);
+    }
+    size_t chunks = (bytes + kChunk - 1) / kChunk;
+    for (size_t c = 0; c < chunks + 1 && !e; ++c) {
+        if (c < chunks) {  // start chunk c
+            size_t off = c * kChunk, len = std::min(kChunk, bytes - off);
+            e = cudaMemcpyAsync(staging[c & 1], static_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost, st);
+            if (!e) e = cudaEventRecord(done[c & 1], st);
+        }
+        if (c > 0 && !e) {  // finish chunk c - 1
+            size_t p = c - 1, off = p * kChunk, len = std::min(kChunk, bytes - off);
+            e = cudaEventSynchronize(done[p & 1]);
+            if (!e) std::memcpy(static_cast<char*>(dst) + off, staging[p & 1], len);
+        }
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (done[k]) cudaEventDestroy(done[k]);
+        if (staging[k]) cudaFreeHost(staging[k]);
+    }
+    return e;
+}
+
+uint32_t blocks_for(uint32_t n, uint32_t threads) { return (n + threads - 1) / threads; }
+
+}  // namespace
+
+bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t n, std::vector<BvhBinaryNode>& out, int max_depth,
+                          char* why, size_t why_size) {
+    auto failed = [&](const char* what, cudaError_t e) {
+        if (why && why_size) std::snprintf(why, why_size, "%s: %s", what, cudaGetErrorString(e));
+        return false;
+    };
+    out.clear();
+    if (n == 0) return true;
+    cudaStream_t st = nullptr;
+    if (cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) return failed("cudaStreamCreate", e);
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } guard{st};
+    Scratch scratch;
+    const uint32_t node_count = 2 * n - 1;
+    BvhBox* d_prims = scratch.alloc<BvhBox>(n);
+    BvhBinaryNode* d_nodes = scratch.alloc<BvhBinaryNode>(node_count);
+    unsigned long long* keys[2] = {scratch.alloc<unsigned long long>(n), scratch.alloc<unsigned long long>(n)};
+    uint32_t* values[2] = {scratch.alloc<uint32_t>(n), scratch.alloc<uint32_t>(n)};
+    uint32_t sort_blocks = blocks_for(n, kSortTile);
+    uint32_t* hist = scratch.alloc<uint32_t>(size_t(sort_blocks) * 256);
+    uint32_t* hist_at = scratch.alloc<uint32_t>(size_t(sort_blocks) * 256);
+    uint32_t* bounds = scratch.alloc<uint32_t>(6);
+    uint32_t* clusters[2] = {scratch.alloc<uint32_t>(n), scratch.alloc<uint32_t>(n)};
+    BvhBox* boxes[2] = {scratch.alloc<BvhBox>(n), scratch.alloc<BvhBox>(n)};
+    uint32_t* heights[2] = {scratch.alloc<uint32_t>(n), scratch.alloc<uint32_t>(n)};
+    uint32_t* nearest = scratch.alloc<uint32_t>(n);
+    uint32_t* alive = scratch.alloc<uint32_t>(n);
+    uint32_t* alive_at = scratch.alloc<uint32_t>(n);
+    uint32_t* leader = scratch.alloc<uint32_t>(n);
+    uint32_t* leader_at = scratch.alloc<uint32_t>(n);
+    if (scratch.error != cudaSuccess) return failed("device memory for the BVH build", scratch.error);
+    cudaError_t e = cudaMemcpyAsync(d_prims, prims, sizeof(BvhBox) * n, cudaMemcpyHostToDevice, st);
+    uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    if (!e) e = cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st);
+    if (e) return failed("BVH input upload", e);
+
+    k_centroid_bounds<<<std::min(blocks_for(n, 256), 4096u), 256, 0, st>>>(d_prims, n, bounds);
+    k_morton<<<blocks_for(n, 256), 256, 0, st>>>(d_prims, n, bounds, keys[0], values[0]);
+    if ((e = cudaGetLastError())) return failed("Morton keys", e);
+    int cur = 0;
+    for (int shift = 0; shift < 64; shift += 8) {
+        k_sort_histogram<<<sort_blocks, kSortThreads, 0, st>>>(keys[cur], n, shift, hist);
+        if ((e = exclusive_scan(hist, hist_at, sort_blocks * 256, st, scratch))) return failed("sort scan", e);
+        k_sort_scatter<<<sort_blocks, kSortThreads, 0, st>>>(keys[cur], values[cur], n, shift, hist_at,
+                                                             keys[cur ^ 1], values[cur ^ 1]);
+        if ((e = cudaGetLastError())) return failed("sort scatter", e);
+        cur ^= 1;
+    }
+    k_leaves<<<blocks_for(n, 256), 256, 0, st>>>(d_prims, values[cur], n, d_nodes, clusters[0], boxes[0],
+                                                 heights[0]);
+    if ((e = cudaGetLastError())) return failed("PLOC leaves", e);
+
+    uint32_t m = n, node_base = n;
+    int c = 0, rounds = 0;
+    while (m > 1) {
+        if (++rounds > kMaxRounds) {  // far beyond the ~log(n) rounds PLOC takes: leave it to the host builder
+            if (why && why_size) std::snprintf(why, why_size, "PLOC exceeded %d rounds", kMaxRounds);
+            return false;
+        }
+        k_nearest<<<blocks_for(m, kNearestThreads), kNearestThreads, 0, st>>>(boxes[c], m, nearest);
+        k_merge_flags<<<blocks_for(m, 256), 256, 0, st>>>(nearest, m, alive, leader);
+        if ((e = cudaGetLastError())) return failed("PLOC neighbours", e);
+        if ((e = exclusive_scan(alive, alive_at, m, st, scratch))) return failed("PLOC scan", e);
+        if ((e = exclusive_scan(leader, leader_at, m, st, scratch))) return failed("PLOC scan", e);
+        k_merge<<<blocks_for(m, 256), 256, 0, st>>>(clusters[c], boxes[c], heights[c], nearest, m, alive, alive_at,
+                                                    leader, leader_at, node_base, d_nodes, clusters[c ^ 1],
+                                                    boxes[c ^ 1], heights[c ^ 1]);
+        if ((e = cudaGetLastError())) return failed("PLOC merge", e);
+        uint32_t tail[4];
+        e = cudaMemcpyAsync(&tail[0], alive_at + m - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaMemcpyAsync(&tail[1], alive + m - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaMemcpyAsync(&tail[2], leader_at + m - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaMemcpyAsync(&tail[3], leader + m - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaStreamSynchronize(st);
+        if (e) return failed("PLOC round", e);
+        uint32_t survivors = tail[0] + tail[1], merges = tail[2] + tail[3];
+        if (merges == 0 || survivors + merges != m) {  // a round always merges the closest pair
+            if (why && why_size) std::snprintf(why, why_size, "PLOC made no progress at %u clusters", m);
+            return false;
+        }
+        node_base += merges;
+        m = survivors;
+        c ^= 1;
+    }
+    uint32_t depth = 0;
+    e = cudaMemcpyAsync(&depth, heights[c], 4, cudaMemcpyDeviceToHost, st);
+    if (!e) e = cudaStreamSynchronize(st);
+    if (e) return failed("BVH depth", e);
+    if (int(depth) > max_depth) {
+        if (why && why_size) std::snprintf(why, why_size, "PLOC tree depth %u exceeds %d", depth, max_depth);
+        return false;
+    }
+    // Leaves are known on the host (box i, primitive i); only the n-1
+    // internal nodes come back.
+    out.resize(node_count);
+    for (uint32_t i = 0; i < n; ++i) out[i] = BvhBinaryNode{prims[i], kInvalidChild, i};
+    e = download(out.data() + n, d_nodes + n, sizeof(BvhBinaryNode) * (node_count - n), st);
+    if (e) {
+        out.clear();
+        return failed("BVH download", e);
+    }
+    return true;
+}
+
+}  // namespace wf

@@ -1,0 +1,19 @@
+// GPU BVH2 builder (PLOC), wf_bvh_gpu.cu.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "bvh_build.h"
+
+namespace wf {
+
+// Builds the tree over `count` primitive boxes (host memory) on the current
+// device, in the host builder's output format (bvh_build.h).  Synchronous.
+// Returns false with a message in `why` on a CUDA error, a stalled build or a
+// leaf deeper than `max_depth` (checked on the device before the download).
+bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t count, std::vector<BvhBinaryNode>& nodes, int max_depth,
+                          char* why, size_t why_size);
+
+}  // namespace wf

@@ -10,6 +10,7 @@
 #include <memory>
 
 #include "wf_renderer.h"
+#include "wf_bvh_gpu.h"
 
 namespace wf {
 const char* last_error_text();
@@ -178,6 +179,8 @@ wf_status wf_scene_create(const wf_scene_desc* desc, wf_scene** out) {
     s->blas_count = uint32_t(h.blases.size());
     s->material_count = v.material_count;
     s->bounds = h.bounds;
+    s->gpu_bvh_builds = h.gpu_bvh_builds;
+    s->bvh_build_ms = h.bvh_build_ms;
     s->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = s.release();
     return WF_OK;
@@ -237,6 +240,32 @@ wf_status wf_scene_destroy(wf_scene* s) {
     return WF_OK;
 }
 
+wf_status wf_bvh_build(uint32_t builder, const float* boxes, uint32_t count, uint32_t* nodes,
+                       double* milliseconds) {
+    if ((count && !boxes) || (count && !nodes)) return fail(WF_ERR_INVALID_ARG, "null boxes or nodes");
+    if (builder != WF_BVH_HOST_SAH && builder != WF_BVH_GPU_PLOC)
+        return fail(WF_ERR_INVALID_ARG, "unknown BVH builder %u", builder);
+    std::vector<BvhBox> prims(count);
+    for (uint32_t i = 0; i < count; ++i)
+        for (int a = 0; a < 3; ++a) {
+            prims[i].lo[a] = boxes[6 * size_t(i) + a];
+            prims[i].hi[a] = boxes[6 * size_t(i) + 3 + a];
+        }
+    std::vector<BvhBinaryNode> out;
+    auto t0 = std::chrono::steady_clock::now();
+    if (builder == WF_BVH_GPU_PLOC) {
+        char why[256] = {0};
+        if (!build_binary_bvh_gpu(prims.data(), count, out, 1 << 30, why, sizeof(why)))
+            return fail(WF_ERR_CUDA, "GPU BVH build failed: %s", why);
+    } else {
+        build_binary_bvh(prims.data(), count, out, 0);
+    }
+    if (milliseconds) *milliseconds = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    static_assert(sizeof(BvhBinaryNode) == 8 * sizeof(uint32_t), "node record is 8 words");
+    if (!out.empty()) std::memcpy(nodes, out.data(), sizeof(BvhBinaryNode) * out.size());
+    return WF_OK;
+}
+
 wf_status wf_scene_get_info(const wf_scene* s, wf_scene_info* info) {
     if (!s || !info) return fail(WF_ERR_INVALID_ARG, "null argument");
     info->light_count = s->light_count;
@@ -245,6 +274,8 @@ wf_status wf_scene_get_info(const wf_scene* s, wf_scene_info* info) {
     info->material_count = s->material_count;
     info->device_bytes = s->device_bytes;
     info->build_seconds = s->build_seconds;
+    info->gpu_bvh_builds = s->gpu_bvh_builds;
+    info->bvh_build_ms = float(s->bvh_build_ms);
     return WF_OK;
 }
 

@@ -40,6 +40,8 @@ struct HostScene {
     bool black_background = false;
     bool ignore_occlusion = false;
     Box bounds{};  // world bounds of all geometry (photon-grid default)
+    uint32_t gpu_bvh_builds = 0;
+    double bvh_build_ms = 0.0;
 };
 
 // Builds the device-layout scene: light registration, light alias table,
@@ -78,6 +80,8 @@ struct wf_scene {
     uint32_t blas_count = 0;
     uint32_t material_count = 0;
     double build_seconds = 0.0;
+    uint32_t gpu_bvh_builds = 0;
+    double bvh_build_ms = 0.0;
     wf::Box bounds{};
     int device = 0;
 };

@@ -5,6 +5,7 @@
 // wf_device.cuh.  Floating-point expressions keep the reference's order so the
 // light and environment tables are bit-identical to the reference's.
 #include "wf_internal.h"
+#include "wf_bvh_gpu.h"
 
 #include <algorithm>
 #include <chrono>
@@ -15,6 +16,10 @@
 #include <limits>
 
 namespace wf {
+
+// Smallest BVH2 input the GPU builder takes; smaller trees build on the host
+// in well under a millisecond.
+constexpr uint32_t kGpuBvhMinPrimitives = 4096;
 
 namespace {
 thread_local std::string g_error;
@@ -318,6 +323,20 @@ wf_status build_host_scene(const wf_scene_desc* d, HostScene& s) {
     for (uint32_t i = 0; i < d->instance_count; ++i)
         if (d->instances[i].accel == WF_ACCEL_BVH) needs_bvh[d->instances[i].mesh] = true;
     int threads = int(d->build_threads);
+    // BVH2 builds: the host binned-SAH builder, or the GPU PLOC builder for
+    // large inputs (falls back to the host builder on any failure or a tree
+    // deeper than kMaxBvhDepth).
+    auto build_bvh = [&](const BvhBox* prims, uint32_t n, std::vector<BvhBinaryNode>& out) {
+        auto t0 = std::chrono::steady_clock::now();
+        bool done = false;
+        if (d->bvh_builder == WF_BVH_GPU_PLOC && n >= kGpuBvhMinPrimitives) {
+            char why[256] = {0};
+            done = build_binary_bvh_gpu(prims, n, out, kMaxBvhDepth, why, sizeof(why));
+            if (done) ++s.gpu_bvh_builds;
+        }
+        if (!done) build_binary_bvh(prims, n, out, threads);
+        s.bvh_build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
     std::vector<BvhBox> boxes;
     std::vector<BvhBinaryNode> bin;
     std::vector<uint32_t> order;
@@ -332,7 +351,7 @@ wf_status build_host_scene(const wf_scene_desc* d, HostScene& s) {
         if (needs_bvh[m] && mesh.triangle_count > 0) {
             boxes.resize(mesh.triangle_count);
             for (uint32_t i = 0; i < mesh.triangle_count; ++i) boxes[i] = triangle_box(mesh.triangles[i]);
-            build_binary_bvh(boxes.data(), mesh.triangle_count, bin, threads);
+            build_bvh(boxes.data(), mesh.triangle_count, bin);
             leaf_order(bin, order);
             std::vector<uint32_t> position(mesh.triangle_count);
             for (uint32_t k = 0; k < order.size(); ++k) {
@@ -413,7 +432,7 @@ wf_status build_host_scene(const wf_scene_desc* d, HostScene& s) {
         s.tlas_leaves.push_back(i);
     }
     if (!leaf_boxes.empty()) {
-        build_binary_bvh(leaf_boxes.data(), uint32_t(leaf_boxes.size()), bin, threads);
+        build_bvh(leaf_boxes.data(), uint32_t(leaf_boxes.size()), bin);
         Converter c{bin, s.nodes, [](uint32_t leaf) { return leaf; }};
         s.tlas = c.root();
     }
@@ -433,7 +452,7 @@ wf_status build_host_scene(const wf_scene_desc* d, HostScene& s) {
     if (d->triangle_count > 0 && d->mesh_count == 0) {
         boxes.resize(d->triangle_count);
         for (uint32_t i = 0; i < d->triangle_count; ++i) boxes[i] = triangle_box(d->triangles[i]);
-        build_binary_bvh(boxes.data(), d->triangle_count, bin, threads);
+        build_bvh(boxes.data(), d->triangle_count, bin);
         leaf_order(bin, order);
         std::vector<uint32_t> position(d->triangle_count);
         for (uint32_t k = 0; k < order.size(); ++k) {

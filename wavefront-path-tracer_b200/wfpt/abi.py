@@ -60,6 +60,10 @@ assert MATERIAL_DTYPE.itemsize == 124 and PUNCTUAL_DTYPE.itemsize == 52
 assert RAY_DTYPE.itemsize == 24 and HIT_DTYPE.itemsize == 68
 
 
+BVH_HOST_SAH = 0
+BVH_GPU_PLOC = 1
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("spheres", C.c_void_p), ("sphere_count", C.c_uint32),
@@ -73,6 +77,7 @@ class SceneDesc(C.Structure):
         ("ignore_direct_light_occlusion", C.c_uint32),
         ("register_triangle_lights", C.c_uint32),
         ("build_threads", C.c_uint32),
+        ("bvh_builder", C.c_uint32), ("reserved", C.c_uint32),
     ]
 
 
@@ -83,7 +88,8 @@ class Environment(C.Structure):
 
 class SceneInfo(C.Structure):
     _fields_ = [("light_count", C.c_uint32), ("tlas_leaf_count", C.c_uint32), ("blas_count", C.c_uint32),
-                ("material_count", C.c_uint32), ("device_bytes", C.c_uint64), ("build_seconds", C.c_double)]
+                ("material_count", C.c_uint32), ("device_bytes", C.c_uint64), ("build_seconds", C.c_double),
+                ("gpu_bvh_builds", C.c_uint32), ("bvh_build_ms", C.c_float)]
 
 
 class Camera(C.Structure):
@@ -159,6 +165,7 @@ def declare(lib):
         "wf_scene_set_environment": (S, [P, C.POINTER(Environment)]),
         "wf_scene_destroy": (S, [P]),
         "wf_scene_get_info": (S, [P, C.POINTER(SceneInfo)]),
+        "wf_bvh_build": (S, [U32, P, U32, P, P]),
         "wf_trace_closest": (S, [P, P, U32, P, P]),
         "wf_trace_any": (S, [P, P, P, U32, P, P]),
         "wf_render_config_default": (None, [C.POINTER(RenderConfig), U32, U32]),

@@ -83,6 +83,7 @@ class Scene:
         self.ignore_direct_light_occlusion = False
         self.register_triangle_lights = True
         self.build_threads = 0
+        self.bvh_builder = abi.BVH_HOST_SAH  # or abi.BVH_GPU_PLOC
 
     def add_material(self, record):
         self.materials = np.concatenate([self.materials, np.array([record], abi.MATERIAL_DTYPE)])
@@ -127,6 +128,7 @@ class Scene:
         d.ignore_direct_light_occlusion = int(self.ignore_direct_light_occlusion)
         d.register_triangle_lights = int(self.register_triangle_lights)
         d.build_threads = self.build_threads
+        d.bvh_builder = self.bvh_builder
         return d, keep
 
     def environment_struct(self):
@@ -202,6 +204,20 @@ class DeviceScene:
         check(library().wf_trace_any(self.handle, d_rays.data_ptr(), d_max.data_ptr(), n, d_out.data_ptr(), stream))
         torch.cuda.synchronize()
         return d_out.cpu().numpy()
+
+
+BVH_NODE_DTYPE = np.dtype([("lo", np.float32, 3), ("hi", np.float32, 3), ("left", np.uint32), ("right", np.uint32)])
+
+
+def build_bvh(boxes, builder=abi.BVH_HOST_SAH):
+    """wf_bvh_build: one binary BVH2 over boxes (n, 6) = lo xyz, hi xyz.
+    Returns (nodes as BVH_NODE_DTYPE, milliseconds); the root is nodes[-1]."""
+    boxes = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+    n = len(boxes)
+    nodes = np.zeros(max(2 * n - 1, 0), BVH_NODE_DTYPE)
+    ms = C.c_double(0.0)
+    check(library().wf_bvh_build(builder, boxes.ctypes.data, n, nodes.ctypes.data, C.byref(ms)))
+    return nodes, ms.value
 
 
 def camera_struct(cam):

@@ -81,8 +81,10 @@ typedef struct wf_material {
  * roughness 0 and ior 1 as makeMaterial sets them (src/scene/scene_host.cpp:44-52). */
 void wf_material_default(wf_material* material, uint32_t type);
 
-/* Triangle, include/scene/geometry.cuh:13-45 (positions, optional vertex
- * normals and material; texture coordinates and tangents are not carried). */
+/* Triangle, include/scene/geometry.cuh:13-45: positions, optional vertex
+ * normals and material.  Texture coordinates and tangent frames, which only
+ * textured materials read, come in an optional parallel array
+ * (wf_triangle_attributes). */
 typedef struct wf_triangle {
     float v0[3], v1[3], v2[3];
     float n0[3], n1[3], n2[3];
@@ -99,10 +101,56 @@ typedef struct wf_sphere {
 } wf_sphere;
 
 /* MeshAsset, include/scene/scene.cuh:117-119 */
+/* The texture coordinates and tangent frames of a Triangle,
+ * include/scene/geometry.cuh:22-41 (uv0-uv2, uv1_0-uv1_2, tangent,
+ * bitangent, tangent1, bitangent1, vertexTangent0-2, vertexTangentSign0-2,
+ * hasVertexTangents, hasTexcoords, hasTexcoords1; geometry.cuh:22-48).
+ * Without has_texcoords (has_texcoords1) a set reads as (0, 0). */
+typedef struct wf_triangle_attributes {
+    float uv[3][2];
+    float uv1[3][2];
+    float tangent[3], bitangent[3], tangent1[3], bitangent1[3];
+    float vertex_tangent[3][3];
+    float vertex_tangent_sign[3];
+    uint32_t has_vertex_tangents;
+    uint32_t has_texcoords;
+    uint32_t has_texcoords1;
+} wf_triangle_attributes;
+
 typedef struct wf_mesh {
     const wf_triangle* triangles;
     uint32_t triangle_count;
+    const wf_triangle_attributes* attributes; /* NULL, or triangle_count records */
 } wf_mesh;
+
+#define WF_NO_TEXTURE 0xffffffffu
+
+/* ObjTexture, include/scene/obj_loader.hpp:9-13: RGBA8 texels, row-major
+ * from the first stored row; sampled with wrapping and bilinear filtering
+ * at (u, 1 - v) (src/scene/scene.cu:44-80, device_traversal.cuh:341-347). */
+typedef struct wf_texture {
+    uint32_t width, height;
+    const uint8_t* rgba;
+} wf_texture;
+
+/* TextureBinding, include/scene/material.cuh:14-21 (KHR_texture_transform). */
+typedef struct wf_texture_binding {
+    uint32_t texture;  /* WF_NO_TEXTURE, or an index into wf_scene_desc::textures */
+    uint32_t texcoord; /* 0 or 1 */
+    float offset[2];
+    float scale[2];
+    float rotation;
+    uint32_t has_transform;
+} wf_texture_binding;
+
+/* The texture bindings of a Material, include/scene/material.cuh:42-69, and
+ * its normal-map scales. */
+typedef struct wf_material_textures {
+    float normal_scale;           /* Material::normalScale (1) */
+    float clearcoat_normal_scale; /* Material::clearcoatNormalScale (1) */
+    wf_texture_binding albedo, metallic_roughness, emissive, normal, thickness, specular_glossiness,
+        specular_weight, specular_color, clearcoat, clearcoat_roughness, clearcoat_normal;
+} wf_material_textures;
 
 /* SceneInstance + InstanceTransform, include/scene/scene.cuh:27-35,121-126.
  * local_to_world[i] / world_to_local[i] are the reference's X, Y, Z basis
@@ -168,6 +216,20 @@ typedef struct wf_scene_desc {
      * in the reference. */
     uint32_t bvh_builder;
     uint32_t reserved;
+    /* Textured materials (all optional): RGBA8 textures, one
+     * wf_material_textures per material, and the attributes of `triangles`
+     * and `static_triangles` (those of mesh triangles are in wf_mesh).
+     * Scene::useNormalMaps and normalMapMinimumCosine
+     * (include/scene/scene.cuh:159-160): normal maps apply unless
+     * disable_normal_maps is set. */
+    const wf_texture* textures;
+    uint32_t texture_count;
+    uint32_t disable_normal_maps;
+    const wf_material_textures* material_textures;
+    const wf_triangle_attributes* triangle_attributes;
+    const wf_triangle_attributes* static_triangle_attributes;
+    float normal_map_minimum_cosine;
+    uint32_t reserved2;
 } wf_scene_desc;
 
 enum { WF_BVH_HOST_SAH = 0, WF_BVH_GPU_PLOC = 1 };

@@ -114,6 +114,7 @@ void* wfcuda_scene_create(const wf_scene_desc* d, const wf_environment* env) {
         auto r = std::make_unique<CudaRefScene>();
         r->device = uploadScene(h);
         r->device.scene.ignoreDirectLightOcclusion = d->ignore_direct_light_occlusion != 0;
+        wfref::apply_normal_map_settings(r->device.scene, d);
         if (env && env->width && env->height) {
             HostEnvironment map;
             map.width = env->width;

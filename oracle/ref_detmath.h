@@ -18,6 +18,13 @@
 #include <sstream>
 #include <string>
 #include "../wavefront-path-tracer_b200/csrc/wf_math.h"
+// sincosf (texture transforms, device_traversal.cuh:335): sine and cosine
+// from the same functions as sinf/cosf below.
+inline void wfref_det_sincosf(float x, float* s, float* c) {
+    *s = wfm::sinf(x);
+    *c = wfm::cosf(x);
+}
+#define sincosf wfref_det_sincosf
 #define sinf wfm::sinf
 #define cosf wfm::cosf
 #define tanf wfm::tanf

@@ -214,6 +214,7 @@ void* wfref_scene_create(const wf_scene_desc* d, const wf_environment* env, int 
         r->original_material_count = d->material_count;
         r->device = uploadScene(h);
         r->device.scene.ignoreDirectLightOcclusion = d->ignore_direct_light_occlusion != 0;
+        wfref::apply_normal_map_settings(r->device.scene, d);
         if (probe) {
             for (uint32_t i = 0; i < r->device.scene.instanceCount; ++i)
                 r->device.instances[i].lightOffset = i << 24;

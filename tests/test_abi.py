@@ -38,7 +38,7 @@ def test_struct_layouts_match_header():
     assert abi.TRIANGLE_DTYPE.itemsize == 80
     assert abi.MATERIAL_DTYPE.itemsize == 124
     assert abi.HIT_DTYPE.itemsize == 68
-    assert ctypes.sizeof(abi.SceneDesc) == 136
+    assert ctypes.sizeof(abi.SceneDesc) == 184
     assert ctypes.sizeof(abi.RenderConfig) == 120
     assert ctypes.sizeof(abi.Camera) == 56
 

@@ -90,3 +90,26 @@ def test_batch_rejects_caustics_and_autotunes(cuda):
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     finally:
         dev.close()
+
+
+def test_batch_with_textured_job_matches_per_job_renders(cuda):
+    """A job whose scene has textured and alpha-textured materials switches
+    the batch to the alpha-capable trace and shadow kernels; every job still
+    matches its own render bit for bit."""
+    tex_scene, tex_cam = scenes.textured_room(48, 40)
+    box_scene, box_cam = scenes.cornell_box(32, 32)
+    jobs = [dict(scene=wfpt.DeviceScene(tex_scene), camera=tex_cam, sample_start=4, sample_count=3,
+                 config=wfpt.render_config(48, 40, max_depth=6, rr_start_depth=3)),
+            dict(scene=wfpt.DeviceScene(box_scene), camera=box_cam, sample_start=0, sample_count=2,
+                 config=wfpt.render_config(32, 32, max_depth=8, rr_start_depth=3))]
+    try:
+        want = [_per_job(j)[0] for j in jobs]
+        batch = wfpt.Batch(jobs)
+        batch.run()
+        batch.synchronize()
+        for k, image in enumerate(want):
+            assert np.array_equal(batch.download(k).view(np.uint32), image.view(np.uint32)), f"job {k}"
+        batch.close()
+    finally:
+        for j in jobs:
+            j["scene"].close()

@@ -48,6 +48,8 @@ struct BatchView {
 struct wf_batch {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    bool opaque = true;     // no job's scene has alpha-textured materials: the Opaque<> trace and shadow kernels
+    bool textured = false;  // some job's scene has textured materials: k_batch_shade<true>
     int device = 0, sm_count = 148;
     std::vector<void*> allocations;
     std::vector<wf_batch_job> jobs;
@@ -163,6 +165,7 @@ __global__ void __maxnreg__(72) k_batch_trace(BatchView b, PathSoA ps, const uin
     }
 }
 
+template <bool kTextures>
 __global__ void __launch_bounds__(128, 4) k_batch_shade(BatchView b, PathSoA ps, const uint32_t* queue,
                                                         const uint32_t* count, const float4* hit_a,
                                                         const uint32_t* hit_inst, float4* terms, int4* shade_out,
@@ -199,7 +202,7 @@ __global__ void __launch_bounds__(128, 4) k_batch_shade(BatchView b, PathSoA ps,
         sink.nterms = 0;
         sink.kill = kUnconditional;
         sink.overflow = &c->overflow;
-        bool alive = shade_path(J.scene, J.rp, path, did_hit, sh, sink);
+        bool alive = shade_path<DeferredSink, kTextures>(J.scene, J.rp, path, did_hit, sh, sink);
         if (sink.nterms > kMaxTerms) atomicOr(&c->overflow, 2u);
         store_path(ps, p, path);
         shade_out[i] = make_int4(min(sink.nterms, kMaxTerms), sink.kill, alive ? 1 : 0, 0);
@@ -372,13 +375,28 @@ wf_status capture_batch(wf_batch* b) {
         uint32_t nxt = cur ^ 1;
         uint32_t* cur_count = &b->counters->queue_count[cur];
         uint32_t* next_count = &b->counters->queue_count[nxt];
-        k_batch_trace<NoTally><<<batch_grid(b, 0, cap, b->block), b->block, 0, st>>>(
-            b->view, b->paths, b->queue[cur], cur_count, b->hit_a, b->hit_inst, b->counters, b->refill);
-        k_batch_shade<<<batch_grid(b, 1, cap, 128), 128, 0, st>>>(
-            b->view, b->paths, b->queue[cur], cur_count, b->hit_a, b->hit_inst, b->terms, b->shade_out,
-            b->shadow_origin, b->shadow_dir, b->shadow_capacity, b->counters, next_count);
-        k_batch_shadow<NoTally><<<batch_grid(b, 2, b->shadow_capacity, b->block), b->block, 0, st>>>(
-            b->view, b->shadow_origin, b->shadow_dir, b->shadow_result, b->counters, b->shadow_capacity, b->refill);
+        if (b->opaque)
+            k_batch_trace<Opaque<NoTally>><<<batch_grid(b, 0, cap, b->block), b->block, 0, st>>>(
+                b->view, b->paths, b->queue[cur], cur_count, b->hit_a, b->hit_inst, b->counters, b->refill);
+        else
+            k_batch_trace<NoTally><<<batch_grid(b, 0, cap, b->block), b->block, 0, st>>>(
+                b->view, b->paths, b->queue[cur], cur_count, b->hit_a, b->hit_inst, b->counters, b->refill);
+        if (b->textured)
+            k_batch_shade<true><<<batch_grid(b, 1, cap, 128), 128, 0, st>>>(
+                b->view, b->paths, b->queue[cur], cur_count, b->hit_a, b->hit_inst, b->terms, b->shade_out,
+                b->shadow_origin, b->shadow_dir, b->shadow_capacity, b->counters, next_count);
+        else
+            k_batch_shade<false><<<batch_grid(b, 1, cap, 128), 128, 0, st>>>(
+                b->view, b->paths, b->queue[cur], cur_count, b->hit_a, b->hit_inst, b->terms, b->shade_out,
+                b->shadow_origin, b->shadow_dir, b->shadow_capacity, b->counters, next_count);
+        if (b->opaque)
+            k_batch_shadow<Opaque<NoTally>><<<batch_grid(b, 2, b->shadow_capacity, b->block), b->block, 0, st>>>(
+                b->view, b->shadow_origin, b->shadow_dir, b->shadow_result, b->counters, b->shadow_capacity,
+                b->refill);
+        else
+            k_batch_shadow<NoTally><<<batch_grid(b, 2, b->shadow_capacity, b->block), b->block, 0, st>>>(
+                b->view, b->shadow_origin, b->shadow_dir, b->shadow_result, b->counters, b->shadow_capacity,
+                b->refill);
         k_batch_finalize<<<batch_grid(b, 3, cap, 256), 256, 0, st>>>(
             b->view, b->paths, b->queue[cur], cur_count, b->terms, b->shade_out, b->shadow_result, b->queue[nxt],
             next_count, cap, b->counters);
@@ -449,6 +467,10 @@ wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_
     b->jobs.assign(jobs, jobs + count);
     b->block = config.block_size ? config.block_size : 128u;
     b->refill = config.refill_threshold ? config.refill_threshold : 8u;
+    for (uint32_t i = 0; i < count; ++i) {
+        b->opaque = b->opaque && !jobs[i].scene->alpha_textures;
+        b->textured = b->textured || jobs[i].scene->textured;
+    }
 
     // Unit order: job by job, in the given order or longest per-pixel work first.
     std::vector<uint32_t> order(count);
@@ -532,9 +554,12 @@ wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_
     b->view.jobs = b->jobs_dev;
     b->view.unit_job = b->unit_job;
     b->view.units = b->units;
-    WF_BATCH_CUDA(batch_resident(bp, 0, k_batch_trace<NoTally>, b->block));
-    WF_BATCH_CUDA(batch_resident(bp, 1, k_batch_shade, 128));
-    WF_BATCH_CUDA(batch_resident(bp, 2, k_batch_shadow<NoTally>, b->block));
+    WF_BATCH_CUDA(b->opaque ? batch_resident(bp, 0, k_batch_trace<Opaque<NoTally>>, b->block)
+                            : batch_resident(bp, 0, k_batch_trace<NoTally>, b->block));
+    WF_BATCH_CUDA(b->textured ? batch_resident(bp, 1, k_batch_shade<true>, 128)
+                              : batch_resident(bp, 1, k_batch_shade<false>, 128));
+    WF_BATCH_CUDA(b->opaque ? batch_resident(bp, 2, k_batch_shadow<Opaque<NoTally>>, b->block)
+                            : batch_resident(bp, 2, k_batch_shadow<NoTally>, b->block));
     WF_BATCH_CUDA(batch_resident(bp, 3, k_batch_finalize, 256));
     if (wf_status e = capture_batch(bp)) return e;
     WF_BATCH_CUDA(cudaStreamSynchronize(b->stream));

@@ -150,6 +150,10 @@ wf_status wf_scene_create(const wf_scene_desc* desc, wf_scene** out) {
     up(&v.direct_spheres, h.direct_spheres);
     up(&v.direct_instances, h.direct_instances);
     up(&v.materials, h.materials);
+    up(&v.material_textures, h.material_textures);
+    up(&v.texels, h.texels);
+    up(&v.textures, h.textures);
+    up(&v.tri_attr, h.tri_attr);
     up(&v.lights, h.lights);
     up(&v.punctual, h.punctual);
     if (e != cudaSuccess) {
@@ -172,6 +176,9 @@ wf_status wf_scene_create(const wf_scene_desc* desc, wf_scene** out) {
     v.punctual_count = uint32_t(h.punctual.size());
     v.directional_count = h.directional_count;
     v.any_alpha_reject = h.any_alpha_reject ? 1u : 0u;
+    v.texture_count = uint32_t(h.textures.size());
+    v.use_normal_maps = h.use_normal_maps ? 1u : 0u;
+    v.normal_map_min_cosine = h.normal_map_min_cosine;
     v.black_background = h.black_background ? 1u : 0u;
     v.ignore_direct_light_occlusion = h.ignore_occlusion ? 1u : 0u;
     s->light_count = v.light_count;
@@ -180,6 +187,8 @@ wf_status wf_scene_create(const wf_scene_desc* desc, wf_scene** out) {
     s->material_count = v.material_count;
     s->bounds = h.bounds;
     s->gpu_bvh_builds = h.gpu_bvh_builds;
+    s->alpha_textures = h.alpha_textures;
+    s->textured = h.textured;
     s->bvh_build_ms = h.bvh_build_ms;
     s->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = s.release();

@@ -136,6 +136,8 @@ struct Instance {
 constexpr uint32_t kMatGltfPbr = 1u;
 constexpr uint32_t kMatSpecGlossWorkflow = 2u;
 constexpr uint32_t kMatAlphaReject = 4u;  // alphaMasked && opacity < alphaCutoff (untextured)
+constexpr uint32_t kMatTextured = 8u;      // some texture binding is set: resolve factors at the hit
+constexpr uint32_t kMatAlphaTexture = 16u; // alphaMasked with an albedo texture: opacity per hit
 
 // Untextured Material (include/scene/material.cuh:30-70): every texture
 // lookup returns its factor, so only the factors are kept.
@@ -158,6 +160,52 @@ struct Material {
 };
 
 enum MaterialType : uint32_t { kDiffuse = 0, kMetal = 1, kDielectric = 2, kEmissive = 3, kSpecGloss = 4 };
+
+// TextureBinding, include/scene/material.cuh:14-21.
+struct TexBinding {
+    uint32_t texture;  // kInvalid: none
+    uint32_t texcoord;
+    float offset_x, offset_y, scale_x, scale_y, rotation;
+    uint32_t has_transform;
+};
+
+enum TexSlot : uint32_t {
+    kTexAlbedo = 0,
+    kTexMetallicRoughness,
+    kTexEmissive,
+    kTexNormal,
+    kTexThickness,
+    kTexSpecGloss,
+    kTexSpecularWeight,
+    kTexSpecularColor,
+    kTexClearcoat,
+    kTexClearcoatRoughness,
+    kTexClearcoatNormal,
+    kTexSlots
+};
+
+// The texture side of a Material (include/scene/material.cuh:42-69), read
+// only for materials flagged kMatTextured / kMatAlphaTexture.
+struct MaterialTextures {
+    float normal_scale, clearcoat_normal_scale;
+    float opacity, alpha_cutoff;
+    TexBinding slot[kTexSlots];
+};
+
+// Texture coordinates and tangent frames of one triangle
+// (include/scene/geometry.cuh:22-41), in triangle packing order.
+struct TriAttr {
+    float uv[3][2];
+    float uv1[3][2];
+    float tangent[3], bitangent[3], tangent1[3], bitangent1[3];
+    float vertex_tangent[3][3];
+    float vertex_tangent_sign[3];
+    uint32_t has_vertex_tangents;
+    uint32_t has_texcoords;
+    uint32_t has_texcoords1;
+    uint32_t pad;
+};
+static_assert(sizeof(TriAttr) == 160, "TriAttr is 40 words");
 
 // TriangleLight, include/scene/geometry.cuh:49-57.
 struct Light {
@@ -232,6 +280,14 @@ struct DeviceScene {
     uint32_t any_alpha_reject;
     uint32_t black_background;
     uint32_t ignore_direct_light_occlusion;
+    // textured materials (the shading stage and alpha-textured hits only)
+    const MaterialTextures* material_textures;  // one per material, or null
+    const uchar4* texels;                       // all textures, RGBA8
+    const uint4* textures;                      // width, height, first texel
+    const TriAttr* tri_attr;                    // per packed triangle, or null
+    uint32_t texture_count;
+    uint32_t use_normal_maps;
+    float normal_map_min_cosine;
 };
 
 // ----------------------------------------------------------- parameters

@@ -29,6 +29,12 @@ struct HostScene {
     std::vector<uint32_t> direct_spheres;
     std::vector<uint32_t> direct_instances;
     std::vector<Material> materials;
+    std::vector<MaterialTextures> material_textures;  // empty without texture bindings
+    std::vector<uchar4> texels;
+    std::vector<uint4> textures;
+    std::vector<TriAttr> tri_attr;                    // empty without triangle attributes
+    bool use_normal_maps = true;
+    float normal_map_min_cosine = 0.0f;
     std::vector<Light> lights;
     std::vector<Punctual> punctual;
     uint32_t directional_count = 0;
@@ -42,6 +48,8 @@ struct HostScene {
     Box bounds{};  // world bounds of all geometry (photon-grid default)
     uint32_t gpu_bvh_builds = 0;
     double bvh_build_ms = 0.0;
+    bool alpha_textures = false;
+    bool textured = false;
 };
 
 // Builds the device-layout scene: light registration, light alias table,
@@ -82,6 +90,8 @@ struct wf_scene {
     double build_seconds = 0.0;
     uint32_t gpu_bvh_builds = 0;
     double bvh_build_ms = 0.0;
+    bool alpha_textures = false;  // some material is alpha-masked with an albedo texture
+    bool textured = false;        // some material has a texture binding
     wf::Box bounds{};
     int device = 0;
 };

@@ -65,7 +65,7 @@ WF_DEV void closest_begin_direct(ClosestLane& L, const DeviceScene& s, Tally& ta
         TriVerts tri = load_triangle(s, ti);
         float t, u, v;
         if (!intersect_triangle(L.wo, L.wd, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
-        if (alpha_rejects(s, tri.material)) continue;
+        if (alpha_rejects<Tally>(s, tri.material, ti, u, v)) continue;
         h.t = t;
         h.u = u;
         h.v = v;
@@ -91,7 +91,7 @@ WF_DEV void closest_begin(ClosestLane& L, const DeviceScene& s, V3 o, V3 d, Tall
         TriVerts tri = load_triangle(s, ti);
         float t, u, v;
         if (!intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
-        if (alpha_rejects(s, tri.material)) continue;
+        if (alpha_rejects<Tally>(s, tri.material, ti, u, v)) continue;
         h.t = t;
         h.u = u;
         h.v = v;
@@ -211,7 +211,7 @@ WF_DEV void closest_step(ClosestLane& L, const DeviceScene& s, Tally& tally) {
         if (intersect_triangle(L.o, L.d, tri.v0, tri.v1, tri.v2, t, u, v) && t < L.h.t) {
             uint32_t override_m = blas ? L.material_override : kInvalid;
             uint32_t m = override_m == kInvalid ? tri.material : override_m;
-            if (!alpha_rejects(s, m)) {
+            if (!alpha_rejects<Tally>(s, m, ti, u, v)) {
                 L.h.t = t;
                 L.h.u = u;
                 L.h.v = v;
@@ -255,7 +255,7 @@ WF_DEV void any_begin_direct(AnyLane& L, const DeviceScene& s, Tally& tally) {
         TriVerts tri = load_triangle(s, s.direct_first + i);
         float t, u, v;
         if (intersect_triangle(L.wo, L.wd, tri.v0, tri.v1, tri.v2, t, u, v) && t < L.t_max &&
-            !alpha_rejects(s, tri.material)) {
+            !alpha_rejects<Tally>(s, tri.material, s.direct_first + i, u, v)) {
             L.hit = true;
             return;
         }
@@ -288,7 +288,7 @@ WF_DEV void any_begin(AnyLane& L, const DeviceScene& s, V3 o, V3 d, float t_max,
         TriVerts tri = load_triangle(s, s.static_first + i);
         float t, u, v;
         if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < t_max &&
-            !alpha_rejects(s, tri.material)) {
+            !alpha_rejects<Tally>(s, tri.material, s.static_first + i, u, v)) {
             L.hit = true;
             return;
         }
@@ -389,7 +389,7 @@ WF_DEV void any_step(AnyLane& L, const DeviceScene& s, Tally& tally) {
                     float t, u, v;
                     if (!intersect_triangle(lo, ld, tri.v0, tri.v1, tri.v2, t, u, v) || t >= L.t_max) continue;
                     uint32_t m = in.material_override == kInvalid ? tri.material : in.material_override;
-                    if (!alpha_rejects(s, m)) {
+                    if (!alpha_rejects<Tally>(s, m, s.mesh_linear[b.first_linear + i], u, v)) {
                         L.hit = true;
                         L.stage = kStageDone;
                         return;
@@ -405,7 +405,7 @@ WF_DEV void any_step(AnyLane& L, const DeviceScene& s, Tally& tally) {
         if (intersect_triangle(L.o, L.d, tri.v0, tri.v1, tri.v2, t, u, v) && t < L.t_max) {
             uint32_t override_m = L.stage == kStageBlas ? L.material_override : kInvalid;
             uint32_t m = override_m == kInvalid ? tri.material : override_m;
-            if (!alpha_rejects(s, m)) {
+            if (!alpha_rejects<Tally>(s, m, ti, u, v)) {
                 L.hit = true;
                 L.stage = kStageDone;
                 return;

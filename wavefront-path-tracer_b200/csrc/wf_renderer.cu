@@ -118,7 +118,7 @@ __global__ void __maxnreg__(72) k_trace(DeviceScene s, PathSoA ps, const uint32_
             hit_a[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
             hit_inst[i] = h.inst;
         }
-        if constexpr (std::is_same<Tally, CountTally>::value) flush_tally(tally, totals);
+        if constexpr (Tally::kCounts) flush_tally(tally, totals);
         return;
     }
     ClosestLane L;
@@ -151,7 +151,7 @@ __global__ void __maxnreg__(72) k_trace(DeviceScene s, PathSoA ps, const uint32_
             }
         }
     }
-    if constexpr (std::is_same<Tally, CountTally>::value) flush_tally(tally, totals);
+    if constexpr (Tally::kCounts) flush_tally(tally, totals);
 }
 
 // Shading categories: warps of k_shade take entries of one category at a
@@ -228,6 +228,7 @@ __global__ void k_scatter(const uint32_t* count, const uint8_t* key, uint32_t* o
 }
 
 // 128 registers: 4 CTAs per SM; the few spills cost less than the lost warps.
+template <bool kTextures>
 __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ RenderParams rp, PathSoA ps, const uint32_t* queue, const uint32_t* count,
                         const float4* hit_a, const uint32_t* hit_inst, float4* terms, int4* shade_out,
                         float4* shadow_origin, float4* shadow_dir, uint32_t shadow_capacity, Counters* c,
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ Device
         sink.kill = kUnconditional;
         sink.overflow = &c->overflow;
         sink.gathers = gathers;
-        bool alive = shade_path(s, rp, path, did_hit, sh, sink);
+        bool alive = shade_path<DeferredSink, kTextures>(s, rp, path, did_hit, sh, sink);
         if (sink.nterms > kMaxTerms) atomicOr(&c->overflow, 2u);
         store_path(ps, p, path);
         shade_out[i] = make_int4(min(sink.nterms, kMaxTerms), sink.kill, alive ? 1 : 0, 0);
@@ -351,7 +352,7 @@ __global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float
             if (L.stage == kStageDone) result[j] = L.hit ? 1 : 0;
         }
     }
-    if constexpr (std::is_same<Tally, CountTally>::value) flush_tally(tally, totals);
+    if constexpr (Tally::kCounts) flush_tally(tally, totals);
 }
 
 // Adds each path's accepted terms in emission order, applies the kill rule,
@@ -907,6 +908,32 @@ wf_status build_photon_map(wf_renderer* r) {
     return WF_OK;
 }
 
+// k_trace / k_shadow for this renderer's scene: the Opaque<> variants (the
+// per-hit alpha-texture test compiled out, fewer registers) unless some
+// material of the scene is alpha-textured.
+template <typename Tally, bool kLanes, typename... A>
+void launch_trace(const wf_renderer* r, uint32_t grid_size, uint32_t block, cudaStream_t st, A... args) {
+    if (r->opaque)
+        k_trace<Opaque<Tally>, kLanes><<<grid_size, block, 0, st>>>(args...);
+    else
+        k_trace<Tally, kLanes><<<grid_size, block, 0, st>>>(args...);
+}
+// k_shade with the texture code only for scenes that have textured materials.
+template <typename... A>
+void launch_shade(const wf_renderer* r, uint32_t grid_size, uint32_t block, cudaStream_t st, A... args) {
+    if (r->textured)
+        k_shade<true><<<grid_size, block, 0, st>>>(args...);
+    else
+        k_shade<false><<<grid_size, block, 0, st>>>(args...);
+}
+template <typename Tally, typename... A>
+void launch_shadow(const wf_renderer* r, uint32_t grid_size, uint32_t block, cudaStream_t st, A... args) {
+    if (r->opaque)
+        k_shadow<Opaque<Tally>><<<grid_size, block, 0, st>>>(args...);
+    else
+        k_shadow<Tally><<<grid_size, block, 0, st>>>(args...);
+}
+
 wf_status capture_graph(wf_renderer* r) {
     const DeviceScene& s = r->scene->view;
     cudaStream_t st = r->stream;
@@ -918,15 +945,15 @@ wf_status capture_graph(wf_renderer* r) {
         uint32_t* cur_count = &r->counters->queue_count[cur];
         uint32_t* next_count = &r->counters->queue_count[nxt];
         if (b == 0)
-            k_trace<NoTally, false><<<grid(r, 5, cap, r->block_trace), r->block_trace, 0, st>>>(
+            launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st, 
                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill);
         else
-            k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
+            launch_trace<NoTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st, 
                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill);
         k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
                                                           r->counters);
         k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order, r->counters);
-        k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
+        launch_shade(r, grid(r, 1, cap, r->block_shade), r->block_shade, st, 
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
             r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers, r->shade_order);
         bool fork = r->params.photons.enabled != 0;
@@ -939,7 +966,7 @@ wf_status capture_graph(wf_renderer* r) {
                 r->params, r->gathers, r->terms, r->counters);
             WF_CUDA(cudaEventRecord(r->join_event, r->side));
         }
-        k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
+        launch_shadow<NoTally>(r, grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, st, 
             s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr, r->refill);
         if (fork) WF_CUDA(cudaStreamWaitEvent(st, r->join_event, 0));
         k_finalize<false><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
@@ -990,12 +1017,12 @@ wf_status capture_stream_graph(wf_renderer* r) {
         uint32_t nxt = cur ^ 1;
         uint32_t* cur_count = &r->counters->queue_count[cur];
         uint32_t* next_count = &r->counters->queue_count[nxt];
-        k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
+        launch_trace<NoTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st, 
             s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, kMaxBounces, nullptr, r->refill);
         k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
                                                           r->counters);
         k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order, r->counters);
-        k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
+        launch_shade(r, grid(r, 1, cap, r->block_shade), r->block_shade, st, 
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
             r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers, r->shade_order);
         bool fork = r->params.photons.enabled != 0;
@@ -1008,7 +1035,7 @@ wf_status capture_stream_graph(wf_renderer* r) {
                 r->params, r->gathers, r->terms, r->counters);
             WF_CUDA(cudaEventRecord(r->join_event, r->side));
         }
-        k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0, st>>>(
+        launch_shadow<NoTally>(r, grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, st, 
             s, r->shadow_origin, r->shadow_dir, r->shadow_result, r->counters, r->shadow_capacity, nullptr, r->refill);
         if (fork) WF_CUDA(cudaStreamWaitEvent(st, r->join_event, 0));
         k_finalize<true><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
@@ -1094,6 +1121,8 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
     if (c.block_size) r->block_trace = r->block_shade = c.block_size;
     if (c.refill_threshold > 32) return fail(WF_ERR_INVALID_ARG, "refill threshold must be between 0 and 32");
     r->refill = c.refill_threshold ? c.refill_threshold : 8u;
+    r->opaque = !scene->alpha_textures;
+    r->textured = scene->textured;
     if (stream) {
         r->stream = static_cast<cudaStream_t>(stream);
     } else {
@@ -1163,10 +1192,14 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
             r->gathers.dense_count = &r->counters->dense_count;
             WF_CUDA(resident_grid(rr, 4, k_gather, r->block_gather));
         }
-        WF_CUDA(resident_grid(rr, 0, k_trace<NoTally>, r->block_trace));
-        WF_CUDA(resident_grid(rr, 5, k_trace<NoTally, false>, r->block_trace));
-        WF_CUDA(resident_grid(rr, 1, k_shade, r->block_shade));
-        WF_CUDA(resident_grid(rr, 2, k_shadow<NoTally>, r->block_trace));
+        WF_CUDA(r->opaque ? resident_grid(rr, 0, k_trace<Opaque<NoTally>>, r->block_trace)
+                          : resident_grid(rr, 0, k_trace<NoTally>, r->block_trace));
+        WF_CUDA(r->opaque ? resident_grid(rr, 5, k_trace<Opaque<NoTally>, false>, r->block_trace)
+                          : resident_grid(rr, 5, k_trace<NoTally, false>, r->block_trace));
+        WF_CUDA(r->textured ? resident_grid(rr, 1, k_shade<true>, r->block_shade)
+                            : resident_grid(rr, 1, k_shade<false>, r->block_shade));
+        WF_CUDA(r->opaque ? resident_grid(rr, 2, k_shadow<Opaque<NoTally>>, r->block_trace)
+                          : resident_grid(rr, 2, k_shadow<NoTally>, r->block_trace));
         WF_CUDA(resident_grid(rr, 3, k_finalize<true>, r->block_finalize));
     } else {
         int cooperative = 0;
@@ -1456,19 +1489,19 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                     uint32_t* next_count = &r->counters->queue_count[nxt];
                     auto trace = [&] {
                         if (count && b == 0)
-                            k_trace<CountTally, false><<<grid(r, 5, cap, r->block_trace), r->block_trace, 0, st>>>(
+                            launch_trace<CountTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st, 
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
                                 r->tally, r->refill);
                         else if (count)
-                            k_trace<CountTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
+                            launch_trace<CountTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st, 
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
                                 r->tally, r->refill);
                         else if (b == 0)
-                            k_trace<NoTally, false><<<grid(r, 5, cap, r->block_trace), r->block_trace, 0, st>>>(
+                            launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st, 
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
                                 nullptr, r->refill);
                         else
-                            k_trace<NoTally><<<grid(r, 0, cap, r->block_trace), r->block_trace, 0, st>>>(
+                            launch_trace<NoTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st, 
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
                                 nullptr, r->refill);
                     };
@@ -1477,7 +1510,7 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                                                                           r->shade_key, r->counters);
                         k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order,
                                                                          r->counters);
-                        k_shade<<<grid(r, 1, cap, r->block_shade), r->block_shade, 0, st>>>(
+                        launch_shade(r, grid(r, 1, cap, r->block_shade), r->block_shade, st, 
                             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms,
                             r->shade_out, r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters,
                             next_count, r->gathers, r->shade_order);
@@ -1491,12 +1524,10 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                     bool gathers = r->params.photons.enabled != 0;
                     auto shadow = [&] {
                         if (count)
-                            k_shadow<CountTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace,
-                                                   0, st>>>(s, r->shadow_origin, r->shadow_dir, r->shadow_result,
+                            launch_shadow<CountTally>(r, grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, st, s, r->shadow_origin, r->shadow_dir, r->shadow_result,
                                                             r->counters, r->shadow_capacity, r->tally + 1, r->refill);
                         else
-                            k_shadow<NoTally><<<grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, 0,
-                                                st>>>(s, r->shadow_origin, r->shadow_dir, r->shadow_result,
+                            launch_shadow<NoTally>(r, grid(r, 2, r->shadow_capacity, r->block_trace), r->block_trace, st, s, r->shadow_origin, r->shadow_dir, r->shadow_result,
                                                       r->counters, r->shadow_capacity, nullptr, r->refill);
                     };
                     auto finalize = [&] {

@@ -83,6 +83,8 @@ struct wf_renderer {
     wf::RenderParams params{};
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    bool opaque = true;     // no alpha-textured material: the Opaque<> trace and shadow kernels
+    bool textured = false;  // some textured material: k_shade<true>
     int device = 0;
     int sm_count = 148;
     uint32_t capacity = 0;

@@ -120,7 +120,16 @@ void leaf_order(const std::vector<BvhBinaryNode>& bin, std::vector<uint32_t>& or
     }
 }
 
-void pack_triangle(HostScene& s, const wf_triangle& t, uint32_t original, uint32_t light, bool with_normals) {
+// `attr`: the triangle's texture coordinates and tangents, or null (zeros);
+// stored only when the scene carries attributes at all.
+void pack_triangle(HostScene& s, const wf_triangle& t, uint32_t original, uint32_t light, bool with_normals,
+                   const wf_triangle_attributes* attr, bool with_attributes) {
+    if (with_attributes) {
+        TriAttr a{};
+        static_assert(sizeof(wf_triangle_attributes) <= sizeof(TriAttr), "attribute record fits");
+        if (attr) std::memcpy(&a, attr, sizeof(wf_triangle_attributes));
+        s.tri_attr.push_back(a);
+    }
     uint32_t flags = original | (t.has_vertex_normals ? kTriHasNormals : 0u);
     s.triangles.push_back(make_float4(t.v0[0], t.v0[1], t.v0[2], bits_float(flags)));
     s.triangles.push_back(make_float4(t.v1[0], t.v1[1], t.v1[2], bits_float(t.material)));
@@ -265,11 +274,56 @@ wf_status build_host_scene(const wf_scene_desc* d, HostScene& s) {
             return fail(WF_ERR_INVALID_ARG, "punctual light %u has an unknown type", i);
 
     s = HostScene{};
+    // --- textures (uploadTextures, scene.cu:44-80): one RGBA8 texel pool
+    for (uint32_t i = 0; i < d->texture_count; ++i) {
+        const wf_texture& t = d->textures[i];
+        if (t.width == 0 || t.height == 0 || !t.rgba)
+            return fail(WF_ERR_INVALID_ARG, "texture %u is empty or has no texels", i);
+        s.textures.push_back(make_uint4(t.width, t.height, uint32_t(s.texels.size()), 0u));
+        size_t count = size_t(t.width) * t.height;
+        if (s.texels.size() + count > 0xffffffffull) return fail(WF_ERR_CAPACITY, "more than 2^32 texels");
+        const uchar4* p = reinterpret_cast<const uchar4*>(t.rgba);
+        s.texels.insert(s.texels.end(), p, p + count);
+    }
     for (uint32_t i = 0; i < nm; ++i) {
         s.materials.push_back(to_material(d->materials[i]));
-        if (s.materials.back().flags & kMatAlphaReject) s.any_alpha_reject = true;
         if (d->materials[i].type > WF_MAT_SPECGLOSS) return fail(WF_ERR_INVALID_ARG, "material %u has an unknown type", i);
+        if (d->material_textures) {
+            // sampleTexture ignores bindings past textureCount
+            // (device_traversal.cuh:342-343): they do not flag the material.
+            const wf_material_textures& w = d->material_textures[i];
+            MaterialTextures mt{};
+            mt.normal_scale = w.normal_scale;
+            mt.clearcoat_normal_scale = w.clearcoat_normal_scale;
+            mt.opacity = d->materials[i].opacity;
+            mt.alpha_cutoff = d->materials[i].alpha_cutoff;
+            const wf_texture_binding* slots[kTexSlots] = {
+                &w.albedo, &w.metallic_roughness, &w.emissive, &w.normal, &w.thickness, &w.specular_glossiness,
+                &w.specular_weight, &w.specular_color, &w.clearcoat, &w.clearcoat_roughness, &w.clearcoat_normal};
+            bool any = false;
+            for (uint32_t k = 0; k < kTexSlots; ++k) {
+                const wf_texture_binding& b = *slots[k];
+                mt.slot[k] = TexBinding{b.texture, b.texcoord, b.offset[0], b.offset[1], b.scale[0], b.scale[1],
+                                        b.rotation, b.has_transform};
+                any = any || b.texture < d->texture_count;
+            }
+            Material& m = s.materials.back();
+            if (any) {
+                m.flags |= kMatTextured;
+                s.textured = true;
+            }
+            if (d->materials[i].alpha_masked && w.albedo.texture < d->texture_count) {
+                m.flags = (m.flags & ~kMatAlphaReject) | kMatAlphaTexture;  // opacity * albedo.a per hit
+                s.alpha_textures = true;
+            }
+            s.material_textures.push_back(mt);
+        }
+        if (s.materials.back().flags & (kMatAlphaReject | kMatAlphaTexture)) s.any_alpha_reject = true;
     }
+    s.use_normal_maps = d->disable_normal_maps == 0;
+    s.normal_map_min_cosine = d->normal_map_minimum_cosine;
+    bool with_attributes = d->triangle_attributes != nullptr || d->static_triangle_attributes != nullptr;
+    for (uint32_t m = 0; m < d->mesh_count; ++m) with_attributes = with_attributes || d->meshes[m].attributes;
     bool with_normals = false;
     auto scan_normals = [&](const wf_triangle* t, uint32_t n) {
         for (uint32_t i = 0; i < n && !with_normals; ++i) with_normals = t[i].has_vertex_normals != 0;
@@ -357,14 +411,16 @@ wf_status build_host_scene(const wf_scene_desc* d, HostScene& s) {
             for (uint32_t k = 0; k < order.size(); ++k) {
                 uint32_t prim = order[k];
                 position[prim] = b.first + k;
-                pack_triangle(s, mesh.triangles[prim], prim, mesh_light[m][prim], with_normals);
+                pack_triangle(s, mesh.triangles[prim], prim, mesh_light[m][prim], with_normals,
+                              mesh.attributes ? &mesh.attributes[prim] : nullptr, with_attributes);
             }
             for (uint32_t i = 0; i < mesh.triangle_count; ++i) s.mesh_linear[b.first_linear + i] = position[i];
             Converter c{bin, s.nodes, [&](uint32_t prim) { return position[prim]; }};
             b.bvh = c.root();
         } else {
             for (uint32_t i = 0; i < mesh.triangle_count; ++i) {
-                pack_triangle(s, mesh.triangles[i], i, mesh_light[m][i], with_normals);
+                pack_triangle(s, mesh.triangles[i], i, mesh_light[m][i], with_normals,
+                              mesh.attributes ? &mesh.attributes[i] : nullptr, with_attributes);
                 s.mesh_linear[b.first_linear + i] = b.first + i;
             }
         }
@@ -441,7 +497,8 @@ wf_status build_host_scene(const wf_scene_desc* d, HostScene& s) {
     s.static_first = uint32_t(s.triangles.size() / 3);
     s.static_count = d->static_triangle_count;
     for (uint32_t i = 0; i < d->static_triangle_count; ++i) {
-        pack_triangle(s, d->static_triangles[i], i, static_light[i], with_normals);
+        pack_triangle(s, d->static_triangles[i], i, static_light[i], with_normals,
+                      d->static_triangle_attributes ? &d->static_triangle_attributes[i] : nullptr, with_attributes);
         grow(s.bounds, triangle_box(d->static_triangles[i]));
     }
 
@@ -457,12 +514,15 @@ wf_status build_host_scene(const wf_scene_desc* d, HostScene& s) {
         std::vector<uint32_t> position(d->triangle_count);
         for (uint32_t k = 0; k < order.size(); ++k) {
             position[order[k]] = s.direct_first + k;
-            pack_triangle(s, d->triangles[order[k]], order[k], kInvalid, with_normals);
+            pack_triangle(s, d->triangles[order[k]], order[k], kInvalid, with_normals,
+                          d->triangle_attributes ? &d->triangle_attributes[order[k]] : nullptr, with_attributes);
         }
         Converter c{bin, s.nodes, [&](uint32_t prim) { return position[prim]; }};
         s.direct_bvh = c.root();
     } else {
-        for (uint32_t i = 0; i < d->triangle_count; ++i) pack_triangle(s, d->triangles[i], i, kInvalid, with_normals);
+        for (uint32_t i = 0; i < d->triangle_count; ++i)
+            pack_triangle(s, d->triangles[i], i, kInvalid, with_normals,
+                          d->triangle_attributes ? &d->triangle_attributes[i] : nullptr, with_attributes);
     }
     for (uint32_t i = 0; i < d->triangle_count; ++i) grow(s.bounds, triangle_box(d->triangles[i]));
 

@@ -418,11 +418,100 @@ WF_DEV float material_roughness(const Material& m) {
 }
 
 // Hit as seen by the shading functions (hit / shadedHit of the reference).
+// coat_normal: the clearcoat normal of getGltfPbrSurface before its flip
+// (the hit's shading normal unless a clearcoat normal map applies).
 struct ShadeHit {
     float t;
     V3 position, geometric_normal, normal;
     uint32_t material, light;
+    V3 coat_normal;
 };
+
+// ------------------------------------------------------- textured materials
+// srgbToLinear / gltfSrgbChannel, device_traversal.cuh:349-362.
+WF_DEV V3 srgb_to_linear(float4 t) {
+    return V3{wfm::powf(t.x, 2.2f), wfm::powf(t.y, 2.2f), wfm::powf(t.z, 2.2f)};
+}
+WF_DEV float gltf_srgb_channel(float value) {
+    return value <= 0.04045f ? value / 12.92f : wfm::powf((value + 0.055f) / 1.055f, 2.4f);
+}
+WF_DEV V3 gltf_srgb_to_linear(float4 t) {
+    return V3{gltf_srgb_channel(t.x), gltf_srgb_channel(t.y), gltf_srgb_channel(t.z)};
+}
+
+// The factors of a textured material at a hit: getMaterialAlbedo, Emission,
+// Metallic, Roughness (device_traversal.cuh:363-395), getSpecGlossSurface's
+// specular (:397-401), getGltfPbrSurface's specular weight and colour and
+// clearcoat factors (:500-516) and getMaterialThickness (:443-449), each
+// evaluated once.  Without a binding every one of them returns the factor
+// itself (texel fallback 1, srgb(1) = 1), which is what untextured
+// materials use directly.
+WF_CALL Material resolve_material(const DeviceScene& s, const Material& m, uint32_t index, const SurfaceHit& sh) {
+    const MaterialTextures& mt = s.material_textures[index];
+    const float4 one = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+    Material r = m;
+    bool sg = (m.flags & kMatSpecGlossWorkflow) != 0;
+    float4 albedo = sample_binding(s, mt.slot[kTexAlbedo], sh.uv, sh.uv1, one);
+    r.albedo = hadamard(m.albedo, sg ? gltf_srgb_to_linear(albedo) : srgb_to_linear(albedo));
+    r.emission = hadamard(m.emission, srgb_to_linear(sample_binding(s, mt.slot[kTexEmissive], sh.uv, sh.uv1, one)));
+    float4 mr = sample_binding(s, mt.slot[kTexMetallicRoughness], sh.uv, sh.uv1, one);
+    float4 sgt = sample_binding(s, mt.slot[kTexSpecGloss], sh.uv, sh.uv1, one);
+    r.metallic = m.metallic * mr.z;
+    if (sg)
+        r.glossiness = m.glossiness * sgt.w;  // material_roughness: 1 - glossiness * texel.w
+    else
+        r.roughness = m.roughness * mr.y;
+    r.specular = hadamard(m.specular, gltf_srgb_to_linear(sgt));
+    r.specular_weight = m.specular_weight * sample_binding(s, mt.slot[kTexSpecularWeight], sh.uv, sh.uv1, one).w;
+    r.specular_color = hadamard(m.specular_color,
+                                gltf_srgb_to_linear(sample_binding(s, mt.slot[kTexSpecularColor], sh.uv, sh.uv1, one)));
+    r.clearcoat = m.clearcoat * sample_binding(s, mt.slot[kTexClearcoat], sh.uv, sh.uv1, one).x;
+    r.clearcoat_roughness =
+        m.clearcoat_roughness * sample_binding(s, mt.slot[kTexClearcoatRoughness], sh.uv, sh.uv1, one).y;
+    const TexBinding& th = mt.slot[kTexThickness];
+    float thickness = th.texture == kInvalid || th.texture >= s.texture_count
+                          ? 1.0f
+                          : sample_binding(s, th, sh.uv, sh.uv1, one).x;
+    r.volume_density = m.volume_density * thickness;
+    return r;
+}
+
+WF_DEV bool finite3(V3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
+
+// getMaterialNormal, device_traversal.cuh:451-499: the normal map in the
+// hit's tangent frame (the clearcoat normal map with its own scale for
+// getGltfPbrSurface), or the hit's shading normal.
+WF_CALL V3 material_normal(const DeviceScene& s, const TexBinding& b, float normal_scale, const SurfaceHit& sh) {
+    if (!s.use_normal_maps || b.texture == kInvalid || b.texture >= s.texture_count) return sh.normal;
+    V3 tangent = b.texcoord == 1 ? sh.tangent1 : sh.tangent;
+    V3 bitangent = b.texcoord == 1 ? sh.bitangent1 : sh.bitangent;
+    if (!finite3(tangent) || !finite3(bitangent) || length_squared(tangent) < 0.00000001f ||
+        length_squared(bitangent) < 0.00000001f)
+        return sh.normal;
+    tangent = normalize(tangent - sh.normal * dot(sh.normal, tangent));
+    bitangent = normalize(cross(sh.normal, tangent));
+    if (!finite3(tangent) || !finite3(bitangent)) return sh.normal;
+    if (dot(bitangent, b.texcoord == 1 ? sh.bitangent1 : sh.bitangent) < 0.0f) bitangent = -bitangent;
+    float4 texel = sample_binding(s, b, sh.uv, sh.uv1, make_float4(0.5f, 0.5f, 1.0f, 1.0f));
+    V3 tn{(texel.x * 2.0f - 1.0f) * normal_scale, (texel.y * 2.0f - 1.0f) * normal_scale, texel.z * 2.0f - 1.0f};
+    tn = normalize(tn);
+    if (s.normal_map_min_cosine > 0.0f && tn.z < s.normal_map_min_cosine) {
+        float minimum_cosine = fminf(s.normal_map_min_cosine, 1.0f);
+        float tangent_length = sqrtf(fmaxf(0.0f, tn.x * tn.x + tn.y * tn.y));
+        if (tangent_length > 0.0f) {
+            float scale = sqrtf(fmaxf(0.0f, 1.0f - minimum_cosine * minimum_cosine)) / tangent_length;
+            tn.x *= scale;
+            tn.y *= scale;
+        } else {
+            tn.x = 0.0f;
+            tn.y = 0.0f;
+        }
+        tn.z = minimum_cosine;
+    }
+    V3 normal = tangent * tn.x + bitangent * tn.y + sh.normal * tn.z;
+    if (!finite3(normal) || length_squared(normal) < 0.00000001f) return sh.normal;
+    return normalize(normal);
+}
 
 // evaluateSurface, device_traversal.cuh:427-441.
 WF_CALL V3 evaluate_surface(const DeviceScene& s, const Material& m, const ShadeHit& hit, V3 outgoing, V3 incoming,
@@ -441,14 +530,15 @@ WF_CALL V3 evaluate_surface(const DeviceScene& s, const Material& m, const Shade
     return m.albedo * 0.31830988618f;
 }
 
-// getGltfPbrSurface, device_traversal.cuh:500-516 (untextured).
+// getGltfPbrSurface, device_traversal.cuh:500-516 (texture factors resolved
+// by resolve_material, the clearcoat normal by shade_path).
 WF_CALL GltfPbr gltf_surface(const Material& m, const ShadeHit& hit, const ShadeHit& shaded) {
     float weight = m.specular_weight;
     V3 color = m.specular_color;
     float f0 = (m.ior - 1.f) / (m.ior + 1.f);
     f0 *= f0;
     V3 df0{fminf(1.f, f0 * color.x) * weight, fminf(1.f, f0 * color.y) * weight, fminf(1.f, f0 * color.z) * weight};
-    V3 coat_normal = hit.normal;
+    V3 coat_normal = shaded.coat_normal;
     if (dot(coat_normal, hit.geometric_normal) < 0) coat_normal = -coat_normal;
     GltfPbr g;
     g.color = m.albedo;
@@ -1162,12 +1252,21 @@ WF_DEV V3 continue_gltf(const DeviceScene& s, const RenderParams& rp, Path& path
 // Returns false when the path ends with this event (the caller then adds the
 // path radiance to the framebuffer); the sink may still end it through a
 // visible terminal branch.
-template <typename Sink>
+// kTextures = false compiles the texture code out, for kernels the host
+// launches only on scenes without textured materials.
+template <typename Sink, bool kTextures = true>
 WF_DEV bool shade_path(const DeviceScene& s, const RenderParams& rp, Path& path, bool did_hit, const SurfaceHit& sh,
                        Sink& sink) {
     if (rp.debug == 1 || rp.debug == 2) {
         V3 color{0.05f, 0.10f, 0.25f};
-        if (did_hit) color = 0.5f * (sh.normal + V3{1.0f, 1.0f, 1.0f});
+        V3 n = sh.normal;
+        if constexpr (kTextures) {
+            if (did_hit && rp.debug == 2 && (s.materials[sh.material].flags & kMatTextured) && s.material_textures) {
+                const MaterialTextures& mt = s.material_textures[sh.material];
+                n = material_normal(s, mt.slot[kTexNormal], mt.normal_scale, sh);
+            }
+        }
+        if (did_hit) color = 0.5f * (n + V3{1.0f, 1.0f, 1.0f});
         sink.term(color, kUnconditional);
         path.active = false;
         return false;
@@ -1177,8 +1276,15 @@ WF_DEV bool shade_path(const DeviceScene& s, const RenderParams& rp, Path& path,
         path.active = false;
         return false;
     }
-    ShadeHit hit{sh.t, sh.position, sh.geometric_normal, sh.normal, sh.material, sh.light};
-    const Material& m = s.materials[hit.material];
+    ShadeHit hit{sh.t, sh.position, sh.geometric_normal, sh.normal, sh.material, sh.light, sh.normal};
+    const Material& stored = s.materials[hit.material];
+    bool textured = false;
+    Material resolved;
+    if constexpr (kTextures) {
+        textured = (stored.flags & kMatTextured) && s.material_textures;
+        if (textured) resolved = resolve_material(s, stored, hit.material, sh);
+    }
+    const Material& m = textured ? resolved : stored;
     if (path.medium != kInvalid) {
         const Material& medium = s.materials[path.medium];
         if (medium.attenuation_distance > 0.0f) {
@@ -1208,6 +1314,11 @@ WF_DEV bool shade_path(const DeviceScene& s, const RenderParams& rp, Path& path,
         return false;
     }
     ShadeHit shaded = hit;
+    if (textured) {
+        const MaterialTextures& mt = s.material_textures[hit.material];
+        shaded.normal = material_normal(s, mt.slot[kTexNormal], mt.normal_scale, sh);
+        shaded.coat_normal = material_normal(s, mt.slot[kTexClearcoatNormal], mt.clearcoat_normal_scale, sh);
+    }
     if (dot(shaded.normal, hit.geometric_normal) < 0.0f) shaded.normal = -shaded.normal;
     V3 albedo = m.albedo;
     uint32_t type = m.type == kDiffuse && m.metallic > 0.5f ? uint32_t(kMetal) : m.type;

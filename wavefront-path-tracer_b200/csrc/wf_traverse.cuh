@@ -24,18 +24,30 @@ constexpr int kStackSize = 64;  // leaf depth <= kMaxBvhDepth (60) < 64
 // node visits (one visit = one 64-byte node = two child boxes), triangle,
 // sphere and instance tests a traversal performs, for the algorithmic-byte
 // accounting of the profiling pass.
+// A tally type also fixes, at compile time, whether the traversal may meet
+// alpha-textured materials (kAlphaTextures): the default types handle every
+// scene; Opaque<T> compiles the per-hit texture test out, for kernels that
+// the host launches only on scenes without such materials.
 struct NoTally {
+    static constexpr bool kCounts = false;
+    static constexpr bool kAlphaTextures = true;
     WF_DEV void node() {}
     WF_DEV void triangle() {}
     WF_DEV void sphere() {}
     WF_DEV void instance() {}
 };
 struct CountTally {
+    static constexpr bool kCounts = true;
+    static constexpr bool kAlphaTextures = true;
     uint32_t nodes = 0, triangles = 0, spheres = 0, instances = 0;
     WF_DEV void node() { ++nodes; }
     WF_DEV void triangle() { ++triangles; }
     WF_DEV void sphere() { ++spheres; }
     WF_DEV void instance() { ++instances; }
+};
+template <typename Base>
+struct Opaque : Base {
+    static constexpr bool kAlphaTextures = false;
 };
 
 struct TraceState {
@@ -126,8 +138,78 @@ WF_DEV TriVerts load_triangle(const DeviceScene& s, uint32_t i) {
                     __float_as_uint(c.w)};
 }
 
-WF_DEV bool alpha_rejects(const DeviceScene& s, uint32_t material) {
-    return s.any_alpha_reject && (s.materials[material].flags & kMatAlphaReject);
+// ---------------------------------------------------------------- textures
+// tex2D<float4> on an RGBA8 texture with normalised reads, wrap addressing
+// and linear filtering (src/scene/scene.cu:54-69), in the arithmetic of the
+// host replay of the reference's kernels (cpu_replay.cpp:14-24): texel-centre
+// offset, floor, wrap, weights (1 - f, f), rows then columns, bytes / 255 as
+// bytes * (1 / 255).
+WF_DEV float4 texture_fetch(const DeviceScene& s, uint32_t texture, float u, float v) {
+    uint4 info = s.textures[texture];
+    int w = int(info.x), h = int(info.y);
+    float tx = u * float(info.x) - .5f, ty = v * float(info.y) - .5f;
+    int x = int(floorf(tx)), y = int(floorf(ty));
+    float fx = tx - float(x), fy = ty - float(y);
+    const float scale = 1.0f / 255.0f;
+    float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i) {
+            int xx = (((x + i) % w) + w) % w, yy = (((y + j) % h) + h) % h;
+            uchar4 p = s.texels[info.z + size_t(yy) * uint32_t(w) + uint32_t(xx)];
+            float wt = (i ? fx : 1.0f - fx) * (j ? fy : 1.0f - fy);
+            r.x += wt * (float(p.x) * scale);
+            r.y += wt * (float(p.y) * scale);
+            r.z += wt * (float(p.z) * scale);
+            r.w += wt * (float(p.w) * scale);
+        }
+    return r;
+}
+
+// getTriangleUv, device_traversal.cuh:120-131, for both coordinate sets.
+WF_DEV void triangle_uvs(const DeviceScene& s, uint32_t ti, float u, float v, float2& uv, float2& uv1) {
+    uv = uv1 = make_float2(0.0f, 0.0f);
+    if (!s.tri_attr) return;
+    const TriAttr& a = s.tri_attr[ti];
+    float w = 1.0f - u - v;
+    if (a.has_texcoords)
+        uv = make_float2(w * a.uv[0][0] + u * a.uv[1][0] + v * a.uv[2][0], w * a.uv[0][1] + u * a.uv[1][1] + v * a.uv[2][1]);
+    if (a.has_texcoords1)
+        uv1 = make_float2(w * a.uv1[0][0] + u * a.uv1[1][0] + v * a.uv1[2][0],
+                          w * a.uv1[0][1] + u * a.uv1[1][1] + v * a.uv1[2][1]);
+}
+
+// getTextureUv + sampleTexture, device_traversal.cuh:325-347.
+WF_DEV float4 sample_binding(const DeviceScene& s, const TexBinding& b, float2 uv, float2 uv1, float4 fallback) {
+    if (b.texture == kInvalid || b.texture >= s.texture_count) return fallback;
+    float2 t = b.texcoord == 1 ? uv1 : uv;
+    if (b.has_transform) {
+        t.x *= b.scale_x;
+        t.y *= b.scale_y;
+        float sine = wfm::sinf(b.rotation), cosine = wfm::cosf(b.rotation);
+        t = make_float2(cosine * t.x - sine * t.y + b.offset_x, sine * t.x + cosine * t.y + b.offset_y);
+    }
+    return texture_fetch(s, b.texture, t.x, 1.0f - t.y);
+}
+
+// alphaMasked && getMaterialOpacity < alphaCutoff (device_traversal.cuh:
+// 150,265,370-378): untextured materials carry the answer as a flag; with an
+// albedo texture the opacity is read at the candidate hit.  Tally decides at
+// compile time whether the texture test exists in the kernel.
+template <typename Tally>
+WF_DEV bool alpha_rejects(const DeviceScene& s, uint32_t material, uint32_t ti, float u, float v) {
+    if (!s.any_alpha_reject) return false;
+    uint32_t flags = s.materials[material].flags;
+    if constexpr (Tally::kAlphaTextures) {
+        if (flags & kMatAlphaTexture) {
+            const MaterialTextures& mt = s.material_textures[material];
+            float2 uv, uv1;
+            triangle_uvs(s, ti, u, v, uv, uv1);
+            float opacity =
+                mt.opacity * sample_binding(s, mt.slot[kTexAlbedo], uv, uv1, make_float4(1.0f, 1.0f, 1.0f, 1.0f)).w;
+            return opacity < mt.alpha_cutoff;
+        }
+    }
+    return (flags & kMatAlphaReject) != 0;
 }
 
 // Local stack of (ref, entry distance).
@@ -157,7 +239,7 @@ WF_DEV void bvh_closest(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, Tra
             float t, u, v;
             if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < h.t) {
                 uint32_t m = material_override == kInvalid ? tri.material : material_override;
-                if (!alpha_rejects(s, m)) {
+                if (!alpha_rejects<Tally>(s, m, ti, u, v)) {
                     h.t = t;
                     h.u = u;
                     h.v = v;
@@ -215,7 +297,7 @@ WF_DEV bool bvh_any(const DeviceScene& s, const BvhRef& bvh, V3 o, V3 d, float t
             float t, u, v;
             if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < t_max) {
                 uint32_t m = material_override == kInvalid ? tri.material : material_override;
-                if (!alpha_rejects(s, m)) return true;
+                if (!alpha_rejects<Tally>(s, m, ti, u, v)) return true;
             }
         } else {
             tally.node();
@@ -274,7 +356,7 @@ WF_DEV void mesh_linear_closest(const DeviceScene& s, const Blas& b, V3 o, V3 d,
         float t, u, v;
         if (!intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
         uint32_t m = material_override == kInvalid ? tri.material : material_override;
-        if (alpha_rejects(s, m)) continue;
+        if (alpha_rejects<Tally>(s, m, ti, u, v)) continue;
         h.t = t;
         h.u = u;
         h.v = v;
@@ -315,7 +397,7 @@ WF_DEV bool instance_any(const DeviceScene& s, uint32_t inst, V3 o, V3 d, float 
         float t, u, v;
         if (!intersect_triangle(lo, ld, tri.v0, tri.v1, tri.v2, t, u, v) || t >= t_max) continue;
         uint32_t m = in.material_override == kInvalid ? tri.material : in.material_override;
-        if (!alpha_rejects(s, m)) return true;
+        if (!alpha_rejects<Tally>(s, m, s.mesh_linear[b.first_linear + i], u, v)) return true;
     }
     return false;
 }
@@ -436,7 +518,7 @@ WF_DEV void trace_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h, Tally
         TriVerts tri = load_triangle(s, ti);
         float t, u, v;
         if (!intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
-        if (alpha_rejects(s, tri.material)) continue;
+        if (alpha_rejects<Tally>(s, tri.material, ti, u, v)) continue;
         h.t = t;
         h.u = u;
         h.v = v;
@@ -456,7 +538,7 @@ WF_DEV void trace_closest(const DeviceScene& s, V3 o, V3 d, TraceState& h, Tally
                 TriVerts tri = load_triangle(s, ti);
                 float t, u, v;
                 if (!intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) || t >= h.t) continue;
-                if (alpha_rejects(s, tri.material)) continue;
+                if (alpha_rejects<Tally>(s, tri.material, ti, u, v)) continue;
                 h.t = t;
                 h.u = u;
                 h.v = v;
@@ -484,7 +566,7 @@ WF_DEV bool trace_any(const DeviceScene& s, V3 o, V3 d, float t_max, Tally& tall
         TriVerts tri = load_triangle(s, s.static_first + i);
         float t, u, v;
         if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < t_max &&
-            !alpha_rejects(s, tri.material))
+            !alpha_rejects<Tally>(s, tri.material, s.static_first + i, u, v))
             return true;
     }
     if (tlas_any(s, o, d, t_max, tally)) return true;
@@ -495,7 +577,7 @@ WF_DEV bool trace_any(const DeviceScene& s, V3 o, V3 d, float t_max, Tally& tall
             TriVerts tri = load_triangle(s, s.direct_first + i);
             float t, u, v;
             if (intersect_triangle(o, d, tri.v0, tri.v1, tri.v2, t, u, v) && t < t_max &&
-                !alpha_rejects(s, tri.material))
+                !alpha_rejects<Tally>(s, tri.material, s.direct_first + i, u, v))
                 return true;
         }
     }
@@ -515,7 +597,43 @@ struct SurfaceHit {
     V3 normal;
     uint32_t material;
     uint32_t light;
+    // texture coordinates and tangent frames (Hit::uv .. bitangent1); zero
+    // for spheres and for scenes without triangle attributes
+    float2 uv, uv1;
+    V3 tangent, bitangent, tangent1, bitangent1;
 };
+
+// transformVector, include/scene/scene.cuh:40-42.
+WF_DEV V3 transform_vector(const Instance& in, V3 v) {
+    return V3{in.l2w_x.x, in.l2w_x.y, in.l2w_x.z} * v.x + V3{in.l2w_y.x, in.l2w_y.y, in.l2w_y.z} * v.y +
+           V3{in.l2w_z.x, in.l2w_z.y, in.l2w_z.z} * v.z;
+}
+
+// The texture coordinates and tangent frame intersectTriangleHit records for
+// the winning triangle (device_traversal.cuh:147-174), with `n` its
+// (face-forwarded, instance-local) shading normal.
+WF_DEV void triangle_frames(const DeviceScene& s, uint32_t ti, float u, float v, V3 n, SurfaceHit& out) {
+    triangle_uvs(s, ti, u, v, out.uv, out.uv1);
+    const TriAttr& a = s.tri_attr[ti];
+    V3 tangent{a.tangent[0], a.tangent[1], a.tangent[2]};
+    V3 bitangent{a.bitangent[0], a.bitangent[1], a.bitangent[2]};
+    if (a.has_vertex_tangents) {
+        float w = 1.0f - u - v;
+        V3 t = w * V3{a.vertex_tangent[0][0], a.vertex_tangent[0][1], a.vertex_tangent[0][2]} +
+               u * V3{a.vertex_tangent[1][0], a.vertex_tangent[1][1], a.vertex_tangent[1][2]} +
+               v * V3{a.vertex_tangent[2][0], a.vertex_tangent[2][1], a.vertex_tangent[2][2]};
+        t = t - n * dot(n, t);
+        if (length_squared(t) > 0.00000001f) {
+            tangent = normalize(t);
+            float sign = w * a.vertex_tangent_sign[0] + u * a.vertex_tangent_sign[1] + v * a.vertex_tangent_sign[2];
+            bitangent = (sign < 0.0f ? -1.0f : 1.0f) * normalize(cross(n, tangent));
+        }
+    }
+    out.tangent = tangent;
+    out.bitangent = bitangent;
+    out.tangent1 = V3{a.tangent1[0], a.tangent1[1], a.tangent1[2]};
+    out.bitangent1 = V3{a.bitangent1[0], a.bitangent1[1], a.bitangent1[2]};
+}
 
 WF_DEV V3 triangle_geometric_normal(const TriVerts& tri, V3 d, bool face_forward) {
     V3 n = normalize(cross(tri.v1 - tri.v0, tri.v2 - tri.v0));
@@ -549,6 +667,8 @@ WF_DEV bool finish_hit(const DeviceScene& s, V3 o, V3 d, float t, float u, float
     uint32_t kind = hit_kind(prim), index = hit_index(prim);
     if (kind == kHitMiss) return false;
     out.t = t;
+    out.uv = out.uv1 = make_float2(0.0f, 0.0f);
+    out.tangent = out.bitangent = out.tangent1 = out.bitangent1 = V3{0.0f, 0.0f, 0.0f};
     if (kind == kHitSphere) {
         float4 sp = __ldg(&s.spheres[index]);
         V3 at = o + d * t;
@@ -563,6 +683,7 @@ WF_DEV bool finish_hit(const DeviceScene& s, V3 o, V3 d, float t, float u, float
         out.geometric_normal = triangle_geometric_normal(tri, d, ff);
         out.normal = triangle_shading_normal(s, index, tri, d, u, v, ff);
         out.light = tri.light;
+        if (s.tri_attr) triangle_frames(s, index, u, v, out.normal, out);
     } else {
         Instance in = load_instance(s, inst);
         TriVerts tri = load_triangle(s, index);
@@ -574,6 +695,14 @@ WF_DEV bool finish_hit(const DeviceScene& s, V3 o, V3 d, float t, float u, float
         V3 n = triangle_shading_normal(s, index, tri, ld, u, v, ff);
         out.geometric_normal = transform_normal(in, gn);
         out.normal = transform_normal(in, n);
+        if (s.tri_attr) {  // intersectMeshInstance, device_traversal.cuh:826-829
+            triangle_frames(s, index, u, v, n, out);
+            const Instance& full = s.instances[inst];  // load_instance reads only the world-to-local rows
+            out.tangent = normalize(transform_vector(full, out.tangent));
+            out.bitangent = normalize(transform_vector(full, out.bitangent));
+            out.tangent1 = normalize(transform_vector(full, out.tangent1));
+            out.bitangent1 = normalize(transform_vector(full, out.bitangent1));
+        }
         uint32_t light = in.material_override == kInvalid ? tri.light : kInvalid;
         if (light != kInvalid) light += in.light_offset;
         out.light = light;

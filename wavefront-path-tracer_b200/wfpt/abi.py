@@ -30,7 +30,24 @@ TRIANGLE_DTYPE = np.dtype([
     ("material", "<u4"), ("has_vertex_normals", "<u4"),
 ])
 SPHERE_DTYPE = np.dtype([("center", "<f4", (3,)), ("radius", "<f4"), ("material", "<u4"), ("accel", "<u4")])
-MESH_DTYPE = np.dtype([("triangles", "<u8"), ("triangle_count", "<u4"), ("pad", "<u4")])
+MESH_DTYPE = np.dtype([("triangles", "<u8"), ("triangle_count", "<u4"), ("pad", "<u4"), ("attributes", "<u8")])
+# Texture coordinates and tangent frames of a triangle (wf_triangle_attributes).
+TRIANGLE_ATTRIBUTES_DTYPE = np.dtype([
+    ("uv", "<f4", (3, 2)), ("uv1", "<f4", (3, 2)),
+    ("tangent", "<f4", (3,)), ("bitangent", "<f4", (3,)), ("tangent1", "<f4", (3,)), ("bitangent1", "<f4", (3,)),
+    ("vertex_tangent", "<f4", (3, 3)), ("vertex_tangent_sign", "<f4", (3,)),
+    ("has_vertex_tangents", "<u4"), ("has_texcoords", "<u4"), ("has_texcoords1", "<u4"),
+])
+NO_TEXTURE = 0xFFFFFFFF
+TEXTURE_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("rgba", "<u8")])
+TEXTURE_BINDING_DTYPE = np.dtype([
+    ("texture", "<u4"), ("texcoord", "<u4"), ("offset", "<f4", (2,)), ("scale", "<f4", (2,)),
+    ("rotation", "<f4"), ("has_transform", "<u4"),
+])
+TEXTURE_SLOTS = ("albedo", "metallic_roughness", "emissive", "normal", "thickness", "specular_glossiness",
+                 "specular_weight", "specular_color", "clearcoat", "clearcoat_roughness", "clearcoat_normal")
+MATERIAL_TEXTURES_DTYPE = np.dtype([("normal_scale", "<f4"), ("clearcoat_normal_scale", "<f4")] +
+                                   [(k, TEXTURE_BINDING_DTYPE) for k in TEXTURE_SLOTS])
 INSTANCE_DTYPE = np.dtype([
     ("mesh", "<u4"), ("material_override", "<u4"), ("accel", "<u4"),
     ("local_to_world", "<f4", (3, 3)), ("world_to_local", "<f4", (3, 3)), ("translation", "<f4", (3,)),
@@ -56,6 +73,8 @@ HIT_DTYPE = np.dtype([
 ])
 
 assert TRIANGLE_DTYPE.itemsize == 80 and SPHERE_DTYPE.itemsize == 24 and INSTANCE_DTYPE.itemsize == 96
+assert MESH_DTYPE.itemsize == 24 and TRIANGLE_ATTRIBUTES_DTYPE.itemsize == 156 and TEXTURE_DTYPE.itemsize == 16
+assert TEXTURE_BINDING_DTYPE.itemsize == 32 and MATERIAL_TEXTURES_DTYPE.itemsize == 360
 assert MATERIAL_DTYPE.itemsize == 124 and PUNCTUAL_DTYPE.itemsize == 52
 assert RAY_DTYPE.itemsize == 24 and HIT_DTYPE.itemsize == 68
 
@@ -78,6 +97,10 @@ class SceneDesc(C.Structure):
         ("register_triangle_lights", C.c_uint32),
         ("build_threads", C.c_uint32),
         ("bvh_builder", C.c_uint32), ("reserved", C.c_uint32),
+        ("textures", C.c_void_p), ("texture_count", C.c_uint32), ("disable_normal_maps", C.c_uint32),
+        ("material_textures", C.c_void_p), ("triangle_attributes", C.c_void_p),
+        ("static_triangle_attributes", C.c_void_p), ("normal_map_minimum_cosine", C.c_float),
+        ("reserved2", C.c_uint32),
     ]
 
 

@@ -84,6 +84,17 @@ class Scene:
         self.register_triangle_lights = True
         self.build_threads = 0
         self.bvh_builder = abi.BVH_HOST_SAH  # or abi.BVH_GPU_PLOC
+        # textured materials (all optional): RGBA8 textures (uint8[h, w, 4]),
+        # one MATERIAL_TEXTURES_DTYPE record per material, and per-triangle
+        # TRIANGLE_ATTRIBUTES_DTYPE arrays parallel to triangles,
+        # static_triangles and each mesh (mesh_attributes[i] or None)
+        self.textures = []
+        self.material_textures = None
+        self.triangle_attributes = None
+        self.static_triangle_attributes = None
+        self.mesh_attributes = []
+        self.disable_normal_maps = False
+        self.normal_map_minimum_cosine = 0.0
 
     def add_material(self, record):
         self.materials = np.concatenate([self.materials, np.array([record], abi.MATERIAL_DTYPE)])
@@ -110,6 +121,11 @@ class Scene:
             m = arr(m, abi.TRIANGLE_DTYPE)
             meshes[i]["triangles"] = m.ctypes.data if len(m) else 0
             meshes[i]["triangle_count"] = len(m)
+            attrs = self.mesh_attributes[i] if i < len(self.mesh_attributes) else None
+            if attrs is not None:
+                a = arr(attrs, abi.TRIANGLE_ATTRIBUTES_DTYPE)
+                assert len(a) == len(m), "one attribute record per mesh triangle"
+                meshes[i]["attributes"] = a.ctypes.data
         keep.append(meshes)
         d = abi.SceneDesc()
         for name, src, dtype in [("spheres", self.spheres, abi.SPHERE_DTYPE),
@@ -129,6 +145,28 @@ class Scene:
         d.register_triangle_lights = int(self.register_triangle_lights)
         d.build_threads = self.build_threads
         d.bvh_builder = self.bvh_builder
+        if self.textures:
+            tex = np.zeros(len(self.textures), abi.TEXTURE_DTYPE)
+            for i, t in enumerate(self.textures):
+                t = arr(t, np.uint8)
+                assert t.ndim == 3 and t.shape[2] == 4, "textures are uint8[h, w, 4]"
+                tex[i] = (t.shape[1], t.shape[0], t.ctypes.data)
+            keep.append(tex)
+            d.textures = abi.ptr(tex)
+            d.texture_count = len(tex)
+        if self.material_textures is not None:
+            mt = arr(self.material_textures, abi.MATERIAL_TEXTURES_DTYPE)
+            assert len(mt) == len(self.materials), "one texture record per material"
+            d.material_textures = abi.ptr(mt)
+        for name, attrs, tris in [("triangle_attributes", self.triangle_attributes, self.triangles),
+                                  ("static_triangle_attributes", self.static_triangle_attributes,
+                                   self.static_triangles)]:
+            if attrs is not None:
+                a = arr(attrs, abi.TRIANGLE_ATTRIBUTES_DTYPE)
+                assert len(a) == len(tris), f"one {name} record per triangle"
+                setattr(d, name, abi.ptr(a))
+        d.disable_normal_maps = int(self.disable_normal_maps)
+        d.normal_map_minimum_cosine = float(self.normal_map_minimum_cosine)
         return d, keep
 
     def environment_struct(self):

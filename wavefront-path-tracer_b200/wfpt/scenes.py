@@ -455,3 +455,143 @@ def inverse_parameters(scene, parameter_count, seed, albedo_range=(0.15, 0.85), 
     rlo, rhi = roughness_range
     rough = rlo + (rhi - rlo) * 0.5 * (1.0 + value_noise(centroid, seed + 17, frequency=0.6))
     return albedo[:parameter_count].astype(np.float32), rough[:parameter_count].astype(np.float32)
+
+
+# ------------------------------------------------------ textured materials
+def texture_binding(texture=abi.NO_TEXTURE, texcoord=0, offset=(0.0, 0.0), scale=(1.0, 1.0), rotation=None):
+    """One wf_texture_binding; `rotation` (or a non-unit scale/offset) sets
+    the KHR_texture_transform."""
+    b = np.zeros((), abi.TEXTURE_BINDING_DTYPE)
+    b["texture"], b["texcoord"] = texture, texcoord
+    b["offset"], b["scale"] = offset, scale
+    b["rotation"] = rotation or 0.0
+    b["has_transform"] = int(rotation is not None or tuple(scale) != (1.0, 1.0) or tuple(offset) != (0.0, 0.0))
+    return b
+
+
+def material_textures(**slots):
+    """One wf_material_textures record: unbound slots get WF_NO_TEXTURE,
+    normal scales default to 1."""
+    r = np.zeros(1, abi.MATERIAL_TEXTURES_DTYPE)
+    r["normal_scale"] = slots.pop("normal_scale", 1.0)
+    r["clearcoat_normal_scale"] = slots.pop("clearcoat_normal_scale", 1.0)
+    for k in abi.TEXTURE_SLOTS:
+        r[k] = slots.pop(k, texture_binding())
+    assert not slots, f"unknown slots {sorted(slots)}"
+    return r
+
+
+def _uv_grid(p0, eu, ev, n, mat, uv_scale=1.0, vertex_tangents=True, sign=1.0):
+    """A grid quad (as _grid_quad) with texture coordinates: set 0 runs along
+    (eu, ev) over [0, uv_scale]^2, set 1 along (ev, eu) over [0, 1]^2; face
+    tangents follow eu / ev (set 0) and ev / eu (set 1); vertex tangents
+    (every other cell) carry `sign`."""
+    tris = _grid_quad(p0, eu, ev, n, mat)
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    i, j = i.ravel().astype(np.float64), j.ravel().astype(np.float64)
+    a = np.stack([i / n, j / n], 1)
+    b = np.stack([(i + 1) / n, j / n], 1)
+    c = np.stack([(i + 1) / n, (j + 1) / n], 1)
+    d = np.stack([i / n, (j + 1) / n], 1)
+    uv = np.stack([np.stack([a, b, c], 1), np.stack([a, c, d], 1)], 1).reshape(-1, 3, 2)
+    attrs = np.zeros(len(tris), abi.TRIANGLE_ATTRIBUTES_DTYPE)
+    attrs["uv"] = uv * uv_scale
+    attrs["uv1"] = uv[:, :, ::-1]
+    tu = np.asarray(eu, np.float64) / np.linalg.norm(eu)
+    tv = np.asarray(ev, np.float64) / np.linalg.norm(ev)
+    attrs["tangent"], attrs["bitangent"] = tu, tv
+    attrs["tangent1"], attrs["bitangent1"] = tv, tu
+    attrs["has_texcoords"] = 1
+    attrs["has_texcoords1"] = 1
+    if vertex_tangents:
+        every_other = (np.arange(len(tris)) // 2) % 2 == 0
+        attrs["vertex_tangent"][every_other] = tu
+        attrs["vertex_tangent_sign"][every_other] = sign
+        attrs["has_vertex_tangents"][every_other] = 1
+    return tris, attrs
+
+
+def _procedural_textures(seed=5):
+    """RGBA8 textures (uint8[h, w, 4]): checker, bump normal map, metallic-
+    roughness, emissive pattern, alpha card with round holes, specular-
+    glossiness, clearcoat factors."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:64, 0:64] / 64.0
+    checker = (((x * 8).astype(int) + (y * 8).astype(int)) % 2).astype(np.float64)
+    albedo = np.stack([0.2 + 0.7 * checker, 0.25 + 0.5 * (1 - checker), 0.3 + 0.4 * x, np.ones_like(x)], -1)
+    hx = np.cos(x * 2 * np.pi * 4) * 0.6
+    hy = np.sin(y * 2 * np.pi * 3) * 0.6
+    nrm = np.stack([hx, hy, np.ones_like(x)], -1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    normal = np.concatenate([nrm * 0.5 + 0.5, np.ones_like(x)[..., None]], -1)
+    mr = np.stack([np.zeros_like(x), 0.1 + 0.8 * y, ((x * 6).astype(int) % 2).astype(np.float64), np.ones_like(x)], -1)
+    emissive = np.stack([0.5 + 0.5 * np.sin(x * 20), 0.5 + 0.5 * np.cos(y * 17), 0.8 * x * y, np.ones_like(x)], -1)
+    holes = ((np.mod(x * 5, 1.0) - 0.5) ** 2 + (np.mod(y * 5, 1.0) - 0.5) ** 2) < 0.09
+    card = np.stack([0.3 + 0.5 * y, 0.6 * np.ones_like(x), 0.2 + 0.3 * x, np.where(holes, 0.1, 1.0)], -1)
+    specgloss = np.stack([0.4 + 0.5 * x, 0.4 + 0.5 * y, 0.5 * np.ones_like(x), 0.2 + 0.75 * checker], -1)
+    coat = np.stack([0.3 + 0.7 * checker, 0.1 + 0.8 * x, np.zeros_like(x), np.ones_like(x)], -1)
+    noise = rng.uniform(0, 1, (64, 64, 4)) * 0.02
+    to8 = lambda t: np.clip(np.round((t + noise) * 255.0), 0, 255).astype(np.uint8)
+    return [to8(t) for t in (albedo, normal, mr, emissive, card, specgloss, coat)]
+
+
+def textured_room(width=96, height=96):
+    """A room whose surfaces use every texture path of the shading code:
+    checker albedo with a transform and a normal map (floor), glTF PBR with
+    metallic-roughness, clearcoat and clearcoat normal textures (back wall),
+    specular-glossiness on coordinate set 1 with a rotated transform (left
+    wall), an emissive-textured light panel, an alpha-masked card with holes,
+    two instances of a normal-mapped metal panel (tangents through instance
+    transforms), and a glass block with a thickness texture."""
+    s = Scene()
+    ALB, NRM, MR, EMI, CARD, SG, COAT = range(7)
+    s.textures = _procedural_textures()
+    tex = []
+    white = s.add_material(material(abi.MAT_DIFFUSE, (0.9, 0.9, 0.9)))
+    tex.append(material_textures(albedo=texture_binding(ALB, 0, (0.1, 0.2), (3.0, 3.0), 0.3),
+                                 normal=texture_binding(NRM, 0, scale=(2.0, 2.0)), normal_scale=0.8))
+    pbr = s.add_material(material(abi.MAT_DIFFUSE, (0.95, 0.9, 0.85), roughness=1.0, metallic=1.0, gltf_pbr=1,
+                                  clearcoat=0.8, clearcoat_roughness=0.6, ior=1.5))
+    tex.append(material_textures(albedo=texture_binding(ALB), metallic_roughness=texture_binding(MR),
+                                 clearcoat=texture_binding(COAT), clearcoat_roughness=texture_binding(COAT),
+                                 clearcoat_normal=texture_binding(NRM, 1), clearcoat_normal_scale=0.5))
+    sg = s.add_material(material(abi.MAT_SPECGLOSS, (0.8, 0.8, 0.8), specgloss_workflow=1, glossiness=0.9,
+                                 specular=(0.9, 0.9, 0.9)))
+    tex.append(material_textures(albedo=texture_binding(ALB, 1),
+                                 specular_glossiness=texture_binding(SG, 1, (0.05, 0.0), (1.5, 1.5), -0.7)))
+    plain = s.add_material(material(abi.MAT_DIFFUSE, (0.12, 0.45, 0.15)))
+    tex.append(material_textures())
+    light = s.add_material(material(abi.MAT_EMISSIVE, (1.0, 1.0, 1.0), (12.0, 12.0, 12.0)))
+    tex.append(material_textures(emissive=texture_binding(EMI)))
+    card = s.add_material(material(abi.MAT_DIFFUSE, (1.0, 1.0, 1.0), alpha_masked=1, alpha_cutoff=0.5))
+    tex.append(material_textures(albedo=texture_binding(CARD)))
+    panel = s.add_material(material(abi.MAT_METAL, (0.9, 0.85, 0.7), roughness=0.4, metallic=1.0))
+    tex.append(material_textures(metallic_roughness=texture_binding(MR), normal=texture_binding(NRM, 0, rotation=1.1)))
+    glass = s.add_material(material(abi.MAT_DIELECTRIC, (1.0, 1.0, 1.0), ior=1.5, attenuation_color=(0.6, 0.8, 0.9),
+                                    attenuation_distance=0.8, volume_density=1.5))
+    tex.append(material_textures(thickness=texture_binding(MR)))
+    s.material_textures = np.concatenate(tex)
+
+    w, fy, cy, bz, fz = 2.5, -1.0, 3.0, -2.5, 2.5
+    parts = [
+        _uv_grid((-w, fy, fz), (2 * w, 0, 0), (0, 0, bz - fz), 6, white, uv_scale=2.0, sign=-1.0),
+        _uv_grid((-w, fy, bz), (2 * w, 0, 0), (0, cy - fy, 0), 6, pbr),
+        _uv_grid((-w, fy, fz), (0, 0, bz - fz), (0, cy - fy, 0), 6, sg),
+        _uv_grid((w, fy, bz), (0, 0, fz - bz), (0, cy - fy, 0), 2, plain, vertex_tangents=False),
+        _uv_grid((-w, cy, bz), (2 * w, 0, 0), (0, 0, fz - bz), 2, white),
+        _uv_grid((-0.8, 2.95, -0.8), (1.6, 0, 0), (0, 0, 1.6), 2, light),
+        _uv_grid((-1.8, -0.9, -0.2), (1.6, 0, 0.3), (0, 2.2, 0), 3, card),
+        _uv_grid((0.6, -0.99, -0.2), (0.9, 0, 0), (0, 0, 0.9), 1, glass),
+    ]
+    room = np.concatenate([p[0] for p in parts])
+    room_attrs = np.concatenate([p[1] for p in parts])
+    panel_tris, panel_attrs = _uv_grid((-0.5, 0.0, 0.0), (1.0, 0.0, 0.0), (0.0, 1.0, 0.0), 3, panel, sign=-1.0)
+    m_room = s.add_mesh(room)
+    m_panel = s.add_mesh(panel_tris)
+    s.mesh_attributes = [room_attrs, panel_attrs]
+    s.instances = np.concatenate([instance(m_room), instance(m_panel, (1.2, 0.2, -1.6), 1.2, 35.0),
+                                  instance(m_panel, (-0.2, 1.4, -2.0), 0.8, -20.0)])
+    s.spheres = np.array([((0.9, -0.6, 0.9), 0.4, glass, abi.ACCEL_BVH)], abi.SPHERE_DTYPE)
+    s.black_background = True
+    cam = look_at_camera((0.0, 1.0, 6.2), (0.0, 0.8, -0.6), 45.0, width, height)
+    return s, cam

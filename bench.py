@@ -182,6 +182,45 @@ def cpu_reference_rate(ref, cam, width, height, render_kwargs, seconds_target=15
     return width * band / dt / 1e6, cores, f"{width}x{band} rows at 1 spp (a band of one sample pass)", dt
 
 
+def time_frame_guides(dev_scene, cam, width, height, launches=10):
+    """wf_frame_guides over the whole frame with a previous camera 1 % of the
+    view's width to the side: the denoiser guides of the dataset capture.
+    Device time per launch (CUDA events on the launching stream, 3 warm-up
+    launches) and the fraction of pixels with a valid history."""
+    import ctypes
+    import numpy as np
+    import torch
+    import wfpt
+    lib = wfpt.library()
+    prev = dict(cam)
+    prev["position"] = (np.asarray(cam["position"], np.float32)
+                        + 0.01 * np.asarray(cam["right"], np.float32)).tolist()
+    c, p = wfpt.camera_struct(cam), wfpt.camera_struct(prev)
+    out = torch.empty(width * height * wfpt.abi.FRAME_GUIDE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def call():
+        wfpt.check(lib.wf_frame_guides(dev_scene.handle, ctypes.byref(c), ctypes.byref(p), width, height, 0, 0,
+                                       width, height, out.data_ptr(), stream.cuda_stream))
+    for _ in range(3):
+        call()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(launches):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / launches
+    g = out.cpu().numpy().view(wfpt.abi.FRAME_GUIDE_DTYPE)
+    # a valid pixel that projects into the previous frame traces a second ray
+    second = float((g["valid"] * (np.abs(g["motion"]).sum(axis=1) > 0)).mean())
+    return {"ms_per_frame": round(ms, 3), "mpixels_per_s": round(width * height / ms / 1e3, 1),
+            "valid_fraction": round(float(g["valid"].mean()), 4),
+            "history_valid_fraction": round(float(g["history_valid"].mean()), 4),
+            "traversals_per_pixel_at_least": round(1.0 + second, 3), "launches": launches + 3}
+
+
 def reference_scene(scene):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
@@ -599,6 +638,7 @@ def main():
     reference_cuda = None
     if rank == 0 and world == 1 and args.reference_cuda:
         reference_cuda = reference_cuda_comparison(args.workload)
+    guides = time_frame_guides(dev_scene, cam, width, height) if rank == 0 else None
 
     if rank == 0:
         line = {
@@ -629,6 +669,7 @@ def main():
             "clocks": clock_record,
             "setup_seconds": setup_s,
         }
+        line["frame_guides"] = guides  # measured after the timed region
         if reference_cuda is not None:
             line["reference_cuda"] = reference_cuda
         print(json.dumps(line), flush=True)

@@ -313,6 +313,32 @@ typedef struct wf_camera {
     float aspect_ratio;
 } wf_camera;
 
+/* FrameGuide (include/renderer/frame_guides.cuh:9-17), 56 bytes: the
+ * denoiser guides of one pixel.  Normals are world space and face the
+ * geometric normal's side; depth is the distance along the camera's forward
+ * axis; motion is the previous frame's pixel minus this one (integer pixel
+ * centres); valid = 1 on a hit; history_valid = 1 when the surface also
+ * projects into the previous frame and is visible there. */
+typedef struct wf_frame_guide {
+    float albedo[3];
+    float normal[3];
+    float geometric_normal[3];
+    float depth;
+    float motion[2];
+    float valid;
+    float history_valid;
+} wf_frame_guide;
+
+/* generateFrameGuides (include/renderer/device_frame_guides.cuh:6-41) over
+ * the tile (x, y, w, h) of a width x height image: one unjittered ray through
+ * each pixel centre.  guides is a DEVICE array of w*h records, tile-local and
+ * row-major, as tools/dataset_capture.cu:105-121 launches it.  previous (the
+ * previous frame's camera) may be NULL: motion and history_valid stay 0.
+ * Asynchronous on `stream` (cudaStream_t, may be NULL). */
+wf_status wf_frame_guides(const wf_scene* scene, const wf_camera* camera, const wf_camera* previous,
+                          uint32_t width, uint32_t height, uint32_t x, uint32_t y, uint32_t w, uint32_t h,
+                          wf_frame_guide* guides, void* stream);
+
 /* GRAPH: the reference's captured wavefront, one graph replay per tile and
  * sample (render_driver.cu:264-352).  PERSISTENT: one cooperative launch per
  * tile and sample (renderer.cu:55-125).  STREAM: one graph replay per tile

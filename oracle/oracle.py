@@ -44,6 +44,8 @@ def ref_lib(det=False):
         lib.wfref_photons.argtypes = [P, P, P, P, P, I]
         lib.wfref_render.restype = I
         lib.wfref_render.argtypes = [P, P, P, U32, U32, U32, U32, U32, U32, P, P, P, I, I]
+        lib.wfref_frame_guides.restype = I
+        lib.wfref_frame_guides.argtypes = [P, P, P, U32, U32, U32, U32, U32, U32, P, I]
         lib.wfref_dielectric_reflectance.restype = C.c_float
         lib.wfref_dielectric_reflectance.argtypes = [C.c_float, C.c_float]
         lib.wfref_checkpoint_roundtrip_read.restype = I
@@ -114,6 +116,20 @@ class RefScene:
         self.lib.wfref_photons(self.handle, C.addressof(config), rec.ctypes.data, flux.ctypes.data,
                                C.addressof(stored), threads)
         return rec, flux, stored.value
+
+    def frame_guides(self, camera, width, height, tile=None, previous=None, threads=0):
+        """The reference's generateFrameGuides over a tile: (h, w) FRAME_GUIDE_DTYPE records."""
+        from wfpt import abi
+        from wfpt.native import camera_struct
+        cam = camera_struct(camera)
+        prev = camera_struct(previous) if previous is not None else None
+        x, y, w, h = tile if tile is not None else (0, 0, width, height)
+        out = np.zeros((h, w), abi.FRAME_GUIDE_DTYPE)
+        rc = self.lib.wfref_frame_guides(self.handle, C.addressof(cam), C.addressof(prev) if prev else None,
+                                         width, height, x, y, w, h, out.ctypes.data, threads)
+        if rc != 0:
+            raise RuntimeError("reference frame guides failed")
+        return out
 
     def render(self, camera, config, tile=None, sample_start=0, sample_count=1, threads=0, persistent=False,
                fp64=False):

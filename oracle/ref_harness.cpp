@@ -15,6 +15,7 @@
 #include "scene/environment.hpp"
 #include "scene/scene_host.hpp"
 #include "renderer/render_session.cuh"
+#include "renderer/frame_guides.cuh"
 
 #include "../include/wavefront.h"
 #include "../wavefront-path-tracer_b200/csrc/bvh_build.h"
@@ -432,6 +433,36 @@ int wfref_photons(void* handle, const wf_render_config* c, float* records, float
 // the FP32 framebuffer sums exactly as the reference accumulates them;
 // fb64 (nullable) the per-sample radiance summed in FP64.  queue_counts
 // (nullable) receives max_depth counts per sample (sample-major).
+// generateFrameGuides (device_frame_guides.cuh:6-41) as host code, one host
+// worker per CUDA thread, over the tile (x, y, w, h) of a width x height
+// image; out receives w*h FrameGuide records.  prev may be NULL.
+int wfref_frame_guides(void* handle, const wf_camera* cam, const wf_camera* prev, uint32_t width, uint32_t height,
+                       uint32_t x, uint32_t y, uint32_t w, uint32_t h, wf_frame_guide* out, int threads) {
+    static_assert(sizeof(FrameGuide) == sizeof(wf_frame_guide), "FrameGuide layout");
+    RefScene* r = static_cast<RefScene*>(handle);
+    if (!r || !cam || !out) return 1;
+    auto camera = [](const wf_camera* c) {
+        Camera k;
+        k.position = v3(c->position);
+        k.forward = v3(c->forward);
+        k.right = v3(c->right);
+        k.up = v3(c->up);
+        k.verticalFov = c->vertical_fov;
+        k.aspectRatio = c->aspect_ratio;
+        return k;
+    };
+    Scene scene = r->device.scene;
+    Camera now = camera(cam);
+    Camera before = prev ? camera(prev) : now;
+    RenderTile tile{x, y, w, h, 1};
+    std::vector<FrameGuide> guides(size_t(w) * h);
+    parallel_for(w * h, threads, [&](uint32_t) {
+        generateFrameGuides(guides.data(), scene, now, before, prev != nullptr, width, height, tile);
+    });
+    std::memcpy(out, guides.data(), sizeof(FrameGuide) * guides.size());
+    return 0;
+}
+
 int wfref_render(void* handle, const wf_camera* cam, const wf_render_config* c, uint32_t x0, uint32_t y0,
                  uint32_t tw, uint32_t th, uint32_t sample_start, uint32_t sample_count, float* fb32,
                  double* fb64, uint32_t* queue_counts, int threads, int persistent) {

@@ -53,7 +53,9 @@ def test_struct_sizes_compiled_from_header(tmp_path):
     pairs = {"wf_camera": abi.Camera, "wf_render_config": abi.RenderConfig, "wf_scene_desc": abi.SceneDesc,
              "wf_kernel_profile": abi.KernelProfile, "wf_render_stats": abi.RenderStats,
              "wf_batch_job": abi.BatchJob, "wf_batch_config": abi.BatchConfig, "wf_scene_info": abi.SceneInfo,
-             "wf_environment": abi.Environment, "wf_diff_config": abi.DiffConfig}
+             "wf_environment": abi.Environment, "wf_diff_config": abi.DiffConfig,
+             "wf_frame_guide": abi.FRAME_GUIDE_DTYPE, "wf_hit": abi.HIT_DTYPE, "wf_ray": abi.RAY_DTYPE,
+             "wf_material_textures": abi.MATERIAL_TEXTURES_DTYPE}
     src = tmp_path / "sizes.c"
     body = "".join(f'    printf("%zu\\n", sizeof({name}));\n' for name in pairs)
     src.write_text('#include <stdio.h>\n#include "wavefront.h"\nint main(void) {\n' + body + "    return 0;\n}\n")
@@ -61,7 +63,8 @@ def test_struct_sizes_compiled_from_header(tmp_path):
     subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     sizes = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
     for (name, struct), size in zip(pairs.items(), sizes):
-        assert ctypes.sizeof(struct) == size, name
+        mirrored = struct.itemsize if hasattr(struct, "itemsize") else ctypes.sizeof(struct)
+        assert mirrored == size, name
 
 
 def test_defaults_and_errors_without_gpu():

@@ -299,6 +299,16 @@ wf_status wf_trace_any(const wf_scene* s, const wf_ray* rays, const float* max_d
     return trace_any_batch(s, rays, max_distance, count, occluded, static_cast<cudaStream_t>(stream));
 }
 
+wf_status wf_frame_guides(const wf_scene* s, const wf_camera* camera, const wf_camera* previous, uint32_t width,
+                          uint32_t height, uint32_t x, uint32_t y, uint32_t w, uint32_t h, wf_frame_guide* guides,
+                          void* stream) {
+    if (!s || !camera || (uint64_t(w) * h && !guides)) return fail(WF_ERR_INVALID_ARG, "null argument");
+    if (!width || !height || uint64_t(x) + w > width || uint64_t(y) + h > height)
+        return fail(WF_ERR_INVALID_ARG, "tile (%u, %u, %u, %u) is outside the %u x %u image", x, y, w, h, width,
+                    height);
+    return frame_guides(s, camera, previous, width, height, x, y, w, h, guides, static_cast<cudaStream_t>(stream));
+}
+
 wf_status wf_renderer_create(const wf_scene* scene, const wf_camera* camera, const wf_render_config* config,
                              void* stream, wf_renderer** out) {
     return renderer_create(scene, camera, config, stream, out);

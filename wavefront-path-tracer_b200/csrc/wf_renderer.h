@@ -155,4 +155,7 @@ wf_status trace_closest_batch(const wf_scene* scene, const wf_ray* rays, uint32_
 wf_status trace_any_batch(const wf_scene* scene, const wf_ray* rays, const float* max_distance, uint32_t count,
                           uint8_t* occluded, cudaStream_t stream);
 wf_status cuda_fail(cudaError_t e, const char* what);
+wf_status frame_guides(const wf_scene* scene, const wf_camera* camera, const wf_camera* previous, uint32_t width,
+                       uint32_t height, uint32_t x, uint32_t y, uint32_t w, uint32_t h, wf_frame_guide* guides,
+                       cudaStream_t stream);
 }  // namespace wf

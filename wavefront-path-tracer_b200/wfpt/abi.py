@@ -71,12 +71,17 @@ HIT_DTYPE = np.dtype([
     ("material", "<u4"), ("light_index", "<u4"), ("kind", "<u4"), ("instance", "<u4"), ("primitive", "<u4"),
     ("u", "<f4"), ("v", "<f4"),
 ])
+# wf_frame_guide (FrameGuide, include/renderer/frame_guides.cuh:9-17)
+FRAME_GUIDE_DTYPE = np.dtype([
+    ("albedo", "<f4", (3,)), ("normal", "<f4", (3,)), ("geometric_normal", "<f4", (3,)), ("depth", "<f4"),
+    ("motion", "<f4", (2,)), ("valid", "<f4"), ("history_valid", "<f4"),
+])
 
 assert TRIANGLE_DTYPE.itemsize == 80 and SPHERE_DTYPE.itemsize == 24 and INSTANCE_DTYPE.itemsize == 96
 assert MESH_DTYPE.itemsize == 24 and TRIANGLE_ATTRIBUTES_DTYPE.itemsize == 156 and TEXTURE_DTYPE.itemsize == 16
 assert TEXTURE_BINDING_DTYPE.itemsize == 32 and MATERIAL_TEXTURES_DTYPE.itemsize == 360
 assert MATERIAL_DTYPE.itemsize == 124 and PUNCTUAL_DTYPE.itemsize == 52
-assert RAY_DTYPE.itemsize == 24 and HIT_DTYPE.itemsize == 68
+assert RAY_DTYPE.itemsize == 24 and HIT_DTYPE.itemsize == 68 and FRAME_GUIDE_DTYPE.itemsize == 56
 
 
 BVH_HOST_SAH = 0
@@ -190,6 +195,7 @@ def declare(lib):
         "wf_scene_get_info": (S, [P, C.POINTER(SceneInfo)]),
         "wf_bvh_build": (S, [U32, P, U32, P, P]),
         "wf_trace_closest": (S, [P, P, U32, P, P]),
+        "wf_frame_guides": (S, [P, P, P, U32, U32, U32, U32, U32, U32, P, P]),
         "wf_trace_any": (S, [P, P, P, U32, P, P]),
         "wf_render_config_default": (None, [C.POINTER(RenderConfig), U32, U32]),
         "wf_renderer_create": (S, [P, C.POINTER(Camera), C.POINTER(RenderConfig), P, C.POINTER(P)]),

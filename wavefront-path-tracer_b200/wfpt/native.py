@@ -231,6 +231,21 @@ class DeviceScene:
         torch.cuda.synchronize()
         return d_hits.cpu().numpy().view(abi.HIT_DTYPE)
 
+    def frame_guides(self, camera, width, height, tile=None, previous=None):
+        """wf_frame_guides: the denoiser guides of a tile of a width x height
+        image as (h, w) FRAME_GUIDE_DTYPE records; previous is the previous
+        frame's camera (None: no motion or history)."""
+        import torch
+        x, y, w, h = tile if tile is not None else (0, 0, width, height)
+        out = torch.empty(w * h * abi.FRAME_GUIDE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        cam = camera_struct(camera)
+        prev = camera_struct(previous) if previous is not None else None
+        stream = torch.cuda.current_stream().cuda_stream
+        check(library().wf_frame_guides(self.handle, C.byref(cam), C.byref(prev) if prev is not None else None,
+                                        width, height, x, y, w, h, out.data_ptr(), stream))
+        torch.cuda.synchronize()
+        return out.cpu().numpy().view(abi.FRAME_GUIDE_DTYPE).reshape(h, w)
+
     def trace_any(self, rays, max_distance):
         import torch
         rays = np.ascontiguousarray(rays, abi.RAY_DTYPE)

@@ -46,6 +46,20 @@ def ref_lib(det=False):
         lib.wfref_render.argtypes = [P, P, P, U32, U32, U32, U32, U32, U32, P, P, P, I, I]
         lib.wfref_frame_guides.restype = I
         lib.wfref_frame_guides.argtypes = [P, P, P, U32, U32, U32, U32, U32, U32, P, I]
+        lib.wfref_host_preset.restype = P
+        lib.wfref_host_preset.argtypes = [I, C.c_char_p, C.c_float, P, I, I, I, I, I, I, I, I]
+        lib.wfref_host_scene_destroy.argtypes = [P]
+        lib.wfref_host_scene_counts.argtypes = [P, P]
+        lib.wfref_host_scene_triangle_count.restype = C.c_uint64
+        lib.wfref_host_scene_triangle_count.argtypes = [P, I, U32]
+        lib.wfref_host_scene_triangles.argtypes = [P, I, U32, P, P]
+        lib.wfref_host_scene_materials.argtypes = [P, P, P]
+        lib.wfref_host_scene_instances.argtypes = [P, P]
+        lib.wfref_host_scene_spheres.argtypes = [P, P]
+        lib.wfref_host_scene_punctual.argtypes = [P, P]
+        lib.wfref_host_scene_texture.argtypes = [P, U32, P, P]
+        lib.wfref_scene_from_host.restype = P
+        lib.wfref_scene_from_host.argtypes = [P, I, C.c_float]
         lib.wfref_dielectric_reflectance.restype = C.c_float
         lib.wfref_dielectric_reflectance.argtypes = [C.c_float, C.c_float]
         lib.wfref_checkpoint_roundtrip_read.restype = I
@@ -278,3 +292,83 @@ class PortScene:
         if rc != 0:
             raise RuntimeError("oracle render failed")
         return fb, counts
+
+
+PRESET_KINDS = {"gltf": 0, "cornell": 1, "obj": 2}
+OBJECT_SOURCES = {"obj": 0, "gltf": 1, "procedural_prism": 2}
+LIGHT_PROFILES = {"standard": 0, "prism": 1, "crystal": 2}
+
+
+class RefHostScene:
+    """A HostScene built by the reference's own loaders and preset assembly
+    (ref_assets.cpp), exported in the wfpt array layouts."""
+
+    def __init__(self, kind, filename, scale=1.0, translation=(0.0, 0.0, 0.0), object_source="obj",
+                 neutral_room=False, remove_backdrop=False, dielectric=False, material_override=-1,
+                 light_profile="standard", add_top_light=True, det=True):
+        self.lib = ref_lib(det)
+        t = np.asarray(translation, np.float32)
+        self.handle = self.lib.wfref_host_preset(PRESET_KINDS[kind], str(filename).encode(), float(scale),
+                                                 t.ctypes.data, OBJECT_SOURCES[object_source], int(neutral_room),
+                                                 int(remove_backdrop), int(dielectric), int(material_override),
+                                                 LIGHT_PROFILES[light_profile], int(add_top_light), 0)
+        if not self.handle:
+            raise RuntimeError("the reference's preset assembly failed")
+
+    def close(self):
+        if self.handle:
+            self.lib.wfref_host_scene_destroy(self.handle)
+            self.handle = None
+
+    def arrays(self, texels=True):
+        """dict: spheres, triangles, static_triangles, meshes, mesh_attributes,
+        instances, materials, material_textures, textures, punctual,
+        light_count, black_background."""
+        from wfpt import abi
+        counts = np.zeros(10, np.uint64)
+        self.lib.wfref_host_scene_counts(self.handle, counts.ctypes.data)
+        n_sph, n_tri, n_static, n_mesh, n_inst, n_mat, n_tex, n_punct, n_lights, black = (int(x) for x in counts)
+
+        def tris(which, mesh=0):
+            n = int(self.lib.wfref_host_scene_triangle_count(self.handle, which, mesh))
+            t = np.zeros(n, abi.TRIANGLE_DTYPE)
+            a = np.zeros(n, abi.TRIANGLE_ATTRIBUTES_DTYPE)
+            self.lib.wfref_host_scene_triangles(self.handle, which, mesh, t.ctypes.data, a.ctypes.data)
+            return t, a
+        out = {"light_count": n_lights, "black_background": bool(black)}
+        out["triangles"], out["triangle_attributes"] = tris(0)
+        out["static_triangles"], out["static_triangle_attributes"] = tris(1)
+        meshes = [tris(2, m) for m in range(n_mesh)]
+        out["meshes"] = [m[0] for m in meshes]
+        out["mesh_attributes"] = [m[1] for m in meshes]
+        out["materials"] = np.zeros(n_mat, abi.MATERIAL_DTYPE)
+        out["material_textures"] = np.zeros(n_mat, abi.MATERIAL_TEXTURES_DTYPE)
+        self.lib.wfref_host_scene_materials(self.handle, out["materials"].ctypes.data,
+                                            out["material_textures"].ctypes.data)
+        out["instances"] = np.zeros(n_inst, abi.INSTANCE_DTYPE)
+        self.lib.wfref_host_scene_instances(self.handle, out["instances"].ctypes.data)
+        out["spheres"] = np.zeros(n_sph, abi.SPHERE_DTYPE)
+        self.lib.wfref_host_scene_spheres(self.handle, out["spheres"].ctypes.data)
+        out["punctual"] = np.zeros(n_punct, abi.PUNCTUAL_DTYPE)
+        self.lib.wfref_host_scene_punctual(self.handle, out["punctual"].ctypes.data)
+        textures = []
+        for i in range(n_tex):
+            size = np.zeros(2, np.uint32)
+            self.lib.wfref_host_scene_texture(self.handle, i, size.ctypes.data, None)
+            rgba = np.zeros((int(size[1]), int(size[0]), 4), np.uint8)
+            if texels:
+                self.lib.wfref_host_scene_texture(self.handle, i, size.ctypes.data, rgba.ctypes.data)
+            textures.append(rgba)
+        out["textures"] = textures
+        return out
+
+    def render_scene(self, disable_normal_maps=False, normal_map_minimum_cosine=0.0):
+        """A RefScene rendering this HostScene (BVH2s from the same builder as
+        scenes from a description)."""
+        r = RefScene.__new__(RefScene)
+        r.lib = self.lib
+        r.handle = self.lib.wfref_scene_from_host(self.handle, int(disable_normal_maps),
+                                                  float(normal_map_minimum_cosine))
+        if not r.handle:
+            raise RuntimeError("wfref_scene_from_host failed")
+        return r

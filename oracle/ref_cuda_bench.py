@@ -15,6 +15,7 @@ between the two renderers' images of the last task (the same paths; the two
 builds differ only in floating-point contraction and elementary functions).
 
     python oracle/ref_cuda_bench.py --workload large_mesh --mode graph --steps 5
+    python oracle/ref_cuda_bench.py --manifest assets/scenes/sponza.json --spp 4
 """
 import argparse
 import ctypes as C
@@ -52,13 +53,23 @@ def main():
                     help="schedule of the B200 renderer (default: bench.py's schedule for the workload)")
     ap.add_argument("--steps", type=int, default=5, help="timed tasks (after one warm-up task)")
     ap.add_argument("--sample-start", type=int, default=1000)
+    ap.add_argument("--manifest", default=None,
+                    help="a scene manifest of the reference's presets, loaded by wfpt.assets, instead of a workload")
+    ap.add_argument("--size", default="1280x720", help="image size for --manifest")
     args = ap.parse_args()
 
     import bench
     import wfpt
     from wfpt import native
 
-    scene, cam, width, height, rkw = bench.make_scene(args.workload)
+    if args.manifest:
+        from wfpt import assets
+        width, height = (int(x) for x in args.size.split("x"))
+        scene, cam = assets.preset_scene(args.manifest, width, height)
+        rkw = {}
+        args.workload = "preset " + Path(args.manifest).stem
+    else:
+        scene, cam, width, height, rkw = bench.make_scene(args.workload)
     for k in ("caustics", "photon_count"):
         rkw.pop(k, None)
     args.spp = args.spp or bench.SPP_PER_STEP.get(args.workload, 1)
@@ -107,7 +118,8 @@ def main():
     diff = own_img.astype(np.float64) - ref_img.astype(np.float64)
     rel_rmse = float(np.sqrt(np.mean(diff ** 2)) / max(np.sqrt(np.mean(ref_img.astype(np.float64) ** 2)), 1e-30))
     print(json.dumps({
-        "workload": args.workload, "width": width, "height": height, "spp_per_task": args.spp,
+        "workload": args.workload, "triangles": int(scene.triangle_count()), "width": width, "height": height,
+        "spp_per_task": args.spp,
         "max_depth": cfg.max_depth, "caustics": 0, "reference_mode": args.mode, "own_mode": own_mode,
         "reference_cuda": {"Mpaths/s": paths / ref_t / 1e3, "ms_per_task": ref_t,
                            "ms_per_task_all": [round(x, 3) for x in ref_ms], "scene_setup_s": ref_setup},

@@ -238,6 +238,27 @@ void* wfref_scene_create(const wf_scene_desc* d, const wf_environment* env, int 
     }
 }
 
+HostScene* wfref_host_scene_get(void* host);  // ref_assets.cpp
+
+// A renderable reference scene from a HostScene that the reference's own
+// loaders and preset assembly built (ref_assets.cpp).  Its BVH2s go through
+// the same NexusBVH builder as scenes from a description.
+void* wfref_scene_from_host(void* host, int disable_normal_maps, float normal_map_minimum_cosine) {
+    try {
+        HostScene h = *wfref_host_scene_get(host);
+        h.acceleration = ObjAccelerationPolicy::NexusBvh2;
+        auto r = std::make_unique<RefScene>();
+        r->original_material_count = uint32_t(h.materials.size());
+        r->device = uploadScene(h);
+        r->device.scene.useNormalMaps = disable_normal_maps == 0;
+        r->device.scene.normalMapMinimumCosine = normal_map_minimum_cosine;
+        return r.release();
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "wfref_scene_from_host: %s\n", e.what());
+        return nullptr;
+    }
+}
+
 void wfref_scene_destroy(void* handle) {
     RefScene* r = static_cast<RefScene*>(handle);
     if (!r) return;

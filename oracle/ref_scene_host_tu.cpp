@@ -3,8 +3,8 @@
 // file-local light registration (addMeshTriangleLights, scene_host.cpp:77-106,
 // then addStaticTriangleLights, :60-75, in the order assembleCornellScene and
 // assembleGltfScene call them, :345-346, :413-414) can be applied to the
-// host-compiled reference's scenes.  The asset loaders are not part of the
-// traced path; they are stubbed.
+// host-compiled reference's scenes.  The asset loaders it calls are the
+// reference's own (obj_loader.cpp, gltf_loader.cpp), built beside it.
 #include "../src/scene/scene_host.cpp"
 
 #include <stdexcept>
@@ -14,6 +14,3 @@ void wfref_register_lights(HostScene& scene) {
     addStaticTriangleLights(scene);
 }
 
-ObjScene loadObjScene(const char*) { throw std::runtime_error("asset loaders are not built into the host reference"); }
-ObjMesh loadObjMesh(const char*) { throw std::runtime_error("asset loaders are not built into the host reference"); }
-GltfScene loadGltfScene(const char*) { throw std::runtime_error("asset loaders are not built into the host reference"); }

@@ -294,7 +294,7 @@ class PortScene:
         return fb, counts
 
 
-PRESET_KINDS = {"gltf": 0, "cornell": 1, "obj": 2}
+PRESET_KINDS = {"gltf": 0, "cornell": 1, "obj": 2, "demo": 3, "rtweek": 4}
 OBJECT_SOURCES = {"obj": 0, "gltf": 1, "procedural_prism": 2}
 LIGHT_PROFILES = {"standard": 0, "prism": 1, "crystal": 2}
 
@@ -308,7 +308,7 @@ class RefHostScene:
                  light_profile="standard", add_top_light=True, det=True):
         self.lib = ref_lib(det)
         t = np.asarray(translation, np.float32)
-        self.handle = self.lib.wfref_host_preset(PRESET_KINDS[kind], str(filename).encode(), float(scale),
+        self.handle = self.lib.wfref_host_preset(PRESET_KINDS[kind], str(filename or "").encode(), float(scale),
                                                  t.ctypes.data, OBJECT_SOURCES[object_source], int(neutral_room),
                                                  int(remove_backdrop), int(dielectric), int(material_override),
                                                  LIGHT_PROFILES[light_profile], int(add_top_light), 0)

@@ -87,7 +87,8 @@ extern "C" {
 // The reference's preset assembly.  kind 0: assembleGltfScene(filename,
 // scale, add_top_light) (the sponza preset); kind 1:
 // assembleCornellScene(CornellSceneOptions) (cornell, hurricane, prism,
-// crystal); kind 2: assembleObjScene(ObjSceneOptions) (deer).  NULL when the
+// crystal); kind 2: assembleObjScene(ObjSceneOptions) (deer); kind 3:
+// assembleDemoScene(); kind 4: assembleRtWeekScene(filename).  NULL when the
 // reference throws.
 void* wfref_host_preset(int kind, const char* filename, float scale, const float* translation, int object_source,
                         int neutral_room, int remove_backdrop, int dielectric, int material_override,
@@ -109,6 +110,10 @@ void* wfref_host_preset(int kind, const char* filename, float scale, const float
             o.objectMaterialOverride = material_override;
             o.lightProfile = CornellLightProfile(light_profile);
             handle->scene = assembleCornellScene(o);
+        } else if (kind == 3) {
+            handle->scene = assembleDemoScene();
+        } else if (kind == 4) {
+            handle->scene = assembleRtWeekScene(filename);
         } else if (kind == 2) {
             ObjSceneOptions o;
             o.filename = filename;

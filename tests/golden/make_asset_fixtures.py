@@ -274,6 +274,14 @@ def write_manifests():
                                  "object": {"source": "obj", "file": "mixed.obj", "scale": 0.9,
                                             "translation": [0.0, -0.4, 0.0], "dielectric": True},
                                  "room": {"neutral": True}, "lighting": {"profile": "crystal"}},
+        "fixture_demo.json": {"name": "fixture_demo", "preset": "demo"},
+        "fixture_rtweek.json": {"name": "fixture_rtweek", "preset": "rtweek",
+                                "object": {"source": "obj", "file": "mixed.obj"},
+                                "normal_maps": {"enabled": False}},
+        "fixture_prism.json": {"name": "fixture_prism", "preset": "prism",
+                               "object": {"source": "procedural_prism", "file": "__caustic_prism__", "scale": 1.0,
+                                          "translation": [0.0, 0.0, 0.0], "dielectric": True},
+                               "lighting": {"profile": "prism"}},
         "fixture_deer.json": {"name": "fixture_deer", "preset": "deer",
                               "object": {"source": "obj", "file": "mixed.obj", "scale": 1.5,
                                          "translation": [0.1, 0.2, 0.0]},

@@ -21,7 +21,7 @@ from wfpt import abi, assets
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "assets"
 REFERENCE_SCENES = Path(os.environ.get("WF_REFERENCE", "/root/reference")) / "assets" / "scenes"
-KIND = {"sponza": "gltf", "deer": "obj"}
+KIND = {"sponza": "gltf", "deer": "obj", "demo": "demo", "rtweek": "rtweek"}
 
 needs_oracle = pytest.mark.skipif(not oracle.available(det=True), reason="oracle/_ref/libwfref_det.so not built")
 
@@ -54,9 +54,17 @@ def compare(scene, ref, jpeg_tolerance=0):
     assert len(scene.meshes) == len(ref["meshes"])
     for i, (m, r) in enumerate(zip(scene.meshes, ref["meshes"])):
         same_bits(f"mesh[{i}]", m, r)
-        same_bits(f"mesh_attributes[{i}]", scene.mesh_attributes[i], ref["mesh_attributes"][i])
-    for name in ("instances", "materials", "material_textures", "spheres", "punctual"):
+        attrs = scene.mesh_attributes[i] if i < len(scene.mesh_attributes) else None
+        if attrs is None:  # no attributes: the reference's value-initialised fields
+            attrs = np.zeros(len(m), abi.TRIANGLE_ATTRIBUTES_DTYPE)
+        same_bits(f"mesh_attributes[{i}]", attrs, ref["mesh_attributes"][i])
+    same_bits("triangles", scene.triangles, ref["triangles"])
+    for name in ("instances", "materials", "spheres", "punctual"):
         same_bits(name, getattr(scene, name), ref[name])
+    textures = scene.material_textures
+    if textures is None:  # untextured: every binding empty
+        textures = assets._no_textures(len(scene.materials))
+    same_bits("material_textures", textures, ref["material_textures"])
     assert len(scene.textures) == len(ref["textures"])
     for i, (t, r) in enumerate(zip(scene.textures, ref["textures"])):
         assert t.shape == r.shape, f"texture {i}"

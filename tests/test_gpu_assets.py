@@ -16,7 +16,7 @@ from wfpt import abi, assets
 pytestmark = pytest.mark.gpu
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "assets"
-KIND = {"sponza": "gltf", "deer": "obj"}
+KIND = {"sponza": "gltf", "deer": "obj", "demo": "demo", "rtweek": "rtweek"}
 W, H = 64, 48
 
 

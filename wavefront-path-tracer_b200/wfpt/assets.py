@@ -685,6 +685,39 @@ def _scaled_instance(mesh, translation, scale):
     return r
 
 
+def _rotate_vector(v, axis, angle):
+    """rotateVector (include/scene/scene.cuh:65-70) with the float sine and
+    cosine of the float angle (correctly rounded)."""
+    unit = _normalize(_f3(axis))
+    c = F32(math.cos(float(angle)))
+    s = F32(math.sin(float(angle)))
+    v = _f3(v)
+    return (v * c + _cross(unit, v) * s) + unit * (_dot(unit, v) * (F32(1.0) - c))
+
+
+def _rotate_instance(r, axis, degrees):
+    """rotateTransform (include/scene/scene.cuh:76-95)."""
+    angle = F32(degrees) * (F32(3.14159265359) / F32(180.0))
+    old = r["world_to_local"][0].copy()
+    r["local_to_world"][0] = np.stack([_rotate_vector(r["local_to_world"][0][k], axis, angle) for k in range(3)])
+    inverse = [_rotate_vector(e, axis, -angle) for e in np.eye(3, dtype=F32)]
+    # transformBasis: bx * v.x + by * v.y + bz * v.z
+    r["world_to_local"][0] = np.stack([(old[0] * inv[0] + old[1] * inv[1]) + old[2] * inv[2] for inv in inverse])
+
+
+def _caustic_prism():
+    """makeCausticPrism (scene_host.cpp:26-43)."""
+    h = F32(1.25)
+    a0, b0, c0 = (-h, -0.82, -0.68), (-h, -0.82, 0.68), (-h, 0.38, 0.0)
+    a1, b1, c1 = (h, -0.82, -0.68), (h, -0.82, 0.68), (h, 0.38, 0.0)
+    faces = [(a0, a1, b1), (a0, b1, b0), (b0, b1, c1), (b0, c1, c0), (c0, c1, a1), (c0, a1, a0), (a0, c0, b0),
+             (a1, b1, c1)]
+    t = np.zeros(len(faces), abi.TRIANGLE_DTYPE)
+    for i, (p, q, r) in enumerate(faces):
+        t[i]["v0"], t[i]["v1"], t[i]["v2"] = _f3(p), _f3(q), _f3(r)
+    return t
+
+
 def _scale_instances(instances, scale, translation=None):
     """The instance scaling of assembleGltfScene / assembleCornellScene
     (scene_host.cpp:310-318, 366-374)."""
@@ -698,10 +731,14 @@ def _scale_instances(instances, scale, translation=None):
 
 
 def camera(kind, width, height):
-    """createDemoCamera / createCornellCamera (src/scene/camera.cu:3-28) in float."""
+    """createDemoCamera / createCornellCamera / createRtWeekCamera
+    (src/scene/camera.cu:3-42) in float."""
     if kind == "cornell":
         position, target, fov_deg = _f3([0.0, 1.2, 6.5]), _f3([0.0, 0.8, -0.6]), F32(42.0)
         world_up = _f3([0.0, 1.0, 0.0])
+    elif kind == "rtweek":  # createRtWeekCamera, camera.cu:30-42
+        position, target, fov_deg = _f3([13.0, 2.0, 3.0]), _f3([0.0, 0.8, 0.0]), F32(32.0)
+        world_up = None
     else:
         position, target, fov_deg = _f3([-10.0, 0.35, 0.8]), _f3([6.0, 3.2, 2.4]), F32(45.0)
         world_up = None
@@ -793,7 +830,7 @@ def _from_loaded(scene, loaded, material_offset=0, override=-1):
         tri = tri.copy()
         tri["material"] = np.uint32(override) if override >= 0 else tri["material"] + material_offset
         scene.meshes.append(tri)
-    scene.mesh_attributes = [a.copy() for a in loaded.mesh_attributes]
+    scene.mesh_attributes = [a.copy() if a is not None else None for a in loaded.mesh_attributes]
 
 
 def gltf_scene(path, scale=1.0, add_top_light=True):
@@ -832,18 +869,27 @@ def cornell_scene(config: PresetConfig):
         punctual = loaded.punctual.copy()
         if len(punctual):
             punctual["position"] = punctual["position"] * F32(config.object_scale) + _f3(config.object_translation)
-    elif config.object_source == "obj":
-        loaded = load_obj_scene(config.object_file)
-        instances = np.concatenate([_scaled_instance(i, config.object_translation, config.object_scale)
-                                    for i in range(len(loaded.meshes))])
-        if profile == "prism":
-            raise NotImplementedError("the prism light profile rotates the object (rotateTransform)")
-        punctual = np.zeros(0, abi.PUNCTUAL_DTYPE)
     else:
-        raise NotImplementedError("procedural prism objects")
+        if config.object_source == "obj":
+            loaded = load_obj_scene(config.object_file)
+        else:
+            loaded = LoadedScene(meshes=[_caustic_prism()], mesh_attributes=[None],
+                                 materials=np.array([material(abi.MAT_DIELECTRIC, (0.98, 0.99, 1.0), ior=1.52,
+                                                              dispersion=0.035)], abi.MATERIAL_DTYPE),
+                                 material_textures=_no_textures(1))
+        instances = []
+        for i in range(len(loaded.meshes)):
+            r = _scaled_instance(i, config.object_translation, config.object_scale)
+            if profile == "prism":
+                _rotate_instance(r, (0.0, 1.0, 0.0), -20.0)
+            instances.append(r)
+        instances = np.concatenate(instances)
+        punctual = np.zeros(0, abi.PUNCTUAL_DTYPE)
     object_materials = loaded.materials.copy()
     object_textures = loaded.material_textures.copy()
-    if config.dielectric:
+    # the procedural prism's own material is not an imported one: the
+    # dielectric conversion of imported materials leaves it alone
+    if config.dielectric and config.object_source != "procedural_prism":
         object_materials["type"] = abi.MAT_DIELECTRIC
         object_materials["albedo"] = 1.0
         object_materials["emission"] = 0.0
@@ -900,6 +946,78 @@ def obj_scene(config: PresetConfig):
     return s
 
 
+def demo_scene():
+    """assembleDemoScene (scene_host.cpp:116-163): a cube, a pyramid, a glass
+    sphere and a ground sphere under the sky."""
+    s = Scene()
+    s.spheres = np.array([((0.0, -100.5, 0.0), 100.0, 3, abi.ACCEL_DIRECT), ((1.35, 0.08, 0.0), 0.5, 2, abi.ACCEL_BVH)],
+                         abi.SPHERE_DTYPE)
+    c = [(-1.85, -0.42, -0.5), (-0.85, -0.42, -0.5), (-0.85, 0.58, -0.5), (-1.85, 0.58, -0.5),
+         (-1.85, -0.42, 0.5), (-0.85, -0.42, 0.5), (-0.85, 0.58, 0.5), (-1.85, 0.58, 0.5)]
+    cube = [(4, 5, 6), (4, 6, 7), (0, 2, 1), (0, 3, 2), (0, 4, 7), (0, 7, 3), (1, 2, 6), (1, 6, 5), (3, 7, 6),
+            (3, 6, 2), (0, 1, 5), (0, 5, 4)]
+    p = [(-0.183, -0.42, -0.683), (0.683, -0.42, -0.183), (0.183, -0.42, 0.683), (-0.683, -0.42, 0.183),
+         (0.0, 0.73, 0.0)]
+    pyramid = [(0, 1, 4), (1, 2, 4), (2, 3, 4), (3, 0, 4), (0, 2, 1), (0, 3, 2)]
+    tris = [(c[a], c[b], c[d], 0) for a, b, d in cube] + [(p[a], p[b], p[d], 1) for a, b, d in pyramid]
+    t = np.zeros(len(tris), abi.TRIANGLE_DTYPE)
+    for i, (v0, v1, v2, m) in enumerate(tris):
+        t[i]["v0"], t[i]["v1"], t[i]["v2"], t[i]["material"] = _f3(v0), _f3(v1), _f3(v2), m
+    s.triangles = t
+    s.materials = np.array([material(abi.MAT_DIFFUSE, (0.7, 0.2, 0.15)),
+                            material(abi.MAT_METAL, (0.85, 0.65, 0.25), roughness=0.08),
+                            material(abi.MAT_DIELECTRIC, (1.0, 1.0, 1.0), ior=1.5),
+                            material(abi.MAT_DIFFUSE, (0.75, 0.75, 0.75))], abi.MATERIAL_DTYPE)
+    return s
+
+
+def rtweek_scene(obj_path):
+    """assembleRtWeekScene (scene_host.cpp:165-240): the seeded small-sphere
+    field of Ray Tracing in One Weekend and three instances of an OBJ mesh
+    with material overrides, under the sky, with no area lights."""
+    from .scenes import SceneRng
+    loaded = load_obj_mesh(obj_path)
+    s = Scene()
+    D, M, G = abi.MAT_DIFFUSE, abi.MAT_METAL, abi.MAT_DIELECTRIC
+    s.materials = np.array([material(D, (0.50, 0.50, 0.50)), material(D, (0.72, 0.20, 0.12)),
+                            material(D, (0.16, 0.35, 0.72)), material(D, (0.22, 0.62, 0.28)),
+                            material(M, (0.82, 0.84, 0.88), roughness=0.08),
+                            material(M, (0.88, 0.60, 0.20), roughness=0.05),
+                            material(G, (1.0, 1.0, 1.0), ior=1.5), material(D, (0.80, 0.30, 0.30)),
+                            material(M, (0.80, 0.82, 0.90), roughness=0.05), material(G, (1.0, 1.0, 1.0), ior=1.5)],
+                           abi.MATERIAL_DTYPE)
+    spheres = [((0.0, -1000.0, 0.0), 1000.0, 0, abi.ACCEL_DIRECT)]
+    rng = SceneRng(0x4D595DF4)
+    for x in range(-11, 11):
+        for z in range(-11, 11):
+            choose = F32(rng.next())
+            # Vec3(x + random(), 0.2f, z + random()): the reference's compiler
+            # evaluates the constructor's arguments right to left, so z's
+            # draw comes first
+            cz = F32(z) + F32(rng.next())
+            cx = F32(x) + F32(rng.next())
+            if choose < F32(0.70):
+                color = F32(rng.next())
+                mat = 1 if color < F32(0.34) else (2 if color < F32(0.67) else 3)
+            elif choose < F32(0.85):
+                mat = 4 if F32(rng.next()) < F32(0.5) else 5
+            else:
+                mat = 6
+            spheres.append(((cx, F32(0.2), cz), 0.20, mat, abi.ACCEL_BVH))
+    s.spheres = np.array(spheres, abi.SPHERE_DTYPE)
+    mesh = loaded.meshes[0].copy()
+    mesh["material"] = 0
+    s.meshes = [mesh]
+    s.mesh_attributes = [loaded.mesh_attributes[0].copy()]  # the OBJ's textures are not kept
+    instances = []
+    for offset, mat in zip([(-4.0, -0.043, 1.0), (4.0, -0.043, 1.0), (0.0, -0.043, 1.0)], (7, 8, 9)):
+        r = _scaled_instance(0, offset, 0.0035)
+        r["material_override"] = mat
+        instances.append(r)
+    s.instances = np.concatenate(instances)
+    return s
+
+
 def preset_scene(manifest, width, height):
     """The preset a manifest names, as RenderDriver builds it
     (createSceneFromConfig + applySceneConfig, src/scene/scene_factory.cpp:
@@ -915,6 +1033,12 @@ def preset_scene(manifest, width, height):
     elif c.preset == "deer":
         s = obj_scene(c)
         cam = camera("demo", width, height)
+    elif c.preset == "demo":
+        s = demo_scene()
+        cam = camera("demo", width, height)
+    elif c.preset == "rtweek":
+        s = rtweek_scene(c.object_file)
+        cam = camera("rtweek", width, height)
     else:
         raise NotImplementedError(f"preset {c.preset} has no asset path")
     s.disable_normal_maps = not c.use_normal_maps

@@ -60,6 +60,15 @@ def ref_lib(det=False):
         lib.wfref_host_scene_texture.argtypes = [P, U32, P, P]
         lib.wfref_scene_from_host.restype = P
         lib.wfref_scene_from_host.argtypes = [P, I, C.c_float]
+        lib.wfref_dist_tasks.restype = C.c_uint64
+        lib.wfref_dist_tasks.argtypes = [U32, U32, U32, U32, U32, U32, C.c_uint64, P, C.c_uint64]
+        lib.wfref_dist_task_key.restype = C.c_uint64
+        lib.wfref_dist_task_key.argtypes = [C.c_uint64, U32, U32, U32]
+        lib.wfref_dist_checkpoint_write.restype = I
+        lib.wfref_dist_checkpoint_write.argtypes = [C.c_char_p, C.c_uint64, P, C.c_uint64, P, P, P, C.c_uint64,
+                                                    C.c_char_p, C.c_uint64]
+        lib.wfref_dist_checkpoint_read.restype = I
+        lib.wfref_dist_checkpoint_read.argtypes = [C.c_char_p, P, P, P, P, C.c_char_p, C.c_uint64]
         lib.wfref_dielectric_reflectance.restype = C.c_float
         lib.wfref_dielectric_reflectance.argtypes = [C.c_float, C.c_float]
         lib.wfref_checkpoint_roundtrip_read.restype = I
@@ -372,3 +381,48 @@ class RefHostScene:
         if not r.handle:
             raise RuntimeError("wfref_scene_from_host failed")
         return r
+
+
+def dist_tasks(width, height, tile_width, tile_height, spp, spp_per_task, fingerprint=0):
+    """The reference's createRenderTasks as (n, 7) uint32 rows: tile, sample
+    start, sample count, x, y, width, height."""
+    lib = ref_lib(True)
+    n = lib.wfref_dist_tasks(width, height, tile_width, tile_height, spp, spp_per_task, fingerprint, None, 0)
+    out = np.zeros((n, 7), np.uint32)
+    lib.wfref_dist_tasks(width, height, tile_width, tile_height, spp, spp_per_task, fingerprint, out.ctypes.data, n)
+    return out
+
+
+def dist_task_key(fingerprint, tile, sample_start, sample_count):
+    return int(ref_lib(True).wfref_dist_task_key(fingerprint, tile, sample_start, sample_count))
+
+
+def dist_checkpoint_write(path, fingerprint, job, sequence, radiance, counts, completed):
+    """writeDistributedCheckpoint; job = (width, height, tile width, tile
+    height, spp, spp per task).  Raises with the reference's message."""
+    job = np.asarray(job, np.uint32)
+    radiance = np.ascontiguousarray(radiance, np.float32)
+    counts = np.ascontiguousarray(counts, np.uint32)
+    completed = np.ascontiguousarray(completed, np.uint8)
+    error = C.create_string_buffer(256)
+    if ref_lib(True).wfref_dist_checkpoint_write(str(path).encode(), fingerprint, job.ctypes.data, sequence,
+                                                 radiance.ctypes.data, counts.ctypes.data, completed.ctypes.data,
+                                                 len(completed), error, 256):
+        raise ValueError(error.value.decode())
+
+
+def dist_checkpoint_read(path):
+    """readDistributedCheckpoint: (header (9 uint64), radiance, counts,
+    completed); raises with the reference's message."""
+    lib = ref_lib(True)
+    header = np.zeros(9, np.uint64)
+    error = C.create_string_buffer(256)
+    if lib.wfref_dist_checkpoint_read(str(path).encode(), header.ctypes.data, None, None, None, error, 256):
+        raise ValueError(error.value.decode())
+    pixels = int(header[1]) * int(header[2])
+    radiance = np.zeros((pixels, 3), np.float32)
+    counts = np.zeros(pixels, np.uint32)
+    completed = np.zeros(int(header[8]), np.uint8)
+    lib.wfref_dist_checkpoint_read(str(path).encode(), header.ctypes.data, radiance.ctypes.data, counts.ctypes.data,
+                                   completed.ctypes.data, error, 256)
+    return header, radiance, counts, completed

@@ -604,18 +604,26 @@ def main():
     # Kernel-level roofline from one profiled pass (event-timed eager launches).
     profile = renderer.profile_sample()
     kernels = {k: v for k, v in profile.items() if isinstance(v, dict) and v["launches"]}
-    dominant = max(("trace", "shadow"), key=lambda k: kernels.get(k, {"ms": 0})["ms"])
     total_ms = sum(v["ms"] for v in kernels.values())
-    launches = kernels[dominant]["launches"]
-    avg_ms = kernels[dominant]["ms"] / launches
-    bytes_per_launch = algorithmic_bytes(profile, dominant) / launches
-    peak, peak_kind = measured_peak()
-    achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "kernel": f"k_{dominant}", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": ncu_traffic(f"k_{dominant}", args.workload),
-                "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
-                "kernel_share": {k: v["ms"] / total_ms for k, v in kernels.items()}}
+    if "trace" in kernels or "shadow" in kernels:
+        dominant = max(("trace", "shadow"), key=lambda k: kernels.get(k, {"ms": 0})["ms"])
+        launches = kernels[dominant]["launches"]
+        avg_ms = kernels[dominant]["ms"] / launches
+        bytes_per_launch = algorithmic_bytes(profile, dominant) / launches
+        peak, peak_kind = measured_peak()
+        achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": f"k_{dominant}", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_kind,
+                    "traffic": ncu_traffic(f"k_{dominant}", args.workload),
+                    "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
+                    "kernel_share": {k: v["ms"] / total_ms for k, v in kernels.items()}}
+    else:
+        # the persistent schedule fuses every stage into one kernel that
+        # keeps no traversal tallies: no per-kernel roofline
+        roofline = {"bound": "hbm", "kernel": "k_persistent", "achieved": None, "peak": measured_peak()[0],
+                    "unit": "GB/s", "frac": None, "traffic": None,
+                    "note": "fused persistent kernel; traversal tallies are kept only by the wavefront kernels",
+                    "kernel_share": {k: v["ms"] / total_ms for k, v in kernels.items()}}
 
     # Multi-GPU merge: one NCCL reduce of the framebuffers to rank 0.
     if world > 1:

@@ -573,6 +573,9 @@ constexpr int kUnconditional = -1;
 // radiance terms (each optionally conditional on one test being unoccluded)
 // in the order the reference adds them, and the test (if any) whose
 // unoccluded result ends the path (a terminal branch that escaped).
+// Tally: the traversal variant of the shadow rays (Opaque<NoTally> when no
+// material of the scene is alpha-textured).
+template <typename Tally = NoTally>
 struct InlineSink {
     static constexpr bool kDeferredGather = false;  // caustic gathers run inline
     const DeviceScene* scene;
@@ -582,7 +585,7 @@ struct InlineSink {
     // Returns a handle: 1 = occluded, 0 = visible.
     WF_DEV int request(V3 o, V3 d, float t_max) {
         ++requests;
-        NoTally tally;
+        Tally tally;
         return trace_any(*scene, o, d, t_max, tally) ? 1 : 0;
     }
     WF_DEV bool may_be_visible(int handle) const { return handle == kUnconditional || handle == 0; }

@@ -362,7 +362,8 @@ typedef struct wf_render_config {
     uint32_t tile_width;       /* 0 = full frame; bounds queue memory */
     uint32_t tile_height;
     uint32_t block_size;       /* 0 = tuned default */
-    uint32_t persistent_blocks;/* 0 = SMs x resident blocks */
+    uint32_t persistent_blocks;/* 0 = the resident grid, trimmed for small tiles to
+                                  max(4 x SMs, paths / 128) */
     uint32_t chunk;            /* persistent work chunk in paths, 0 = default */
     uint32_t debug;            /* WF_DEBUG_* */
     /* photon caustics, src/renderer/photon_mapping.cu + render_driver.cu:180-234 */

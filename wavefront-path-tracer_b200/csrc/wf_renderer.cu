@@ -1070,6 +1070,18 @@ wf_status capture_stream_graph(wf_renderer* r) {
     return WF_OK;
 }
 
+// Grid of one persistent launch over `paths` paths: the configured grid, or
+// by default the resident grid trimmed for small tiles to one CTA per 128
+// paths, but never below 4 CTAs per SM.  Every CTA joins each bounce's grid
+// barrier, so on a small tile a full resident grid costs more in barriers
+// than its idle warps give (256x256 Cornell box: 592 CTAs 128.7 Mpaths/s,
+// 1184 CTAs 105.4); large tiles keep the whole resident grid.
+uint32_t persistent_grid(uint32_t configured, uint32_t resident, uint32_t sm_count, uint64_t paths) {
+    if (configured) return std::max(1u, std::min(configured, resident));
+    uint64_t wanted = std::max<uint64_t>(4ull * sm_count, (paths + 127) / 128);
+    return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(wanted, resident)));
+}
+
 wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
     WF_CUDA(cudaMemcpyAsync(r->tile, &tile, sizeof(TileDev), cudaMemcpyHostToDevice, r->stream));
     r->last_tile_width = tile.width;
@@ -1091,7 +1103,9 @@ wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
     float* fb = r->framebuffer;
     uint32_t chunk = r->chunk;
     void* args[] = {&s, &rp, &tp, &c, &ps, &q0, &q1, &cap, &fb, &chunk};
-    WF_CUDA(cudaLaunchCooperativeKernel(persistent_kernel(r->opaque, r->textured), dim3(r->persistent_blocks),
+    uint32_t blocks = persistent_grid(r->config.persistent_blocks, r->persistent_blocks, r->sm_count,
+                                      std::min<uint64_t>(uint64_t(tile.width) * tile.height, r->capacity));
+    WF_CUDA(cudaLaunchCooperativeKernel(persistent_kernel(r->opaque, r->textured), dim3(blocks),
                                         dim3(r->persistent_block_size), args, 0, r->stream));
     k_advance<<<1, 1, 0, r->stream>>>(r->counters, r->tile);
     WF_CUDA(cudaGetLastError());
@@ -1227,8 +1241,7 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
                                                               int(r->persistent_block_size), 0));
         if (per_sm <= 0) return fail(WF_ERR_UNSUPPORTED, "the persistent kernel cannot be resident");
         uint32_t resident = uint32_t(per_sm) * uint32_t(r->sm_count);
-        uint32_t wanted = c.persistent_blocks ? c.persistent_blocks : resident;
-        r->persistent_blocks = std::max(1u, std::min(wanted, resident));
+        r->persistent_blocks = resident;  // the largest grid; persistent_grid picks each launch's
         r->chunk = c.chunk ? std::max(1u, c.chunk / 32) : 1u;
     }
     if (c.caustics && photon_source) {
@@ -1479,7 +1492,12 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
             cudaError_t launch_error = cudaSuccess;
             if (wf_status e = timed(WF_KERNEL_PERSISTENT, [&] {
                     launch_error = cudaLaunchCooperativeKernel(persistent_kernel(r->opaque, r->textured),
-                                                               dim3(r->persistent_blocks),
+                                                               dim3(persistent_grid(
+                                                                   r->config.persistent_blocks, r->persistent_blocks,
+                                                                   r->sm_count,
+                                                                   std::min<uint64_t>(uint64_t(r->last_tile_width) *
+                                                                                          r->last_tile_height,
+                                                                                      r->capacity))),
                                                                dim3(r->persistent_block_size), args, 0, st);
                 }))
                 return e;
@@ -1777,7 +1795,9 @@ extern "C" wf_status wf_render_tile_static(const wf_scene* scene, const wf_camer
     rp.camera.aspect_ratio = camera->aspect_ratio;
     rp.camera.tan_half_fov = wfm::tanf(camera->vertical_fov * 0.5f);
     rp.photons = PhotonGridView{};
-    uint32_t blocks = c.persistent_blocks ? std::max(1u, std::min(c.persistent_blocks, resident)) : resident;
+    int sms = 0;
+    WF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    uint32_t blocks = persistent_grid(c.persistent_blocks, resident, uint32_t(sms), uint64_t(width) * height);
     uint32_t chunk = c.chunk ? std::max(1u, c.chunk / 32) : 1u;
 
     Counters* counters = reinterpret_cast<Counters*>(base + kStaticCountersOffset);

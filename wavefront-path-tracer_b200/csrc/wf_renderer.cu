@@ -87,11 +87,10 @@ __global__ void k_raygen_stream(RenderParams rp, const TileDev* tile_ptr, Counte
 // warp takes 32 consecutive queue entries and every lane runs its ray to the
 // end (camera rays: neighbouring pixels visit the same nodes in lockstep).
 // The per-ray visit order and arithmetic are the same either way.
-// At most 72 registers (7 CTAs of 128 per SM): 8 bytes of spill cost less
-// than the warps a 79-register allocation (6 CTAs) leaves out; a 64-register
-// cap spills far more.  __maxnreg__ keeps every block size launchable.
-template <typename Tally, bool kLanes = true>
-__global__ void __maxnreg__(72) k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
+// The closest-hit stage of one bounce; the kernels below differ only in
+// their register bounds.
+template <typename Tally, bool kLanes>
+WF_DEV void trace_stage(const DeviceScene& s, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
                         uint32_t* hit_inst, Counters* c, uint32_t bounce, TallyTotals* totals, uint32_t refill_at) {
     count_launch(c);
     uint32_t n = *count;
@@ -152,6 +151,29 @@ __global__ void __maxnreg__(72) k_trace(DeviceScene s, PathSoA ps, const uint32_
         }
     }
     if constexpr (Tally::kCounts) flush_tally(tally, totals);
+}
+
+// Lane-refill bounces: at most 72 registers (7 CTAs of 128 per SM): 8 bytes
+// of spill cost less than the warps a 79-register allocation (6 CTAs) leaves
+// out; a 64-register cap spills far more.  __maxnreg__ keeps every block
+// size launchable.
+template <typename Tally, bool kLanes = true>
+__global__ void __maxnreg__(72) k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const uint32_t* count,
+                                        float4* hit_a, uint32_t* hit_inst, Counters* c, uint32_t bounce,
+                                        TallyTotals* totals, uint32_t refill_at) {
+    trace_stage<Tally, kLanes>(s, ps, queue, count, hit_a, hit_inst, c, bounce, totals, refill_at);
+}
+
+// Camera rays (one traversal per thread, coherent): bounded to 8 CTAs of 128
+// per SM (64 registers).  Unlike the lane-refill loop, this traversal gains
+// more from the extra warps than its spills cost: bounce 0 of the 1080p large
+// mesh 2.07 -> 1.98 ms, the frame +0.6 %.
+template <typename Tally>
+__global__ void __launch_bounds__(128, 8) k_trace_camera(DeviceScene s, PathSoA ps, const uint32_t* queue,
+                                                         const uint32_t* count, float4* hit_a, uint32_t* hit_inst,
+                                                         Counters* c, uint32_t bounce, TallyTotals* totals,
+                                                         uint32_t refill_at) {
+    trace_stage<Tally, false>(s, ps, queue, count, hit_a, hit_inst, c, bounce, totals, refill_at);
 }
 
 // Shading categories: warps of k_shade take entries of one category at a
@@ -929,10 +951,16 @@ wf_status build_photon_map(wf_renderer* r) {
 // material of the scene is alpha-textured.
 template <typename Tally, bool kLanes, typename... A>
 void launch_trace(const wf_renderer* r, uint32_t grid_size, uint32_t block, cudaStream_t st, A... args) {
-    if (r->opaque)
+    if constexpr (!kLanes) {
+        if (r->opaque)
+            k_trace_camera<Opaque<Tally>><<<grid_size, block, 0, st>>>(args...);
+        else
+            k_trace_camera<Tally><<<grid_size, block, 0, st>>>(args...);
+    } else if (r->opaque) {
         k_trace<Opaque<Tally>, kLanes><<<grid_size, block, 0, st>>>(args...);
-    else
+    } else {
         k_trace<Tally, kLanes><<<grid_size, block, 0, st>>>(args...);
+    }
 }
 // k_shade with the texture code only for scenes that have textured materials.
 template <typename... A>
@@ -1224,8 +1252,8 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
         }
         WF_CUDA(r->opaque ? resident_grid(rr, 0, k_trace<Opaque<NoTally>>, r->block_trace)
                           : resident_grid(rr, 0, k_trace<NoTally>, r->block_trace));
-        WF_CUDA(r->opaque ? resident_grid(rr, 5, k_trace<Opaque<NoTally>, false>, r->block_trace)
-                          : resident_grid(rr, 5, k_trace<NoTally, false>, r->block_trace));
+        WF_CUDA(r->opaque ? resident_grid(rr, 5, k_trace_camera<Opaque<NoTally>>, r->block_trace)
+                          : resident_grid(rr, 5, k_trace_camera<NoTally>, r->block_trace));
         WF_CUDA(r->textured ? resident_grid(rr, 1, k_shade<true>, r->block_shade)
                             : resident_grid(rr, 1, k_shade<false>, r->block_shade));
         WF_CUDA(r->opaque ? resident_grid(rr, 2, k_shadow<Opaque<NoTally>>, r->block_trace)

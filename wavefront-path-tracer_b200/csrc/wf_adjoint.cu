@@ -134,7 +134,9 @@ WF_DEV void flush_vertex(uint32_t key, float4 value, float4* warp_buffer, const 
 // delta * dU/dtheta to the gradients and returns the replayed radiance.  In
 // adjoint mode all 32 lanes of the warp call it together (`alive` false for
 // lanes without a path) and run the same number of vertex steps.
-template <bool kAdjoint>
+// Tally: the traversal variant (Opaque<NoTally> when no material of the scene
+// is alpha-textured, which drops the per-candidate alpha test).
+template <bool kAdjoint, typename Tally>
 WF_DEV V3 diff_path(const DeviceScene& s, const DiffParams& P, const DiffSettings& cfg, uint32_t px, uint32_t py,
                     uint32_t sample, bool alive, V3 total, V3 delta, const DiffGrads& G, float4* warp_buffer,
                     uint32_t* error) {
@@ -149,7 +151,7 @@ WF_DEV V3 diff_path(const DeviceScene& s, const DiffParams& P, const DiffSetting
     }
     V3 beta{1.0f, 1.0f, 1.0f};
     V3 sum{0.0f, 0.0f, 0.0f};  // terms so far, at emission scale 1
-    NoTally tally;
+    Tally tally;
     for (uint32_t depth = 0; depth < cfg.max_depth; ++depth) {
         if (!kAdjoint && !alive) break;
         uint32_t key = kInvalid;
@@ -241,15 +243,22 @@ WF_DEV V3 diff_path(const DeviceScene& s, const DiffParams& P, const DiffSetting
     return sum;
 }
 
-__global__ void k_diff_forward(const __grid_constant__ DeviceScene s, DiffParams P, DiffSettings cfg, float* image,
-                               uint32_t* error) {
+// Both kernels trace one path per thread; bounded to 8 CTAs of 128 per SM
+// (64 registers) they keep enough warps resident to hide traversal latency.
+// Inverse-rendering config (512x512, 32 spp), with the opaque traversal:
+// forward 58.9 -> 42.0 ms, adjoint 182 -> 124.5 ms against the unbounded
+// kernels (138 and 168 registers, 3 CTAs per SM).
+template <typename Tally>
+__global__ void __launch_bounds__(128, 8) k_diff_forward(const __grid_constant__ DeviceScene s, DiffParams P,
+                                                         DiffSettings cfg, float* image, uint32_t* error) {
     uint32_t n = cfg.w * cfg.h;
     DiffGrads none{};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t px = cfg.x + i % cfg.w, py = cfg.y + i / cfg.w;
         V3 acc{0.0f, 0.0f, 0.0f};
         for (uint32_t k = 0; k < cfg.spp; ++k)
-            acc += diff_path<false>(s, P, cfg, px, py, cfg.sample_start + k, true, V3{}, V3{}, none, nullptr, error);
+            acc += diff_path<false, Tally>(s, P, cfg, px, py, cfg.sample_start + k, true, V3{}, V3{}, none, nullptr,
+                                           error);
         float scale = P.emission_scale / float(cfg.spp);
         float* out = image + 3 * (size_t(py) * cfg.width + px);
         out[0] = acc.x * scale;
@@ -262,9 +271,10 @@ __global__ void k_diff_forward(const __grid_constant__ DeviceScene s, DiffParams
 // Each warp takes up to 32 samples of one pixel, so the lanes of a warp
 // mostly hit the same triangles and their gradients merge before the
 // atomics (flush_vertex).
-__global__ void __launch_bounds__(128) k_diff_backward(const __grid_constant__ DeviceScene s, DiffParams P,
-                                                       DiffSettings cfg, const float* d_image, DiffGrads G,
-                                                       uint32_t* error) {
+template <typename Tally>
+__global__ void __launch_bounds__(128, 8) k_diff_backward(const __grid_constant__ DeviceScene s, DiffParams P,
+                                                          DiffSettings cfg, const float* d_image, DiffGrads G,
+                                                          uint32_t* error) {
     __shared__ float4 buffers[4][32];
     float4* warp_buffer = buffers[threadIdx.x >> 5];
     uint32_t lane = threadIdx.x & 31;
@@ -286,8 +296,8 @@ __global__ void __launch_bounds__(128) k_diff_backward(const __grid_constant__ D
         // the image is scale/spp * sum U: dLoss/dU = dLoss/dImage * scale / spp
         V3 delta = grad_pixel * (P.emission_scale / float(cfg.spp));
         V3 total{0.0f, 0.0f, 0.0f};
-        if (alive) total = diff_path<false>(s, P, cfg, px, py, sample, true, V3{}, V3{}, none, nullptr, error);
-        diff_path<true>(s, P, cfg, px, py, sample, alive, total, delta, G, warp_buffer, error);
+        if (alive) total = diff_path<false, Tally>(s, P, cfg, px, py, sample, true, V3{}, V3{}, none, nullptr, error);
+        diff_path<true, Tally>(s, P, cfg, px, py, sample, alive, total, delta, G, warp_buffer, error);
         if (alive) d_scale += double(dot(grad_pixel, total)) / double(cfg.spp);
     }
     for (int off = 16; off > 0; off >>= 1) d_scale += __shfl_down_sync(0xffffffffu, d_scale, off);
@@ -359,7 +369,10 @@ extern "C" wf_status wf_diff_forward(const wf_scene* scene, const wf_camera* cam
     cudaError_t ce = cudaMemsetAsync(error, 0, sizeof(uint32_t), st);
     if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemsetAsync");
     DiffParams P{albedo, roughness, emission_scale};
-    k_diff_forward<<<diff_grid(cfg.w * cfg.h), 128, 0, st>>>(scene->view, P, cfg, image, error);
+    if (scene->alpha_textures)
+        k_diff_forward<NoTally><<<diff_grid(cfg.w * cfg.h), 128, 0, st>>>(scene->view, P, cfg, image, error);
+    else
+        k_diff_forward<Opaque<NoTally>><<<diff_grid(cfg.w * cfg.h), 128, 0, st>>>(scene->view, P, cfg, image, error);
     ce = cudaGetLastError();
     if (ce != cudaSuccess) return cuda_fail(ce, "k_diff_forward");
     return diff_finish(error, st);
@@ -380,8 +393,11 @@ extern "C" wf_status wf_diff_backward(const wf_scene* scene, const wf_camera* ca
     DiffParams P{albedo, roughness, emission_scale};
     DiffGrads G{d_albedo, d_roughness, d_emission_scale};
     uint32_t items = cfg.w * cfg.h * ((cfg.spp + 31) / 32);  // one warp each
-    k_diff_backward<<<std::max(1u, std::min((items + 3) / 4, 148u * 16u)), 128, 0, st>>>(scene->view, P, cfg, d_image,
-                                                                                          G, error);
+    uint32_t blocks = std::max(1u, std::min((items + 3) / 4, 148u * 16u));
+    if (scene->alpha_textures)
+        k_diff_backward<NoTally><<<blocks, 128, 0, st>>>(scene->view, P, cfg, d_image, G, error);
+    else
+        k_diff_backward<Opaque<NoTally>><<<blocks, 128, 0, st>>>(scene->view, P, cfg, d_image, G, error);
     ce = cudaGetLastError();
     if (ce != cudaSuccess) return cuda_fail(ce, "k_diff_backward");
     return diff_finish(error, st);

@@ -596,7 +596,11 @@ const void* persistent_kernel(bool opaque, bool textured) {
 }
 
 // ---------------------------------------------------------------- batch API
-__global__ void k_trace_batch(DeviceScene s, const wf_ray* rays, uint32_t count, wf_hit* hits) {
+// One closest-hit traversal per thread, bounded to 8 CTAs of 128 per SM (64
+// registers; 68 unbounded): 4 M random rays against the 1080p large mesh,
+// 365 -> 388 Mrays/s.  k_any_batch already fits 8 CTAs (62 registers).
+__global__ void __launch_bounds__(128, 8) k_trace_batch(DeviceScene s, const wf_ray* rays, uint32_t count,
+                                                        wf_hit* hits) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     V3 o{rays[i].origin[0], rays[i].origin[1], rays[i].origin[2]};

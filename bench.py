@@ -33,6 +33,7 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "wavefront-path-tracer_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))  # the CPU baseline and the reference arms only
 
 WORKLOADS = {
     # name: (scene kwargs, render kwargs)
@@ -71,22 +72,22 @@ def make_scene(name):
     return scene, cam, kw["width"], kw["height"], dict(rkw)
 
 
-def reference_cuda_comparison(workload):
-    """The reference's CUDA renderer (oracle/_ref/libwfref_cuda.so) and this
-    renderer timed the same way on the same tasks, in a child process
-    (oracle/ref_cuda_bench.py; caustics off on both sides)."""
+def reference_cuda_comparison(workload, steps=5):
+    """The reference's own CUDA renderer built for sm_100a
+    (oracle/_ref/libwfref_cuda.so), in its graph and persistent schedules,
+    and this renderer, timed the same way on the same whole-frame tasks in a
+    child process after the timed region (oracle/ref_cuda_bench.py).  Both
+    sides render the workload's caustics, each from its own photon map built
+    with grid bounds taken from the stored photons.  A baseline beside the
+    line, not part of `value`."""
     script = ROOT / "oracle" / "ref_cuda_bench.py"
     if not (ROOT / "oracle" / "_ref" / "libwfref_cuda.so").exists():
         return {"unavailable": "reference CUDA build absent (make -C oracle cuda)"}
-    out = {}
-    for mode in ("graph", "persistent"):
-        run = subprocess.run([sys.executable, str(script), "--workload", workload, "--mode", mode, "--steps", "5"],
-                             capture_output=True, text=True, timeout=1200, cwd=ROOT)
-        if run.returncode != 0:
-            out[mode] = {"failed": (run.stdout + run.stderr)[-300:]}
-            continue
-        out[mode] = json.loads(run.stdout.strip().splitlines()[-1])
-    return out
+    run = subprocess.run([sys.executable, str(script), "--workload", workload, "--mode", "graph,persistent",
+                          "--steps", str(steps)], capture_output=True, text=True, timeout=1200, cwd=ROOT)
+    if run.returncode != 0:
+        return {"failed": (run.stdout + run.stderr)[-400:]}
+    return json.loads(run.stdout.strip().splitlines()[-1])
 
 
 def measured_peak():
@@ -162,8 +163,8 @@ def ncu_traffic(kernel, workload):
 def cpu_reference_rate(ref, cam, width, height, render_kwargs, seconds_target=15.0, threads=0):
     """Mpaths/s of the host-compiled reference (an oracle.RefScene) on a band
     of rows at 1 spp, sized to about `seconds_target` seconds."""
-    import wfpt
-    cfg = wfpt.render_config(width, height, **render_kwargs)
+    import oracle
+    cfg = oracle.reference_config(width, height, **render_kwargs)
     cores = threads or os.cpu_count() or 1
     # One untimed row first: builds the reference's photon map once (it is
     # built in RenderDriver::prepare, outside the trace timing).
@@ -222,7 +223,6 @@ def time_frame_guides(dev_scene, cam, width, height, launches=10):
 
 
 def reference_scene(scene):
-    sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
     return oracle.RefScene(scene)
 
@@ -453,10 +453,6 @@ def run_batch(args):
     for r in renderers:
         r.close()
     batch.close()
-    reference_cuda = None
-    if rank == 0 and world == 1 and args.reference_cuda:
-        reference_cuda = reference_cuda_comparison(args.workload)
-
     if rank == 0:
         line = {
             "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
@@ -504,9 +500,9 @@ def main():
                     help="graph mode: 1 = one wavefront, 2 = two on two streams (default)")
     ap.add_argument("--bvh-builder", default="host", choices=["host", "gpu"],
                     help="BVH2 builder of the scene: host binned SAH (default) or GPU PLOC")
-    ap.add_argument("--reference-cuda", action="store_true",
-                    help="also time the reference's own CUDA renderer built for sm_100a (make -C oracle cuda) "
-                         "beside this one, both through their task calls, and add it as `reference_cuda`")
+    ap.add_argument("--no-reference-cuda", dest="reference_cuda", action="store_false",
+                    help="skip timing the reference's own CUDA renderer built for sm_100a (make -C oracle cuda) "
+                         "beside this one after the timed region (the `reference_cuda` object of the line)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -40,6 +40,13 @@ const char* wf_last_error(void);
 /* Library version string ("wavefront-b200 <major>.<minor>"). */
 const char* wf_version(void);
 
+/* Testing hook (no counterpart in the reference, which exits on a failed
+ * cudaMalloc): the library's next `after` device allocations succeed and the
+ * one after them fails with cudaErrorMemoryAllocation, once; the entry point
+ * that made it frees what it had allocated and returns WF_ERR_OOM.  A
+ * negative value disarms the hook.  Process-wide. */
+void wf_test_fail_allocation(int64_t after);
+
 /* ------------------------------------------------------------------ scene */
 /* MaterialType, include/scene/material.cuh:22-28 */
 enum { WF_MAT_DIFFUSE = 0, WF_MAT_METAL = 1, WF_MAT_DIELECTRIC = 2,
@@ -384,6 +391,12 @@ typedef struct wf_render_config {
                                   rendering its own rows of every tile, so the long last bounces of one
                                   overlap the other's work; 1 = one wavefront.  Each pixel stays with one
                                   wavefront, so the sums are the same either way. */
+    uint32_t shadow_queue_capacity; /* graph and streaming modes: shadow-ray requests one bounce can
+                                  queue; 0 = (5 + directional lights) x queue slots, which no bounce
+                                  can exceed.  Requests beyond a smaller capacity are dropped (their
+                                  terms count as unoccluded) and wf_synchronize reports
+                                  WF_ERR_CAPACITY, as the reference's bounded appendWarpCompacted
+                                  drops items beyond a queue's capacity (queue_compaction.cuh:8-29). */
 } wf_render_config;
 
 /* Defaults of RenderConfig (config.hpp:11-41) at the given resolution. */
@@ -426,7 +439,23 @@ wf_status wf_framebuffer_download(wf_renderer* renderer, uint32_t x, uint32_t y,
                                   uint32_t width, uint32_t height, float* rgb);
 /* Device address of the width*height*3 float framebuffer. */
 wf_status wf_framebuffer_device(wf_renderer* renderer, float** rgb);
+/* Waits for the renderer's work and reports the errors its kernels recorded:
+ * WF_ERR_TIMEOUT when a bounded wait gave up (a persistent-kernel grid
+ * barrier, or the streaming loop's iteration bound), WF_ERR_CAPACITY when a
+ * queue overflowed.  The reference exits the process on device errors
+ * (render_driver.cu:18-27); here the flags are cleared once reported, so the
+ * renderer stays usable and the next call renders correctly. */
 wf_status wf_synchronize(wf_renderer* renderer);
+
+/* Bounds of the renderer's device-side waits (no counterpart in the
+ * reference).  barrier_cycles: clock cycles a persistent-kernel grid barrier
+ * waits for the other blocks before it gives up (0 = 2^31).
+ * loop_iterations: passes of the streaming schedule's device-side loop per
+ * launch (0 = the bound samples x max_depth / 2 + 1 that no correct render
+ * reaches).  Smaller values let a watchdog (or a test) make the waits run
+ * out; the render then reports WF_ERR_TIMEOUT from wf_synchronize.
+ * Stream-ordered: applies to work queued after the call. */
+wf_status wf_renderer_set_watchdog(wf_renderer* renderer, uint64_t barrier_cycles, uint32_t loop_iterations);
 
 /* Per-bounce ray-queue sizes of the most recent sample of the most recent
  * tile (the --profile-queues record, renderer.cu:89-90).  Requires
@@ -457,7 +486,9 @@ wf_status wf_render_stats_get(wf_renderer* renderer, wf_render_stats* stats, uin
  * WF_ERR_CAPACITY and configs with caustics return WF_ERR_UNSUPPORTED.
  * The first call on each device looks up the array's device address and the
  * kernel's resident grid (no allocation), so make that first call before any
- * stream capture.  Every call shares the one array (it is reset at the start
+ * stream capture; a device whose context was re-created (cudaDeviceReset)
+ * gets the same set-up again on its next call.  Every call shares the one
+ * array (it is reset at the start
  * of each call): calls whose GPU work overlaps, from several host threads or
  * streams, race and give wrong images.  The call returns after the work on
  * `stream` (cudaStream_t, may be NULL) has finished. */

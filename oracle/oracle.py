@@ -42,6 +42,8 @@ def ref_lib(det=False):
         lib.wfref_occluded.argtypes = [P, P, P, U32, P, I]
         lib.wfref_photons.restype = I
         lib.wfref_photons.argtypes = [P, P, P, P, P, I]
+        lib.wfref_path_rays.restype = U32
+        lib.wfref_path_rays.argtypes = [P, P, P, U32, U32, U32, U32, U32, U32, P, U32, P, I]
         lib.wfref_render.restype = I
         lib.wfref_render.argtypes = [P, P, P, U32, U32, U32, U32, U32, U32, P, P, P, I, I]
         lib.wfref_frame_guides.restype = I
@@ -77,6 +79,34 @@ def ref_lib(det=False):
         lib.wfref_checkpoint_write.argtypes = [C.c_char_p, U32, U32, C.c_uint64, P, U32]
         _libs[key] = lib
     return _libs[key]
+
+
+def reference_config(width, height, **fields):
+    """A wf_render_config holding the reference's RenderConfig defaults
+    (include/config.hpp:11-41) at the given size, made without loading the
+    B200 library: the CPU reference arm of bench.py runs only the
+    reference's code.  tests/test_oracle_pins.py checks it field by field
+    against wf_render_config_default."""
+    from wfpt import abi
+    cfg = abi.RenderConfig()
+    cfg.width, cfg.height = width, height
+    cfg.max_depth, cfg.rr_start_depth = 32, 12
+    cfg.mode, cfg.rng = abi.MODE_GRAPH, abi.RNG_XORSHIFT32
+    cfg.indirect_clamp = 10.0
+    cfg.caustic_gather = 1
+    cfg.photon_count, cfg.photon_max_depth = 1048576, 8
+    cfg.gather_radius = 0.06
+    cfg.photon_grid_min[:] = [-2.5, -1.0, -2.5]
+    cfg.photon_grid_max[:] = [2.5, 3.0, 2.5]
+    cfg.photon_grid_resolution = 64
+    cfg.photon_seed = 0x13579BDF
+    cfg.profile_queues = 1
+    for k, v in fields.items():
+        if k in ("photon_grid_min", "photon_grid_max"):
+            getattr(cfg, k)[:] = [float(x) for x in v]
+        else:
+            setattr(cfg, k, v)
+    return cfg
 
 
 class RefScene:
@@ -122,6 +152,23 @@ class RefScene:
         hits = np.zeros(len(rays), abi.HIT_DTYPE)
         self.lib.wfref_trace(self.handle, rays.ctypes.data, len(rays), hits.ctypes.data, threads)
         return hits
+
+    def path_rays(self, camera, config, tile=None, sample=0, bounces=2, threads=0):
+        """The reference's ray queues of one sample of a tile: the camera
+        rays, then the continuation rays of each following bounce, in queue
+        order.  Returns (rays as RAY_DTYPE, per-bounce counts)."""
+        from wfpt import abi
+        from wfpt.native import camera_struct
+        x, y, w, h = tile if tile is not None else (0, 0, config.width, config.height)
+        cam = camera_struct(camera)
+        cap = w * h * bounces
+        rays = np.zeros(cap, abi.RAY_DTYPE)
+        counts = np.zeros(bounces, np.uint32)
+        n = self.lib.wfref_path_rays(self.handle, C.addressof(cam), C.addressof(config), x, y, w, h, sample,
+                                     bounces, rays.ctypes.data, cap, counts.ctypes.data, threads)
+        if n == 0xFFFFFFFF:
+            raise RuntimeError("wfref_path_rays failed")
+        return rays[:n], counts
 
     def occluded(self, rays, max_distance, threads=0):
         from wfpt import abi

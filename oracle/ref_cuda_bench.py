@@ -6,15 +6,17 @@ times it beside the B200 renderer on the same seeded scene, camera, depth,
 RNG strategy and absolute sample ranges.  Both sides are timed the same way:
 the wall time of one whole-frame task, which is the reference's
 RenderTaskRenderer::render (clear, sample launches, synchronise, download)
-against this renderer's wf_render + wf_framebuffer_download.  Caustics are
-off on both sides: the reference builds a photon map only for its Cornell
-family of presets, with fixed Cornell grid bounds.
+against this renderer's wf_render + wf_framebuffer_download.  With caustics
+(the large mesh's 2M photons), the reference builds its photon map with its
+own kernels (emitPhotons / tracePhotons / buildPhotonGrid), with grid bounds
+taken from the stored photons as this renderer takes them
+(ref_cuda_harness.cu); its own driver would use fixed Cornell-box bounds.
 
 Prints one JSON line: both throughputs in Mpaths/s and the relative RMSE
 between the two renderers' images of the last task (the same paths; the two
 builds differ only in floating-point contraction and elementary functions).
 
-    python oracle/ref_cuda_bench.py --workload large_mesh --mode graph --steps 5
+    python oracle/ref_cuda_bench.py --workload large_mesh --mode graph,persistent --steps 5
     python oracle/ref_cuda_bench.py --manifest assets/scenes/sponza.json --spp 4
 """
 import argparse
@@ -40,45 +42,46 @@ def load():
     lib.wfcuda_scene_create.argtypes = [P, P]
     lib.wfcuda_scene_destroy.argtypes = [P]
     lib.wfcuda_render.restype = C.c_int
-    lib.wfcuda_render.argtypes = [P, P, P, C.c_int, U32, U32, U32, P, P]
+    lib.wfcuda_render.argtypes = [P, P, P, C.c_int, U32, U32, U32, P, P, P, P]
     return lib
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="large_mesh")
-    ap.add_argument("--mode", choices=("graph", "persistent"), default="graph")
-    ap.add_argument("--spp", type=int, default=0, help="samples per task (default: bench.py's samples per step)")
-    ap.add_argument("--own-mode", choices=("graph", "persistent", "stream"), default=None,
-                    help="schedule of the B200 renderer (default: bench.py's schedule for the workload)")
-    ap.add_argument("--steps", type=int, default=5, help="timed tasks (after one warm-up task)")
-    ap.add_argument("--sample-start", type=int, default=1000)
-    ap.add_argument("--manifest", default=None,
-                    help="a scene manifest of the reference's presets, loaded by wfpt.assets, instead of a workload")
-    ap.add_argument("--size", default="1280x720", help="image size for --manifest")
-    args = ap.parse_args()
+def rel_rmse(image, reference):
+    a = np.asarray(image, np.float64)
+    b = np.asarray(reference, np.float64)
+    return float(np.sqrt(np.mean((a - b) ** 2)) / max(np.sqrt(np.mean(b ** 2)), 1e-30))
 
+
+def compare(workload=None, modes=("graph", "persistent"), steps=5, spp=0, own_mode=None, sample_start=1000,
+            manifest=None, size="1280x720", caustics=True):
+    """Times the reference's CUDA renderer (each of `modes`) and this
+    renderer on the same whole-frame tasks; returns the result dict."""
     import bench
     import wfpt
     from wfpt import native
 
-    if args.manifest:
+    if manifest:
         from wfpt import assets
-        width, height = (int(x) for x in args.size.split("x"))
-        scene, cam = assets.preset_scene(args.manifest, width, height)
+        width, height = (int(x) for x in size.split("x"))
+        scene, cam = assets.preset_scene(manifest, width, height)
         rkw = {}
-        args.workload = "preset " + Path(args.manifest).stem
+        workload = "preset " + Path(manifest).stem
     else:
-        scene, cam, width, height, rkw = bench.make_scene(args.workload)
-    for k in ("caustics", "photon_count"):
-        rkw.pop(k, None)
-    args.spp = args.spp or bench.SPP_PER_STEP.get(args.workload, 1)
-    own_mode = args.own_mode or bench.DEFAULT_MODE.get(args.workload, "graph")
+        scene, cam, width, height, rkw = bench.make_scene(workload)
+    if not caustics:
+        for k in ("caustics", "photon_count"):
+            rkw.pop(k, None)
+    if rkw.get("caustics"):  # grid bounds derived from the stored photons on both sides
+        rkw.setdefault("photon_grid_min", (0, 0, 0))
+        rkw.setdefault("photon_grid_max", (0, 0, 0))
+    spp = spp or bench.SPP_PER_STEP.get(workload, 1)
+    own_mode = own_mode or bench.DEFAULT_MODE.get(workload, "graph")
     cfg = wfpt.render_config(width, height, **rkw)
     own_cfg = wfpt.render_config(width, height, mode=bench.MODES[own_mode], **rkw)
     cam_struct = native.camera_struct(cam)
+    paths = width * height * spp
 
-    # --- the reference's CUDA renderer
+    # --- the reference's CUDA renderer, one scene for every mode
     lib = load()
     d, keep = scene.desc()
     env, rgba = scene.environment_struct()
@@ -87,13 +90,28 @@ def main():
     ref_setup = time.perf_counter() - t0
     if not handle:
         raise SystemExit("reference scene creation failed")
-    ref_ms = (C.c_double * args.steps)()
-    ref_img = np.zeros((height, width, 3), np.float32)
-    rc = lib.wfcuda_render(handle, C.addressof(cam_struct), C.addressof(cfg), int(args.mode == "persistent"),
-                           args.sample_start, args.spp, args.steps, ref_img.ctypes.data, ref_ms)
-    lib.wfcuda_scene_destroy(handle)
-    if rc != 0:
-        raise SystemExit(f"reference render failed ({rc})")
+    ref = {}
+    ref_images = {}
+    try:
+        for mode in modes:
+            ms = (C.c_double * steps)()
+            img = np.zeros((height, width, 3), np.float32)
+            photon_ms = C.c_double(0.0)
+            counts = np.zeros(cfg.max_depth, np.uint32)
+            rc = lib.wfcuda_render(handle, C.addressof(cam_struct), C.addressof(cfg), int(mode == "persistent"),
+                                   sample_start, spp, steps, img.ctypes.data, ms, C.byref(photon_ms),
+                                   counts.ctypes.data if mode == "persistent" else None)
+            if rc != 0:
+                raise SystemExit(f"reference render failed ({rc}) in {mode} mode")
+            t = statistics.median(list(ms))
+            ref[mode] = {"Mpaths/s": paths / t / 1e3, "ms_per_task": t, "ms_per_task_all": [round(x, 3) for x in ms],
+                         "photon_map_ms": round(photon_ms.value, 2)}
+            if mode == "persistent":
+                # its --profile-queues record: per-bounce queue sizes of the last sample
+                ref[mode]["extension_rays_last_sample"] = int(counts.sum())
+            ref_images[mode] = img
+    finally:
+        lib.wfcuda_scene_destroy(handle)
     del keep, rgba
 
     # --- this renderer, same tasks, same timing
@@ -101,34 +119,59 @@ def main():
     r = wfpt.Renderer(dev, cam, own_cfg)
     own_ms = []
     own_img = None
-    for i in range(args.steps + 1):
-        start = args.sample_start + i * args.spp
+    r.stats(reset=True)
+    for i in range(steps + 1):
+        start = sample_start + i * spp
+        if i == 1:
+            r.stats(reset=True)
         t0 = time.perf_counter()
-        img = r.render_task((0, 0, width, height), start, args.spp)
+        img = r.render_task((0, 0, width, height), start, spp)
         t1 = time.perf_counter()
         if i:
             own_ms.append((t1 - t0) * 1e3)
         own_img = img
+    stats = r.stats(reset=True)
     r.close()
     dev.close()
-
-    paths = width * height * args.spp
-    ref_t = statistics.median(list(ref_ms))
     own_t = statistics.median(own_ms)
-    diff = own_img.astype(np.float64) - ref_img.astype(np.float64)
-    rel_rmse = float(np.sqrt(np.mean(diff ** 2)) / max(np.sqrt(np.mean(ref_img.astype(np.float64) ** 2)), 1e-30))
-    print(json.dumps({
-        "workload": args.workload, "triangles": int(scene.triangle_count()), "width": width, "height": height,
-        "spp_per_task": args.spp,
-        "max_depth": cfg.max_depth, "caustics": 0, "reference_mode": args.mode, "own_mode": own_mode,
-        "reference_cuda": {"Mpaths/s": paths / ref_t / 1e3, "ms_per_task": ref_t,
-                           "ms_per_task_all": [round(x, 3) for x in ref_ms], "scene_setup_s": ref_setup},
-        "b200_renderer": {"Mpaths/s": paths / own_t / 1e3, "ms_per_task": own_t,
-                          "ms_per_task_all": [round(x, 3) for x in own_ms]},
-        "speedup": ref_t / own_t,
-        "image_relative_rmse": rel_rmse,
+    rays_per_task = (stats["extension_rays"] + stats["shadow_rays"]) / steps
+    for mode in modes:
+        ref[mode]["Mrays/s"] = rays_per_task / ref[mode]["ms_per_task"] / 1e3
+        ref[mode]["speedup"] = ref[mode]["ms_per_task"] / own_t
+        ref[mode]["image_relative_rmse"] = rel_rmse(own_img, ref_images[mode])
+    return {
+        "workload": workload, "triangles": int(scene.triangle_count()), "width": width, "height": height,
+        "spp_per_task": spp, "max_depth": cfg.max_depth,
+        "caustics": int(cfg.caustics), "photons": int(cfg.photon_count) if cfg.caustics else 0,
+        "own_mode": own_mode, "reference_cuda": ref, "reference_scene_setup_s": round(ref_setup, 2),
+        "b200_renderer": {"Mpaths/s": paths / own_t / 1e3, "Mrays/s": rays_per_task / own_t / 1e3,
+                          "ms_per_task": own_t, "ms_per_task_all": [round(x, 3) for x in own_ms],
+                          "extension_rays_per_task": stats["extension_rays"] / steps,
+                          "shadow_rays_per_task": stats["shadow_rays"] / steps},
         "timing": "wall time per whole-frame task: render + download of the radiance (median)",
-    }), flush=True)
+        "rays": "Mrays/s of both renderers count the same rays: this renderer's extension + shadow rays of the "
+                "identical paths (the reference's persistent queue counts give its extension rays: "
+                "extension_rays_last_sample)",
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="large_mesh")
+    ap.add_argument("--mode", default="graph,persistent", help="reference schedules, comma-separated")
+    ap.add_argument("--spp", type=int, default=0, help="samples per task (default: bench.py's samples per step)")
+    ap.add_argument("--own-mode", choices=("graph", "persistent", "stream"), default=None,
+                    help="schedule of the B200 renderer (default: bench.py's schedule for the workload)")
+    ap.add_argument("--steps", type=int, default=5, help="timed tasks (after one warm-up task)")
+    ap.add_argument("--sample-start", type=int, default=1000)
+    ap.add_argument("--no-caustics", action="store_true", help="turn the workload's photon caustics off on both sides")
+    ap.add_argument("--manifest", default=None,
+                    help="a scene manifest of the reference's presets, loaded by wfpt.assets, instead of a workload")
+    ap.add_argument("--size", default="1280x720", help="image size for --manifest")
+    args = ap.parse_args()
+    out = compare(args.workload, tuple(args.mode.split(",")), args.steps, args.spp, args.own_mode, args.sample_start,
+                  args.manifest, args.size, caustics=not args.no_caustics)
+    print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":

@@ -18,24 +18,42 @@
 // here with the project's binned-SAH builder (the same trees the host build of
 // the reference and the B200 renderer traverse), built on the host and
 // uploaded (shim_cuda/NXB/BVH.h).
+// Standard headers first: the access override below must not reach them.
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
 #include "config.hpp"
 #include "renderer/image_output.hpp"
+// The photon map of a caustic render is built here with the reference's
+// public kernels (emitPhotons / tracePhotons / buildPhotonGrid,
+// include/renderer/renderer.cuh:34-41) and handed to the driver's resources
+// before its graph is captured, in place of RenderDriver::buildPhotonMap,
+// whose grid has fixed Cornell-box bounds (render_driver.cu:211-213) and runs
+// only for the Cornell family of presets (render_driver.cu:181-182).  That
+// needs the driver's private members, opened for this file only.
+#define private public
 #include "renderer/render_driver.cuh"
+#undef private
 #include "renderer/render_fingerprint.hpp"
 #include "renderer/render_task.cuh"
+#include "renderer/renderer.cuh"
 #include "scene/environment.hpp"
 #include "scene/scene_host.hpp"
 
 #include "../wavefront-path-tracer_b200/csrc/bvh_build.h"
 #include "ref_scene_convert.h"
-
-#include <algorithm>
-#include <chrono>
-#include <cstdio>
-#include <cstring>
-#include <memory>
-#include <stdexcept>
-#include <vector>
 
 // ------------------------------------------------------------ NXB builder
 namespace {
@@ -105,6 +123,83 @@ struct CudaRefScene {
 };
 }  // namespace
 
+namespace {
+#define WFCUDA_CHECK(call)                                                                      \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) throw std::runtime_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// RenderDriver::buildPhotonMap (render_driver.cu:180-234) with the grid
+// bounds taken from the stored photons instead of the Cornell constants:
+// the bounding box of the valid photons, with a degenerate axis given unit
+// extent -- the bounds the B200 renderer derives when its config's grid
+// minimum equals its maximum.  Explicit bounds (min != max) are used as
+// given.  Returns the build's wall time in milliseconds.
+double build_photon_map(RenderDriver& driver, const wf_render_config* c) {
+    auto t0 = std::chrono::steady_clock::now();
+    RenderResources& res = driver.resources_;
+    const Scene& scene = driver.deviceScene_.scene;
+    uint32_t n = c->photon_count;
+    WFCUDA_CHECK(cudaDeviceSetLimit(cudaLimitStackSize, 16 * 1024));  // as buildPhotonMap sets it
+    WFCUDA_CHECK(cudaMalloc(&res.devicePhotons, sizeof(Photon) * n));
+    WFCUDA_CHECK(cudaMalloc(&res.devicePhotonMaterialHitCounts, sizeof(uint32_t) * 3));
+    WFCUDA_CHECK(cudaMemset(res.devicePhotonMaterialHitCounts, 0, sizeof(uint32_t) * 3));
+    WFCUDA_CHECK(cudaMemset(res.devicePhotons, 0, sizeof(Photon) * n));
+    res.photonQueue.items = res.devicePhotons;
+    res.photonQueue.capacity = n;
+    uint32_t block = driver.config_.blockSize;
+    uint32_t blocks = (n + block - 1) / block;
+    emitPhotons<<<blocks, block>>>(res.photonQueue, scene, n, c->photon_seed, RngStrategy(c->rng), c->spectral != 0);
+    WFCUDA_CHECK(cudaGetLastError());
+    tracePhotons<<<blocks, block>>>(res.photonQueue, scene, n, c->photon_max_depth, res.devicePhotonMaterialHitCounts);
+    WFCUDA_CHECK(cudaGetLastError());
+    WFCUDA_CHECK(cudaDeviceSynchronize());
+    PhotonGrid grid{};
+    grid.photons = res.devicePhotons;
+    grid.resolution = c->photon_grid_resolution ? c->photon_grid_resolution : 64;
+    bool derive = c->photon_grid_min[0] == c->photon_grid_max[0] && c->photon_grid_min[1] == c->photon_grid_max[1] &&
+                  c->photon_grid_min[2] == c->photon_grid_max[2];
+    if (derive) {
+        std::vector<Photon> host(n);
+        WFCUDA_CHECK(cudaMemcpy(host.data(), res.devicePhotons, sizeof(Photon) * n, cudaMemcpyDeviceToHost));
+        float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        bool any = false;
+        for (const Photon& p : host) {
+            if (!p.valid) continue;
+            float v[3] = {p.position.x, p.position.y, p.position.z};
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = any ? std::min(lo[a], v[a]) : v[a];
+                hi[a] = any ? std::max(hi[a], v[a]) : v[a];
+            }
+            any = true;
+        }
+        if (!any) {
+            for (int a = 0; a < 3; ++a) lo[a] = -1.0f, hi[a] = 1.0f;
+        }
+        for (int a = 0; a < 3; ++a)
+            if (!(hi[a] > lo[a])) hi[a] = lo[a] + 1.0f;
+        grid.minimum = Vec3(lo[0], lo[1], lo[2]);
+        grid.maximum = Vec3(hi[0], hi[1], hi[2]);
+    } else {
+        grid.minimum = Vec3(c->photon_grid_min[0], c->photon_grid_min[1], c->photon_grid_min[2]);
+        grid.maximum = Vec3(c->photon_grid_max[0], c->photon_grid_max[1], c->photon_grid_max[2]);
+    }
+    uint32_t cells = grid.resolution * grid.resolution * grid.resolution;
+    WFCUDA_CHECK(cudaMalloc(&grid.heads, sizeof(uint32_t) * cells));
+    WFCUDA_CHECK(cudaMalloc(&grid.next, sizeof(uint32_t) * n));
+    WFCUDA_CHECK(cudaMemset(grid.heads, 0xff, sizeof(uint32_t) * cells));
+    WFCUDA_CHECK(cudaMemset(grid.next, 0xff, sizeof(uint32_t) * n));
+    buildPhotonGrid<<<blocks, block>>>(res.photonQueue, grid, n);
+    WFCUDA_CHECK(cudaGetLastError());
+    WFCUDA_CHECK(cudaDeviceSynchronize());
+    res.photonGrid = grid;  // released with the driver's resources
+    res.shadingPhotonGrid = grid;
+    if (!c->caustic_gather) res.shadingPhotonGrid.heads = nullptr;
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+}  // namespace
+
 extern "C" {
 
 void* wfcuda_scene_create(const wf_scene_desc* d, const wf_environment* env) {
@@ -141,15 +236,19 @@ void wfcuda_scene_destroy(void* handle) {
     delete r;
 }
 
+
 // Renders one warm-up task and then `steps` whole-frame tasks of `spp`
 // samples each (absolute samples from sample_start on) through
 // RenderTaskRenderer::render.  task_ms[i] is the wall time of task i, which
 // covers the reference's own clear, launches, stream synchronisation and
 // download; rgb (optional) receives the last task's unnormalised sums.
-// Caustics stay off: the reference builds a photon map only for its Cornell
-// family of presets, with fixed Cornell grid bounds (render_driver.cu:180-214).
+// With c->caustics the photon map is built first (build_photon_map above)
+// and *photon_ms receives its wall time.  queue_counts (optional, max_depth
+// entries) receives the reference's per-bounce queue sizes of the last task
+// in persistent mode (its --profile-queues record, renderer.cu:89-90).
 int wfcuda_render(void* handle, const wf_camera* cam, const wf_render_config* c, int persistent,
-                  uint32_t sample_start, uint32_t spp, uint32_t steps, float* rgb, double* task_ms) {
+                  uint32_t sample_start, uint32_t spp, uint32_t steps, float* rgb, double* task_ms,
+                  double* photon_ms, uint32_t* queue_counts) {
     try {
         CudaRefScene* r = static_cast<CudaRefScene*>(handle);
         if (!r || spp == 0) return 1;
@@ -169,11 +268,22 @@ int wfcuda_render(void* handle, const wf_camera* cam, const wf_render_config* c,
         config.persistentWavefront = persistent != 0;
         config.indirectRadianceClamp = c->indirect_clamp;
         config.rngStrategy = RngStrategy(c->rng);
-        config.enableCaustics = false;
+        config.blockSize = 256;
+        // The Demo preset is not a caustic preset, so prepare() builds no
+        // photon map of its own; a caustic render gets the one built below.
+        config.enableCaustics = c->caustics != 0;
+        config.enableCausticGather = c->caustic_gather != 0;
+        config.causticPhotonCount = c->caustics ? c->photon_count : config.causticPhotonCount;
+        config.causticMaxDepth = c->photon_max_depth;
+        config.causticGatherRadius = c->gather_radius;
+        config.profileQueues = persistent && queue_counts != nullptr;
         config.distributedRole = DistributedRole::Worker;  // no local checkpoint writer
         SceneConfig scene_config;
         scene_config.preset = ScenePreset::Demo;
         RenderDriver driver(r->device, camera, config, scene_config);
+        if (!driver.prepare()) return 4;
+        double map_ms = c->caustics ? build_photon_map(driver, c) : 0.0;
+        if (photon_ms) *photon_ms = map_ms;
         RenderTaskRenderer renderer(driver);
         RenderTask task;
         task.jobFingerprint = computeRenderFingerprint(config, scene_config);
@@ -187,6 +297,9 @@ int wfcuda_render(void* handle, const wf_camera* cam, const wf_render_config* c,
             if (i > 0) task_ms[i - 1] = std::chrono::duration<double, std::milli>(t1 - t0).count();
             if (i == steps && rgb) std::memcpy(rgb, result.radiance.data(), sizeof(float) * 3 * result.radiance.size());
         }
+        if (config.profileQueues && driver.resources_.deviceQueueCounts)
+            WFCUDA_CHECK(cudaMemcpy(queue_counts, driver.resources_.deviceQueueCounts, sizeof(uint32_t) * c->max_depth,
+                                    cudaMemcpyDeviceToHost));
         return 0;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "wfcuda_render: %s\n", e.what());

@@ -589,6 +589,72 @@ int wfref_render(void* handle, const wf_camera* cam, const wf_render_config* c, 
     }
 }
 
+// The ray queues of one sample of a tile through the reference's captured
+// chain (generatePrimaryRays, then intersectScene + shadePaths per bounce,
+// renderer.cu:10-42, device_path_shading.cuh:6-173): the camera rays
+// (bounce 0) and the continuation rays each bounce appends, for `bounces`
+// queues.  rays receives them back to back (capacity ray_capacity), in queue
+// order; counts[b] the size of queue b.  Caustics are not gathered (the
+// queues do not depend on them).  Returns the number of rays written, or
+// ~0u on an error or an overflow of ray_capacity.
+uint32_t wfref_path_rays(void* handle, const wf_camera* cam, const wf_render_config* c, uint32_t x0, uint32_t y0,
+                         uint32_t tw, uint32_t th, uint32_t sample, uint32_t bounces, wf_ray* rays,
+                         uint32_t ray_capacity, uint32_t* counts, int threads) {
+    try {
+        RefScene* r = static_cast<RefScene*>(handle);
+        Scene scene = r->device.scene;
+        Camera camera;
+        camera.position = v3(cam->position);
+        camera.forward = v3(cam->forward);
+        camera.right = v3(cam->right);
+        camera.up = v3(cam->up);
+        camera.verticalFov = cam->vertical_fov;
+        camera.aspectRatio = cam->aspect_ratio;
+        uint32_t width = c->width, height = c->height;
+        uint32_t capacity = tw * th;
+        std::vector<PathState> paths(capacity);
+        std::vector<RayWorkItem> raysA(capacity), raysB(capacity);
+        std::vector<IntersectionResult> results(capacity);
+        std::vector<Vec3> sampleBuffer(size_t(width) * height);
+        uint32_t countA = 0, countB = 0;
+        RenderTile tile{x0, y0, tw, th, 1};
+        uint32_t sampleIndex = sample;
+        RngStrategy strategy = RngStrategy(c->rng);
+        RayQueue current{raysA.data(), &countA, capacity};
+        RayQueue next{raysB.data(), &countB, capacity};
+        parallel_for(capacity, threads, [&](uint32_t) {
+            generatePrimaryRays(current, paths.data(), camera, width, height, &sampleIndex, &tile, strategy,
+                                c->indirect_clamp);
+        });
+        uint32_t written = 0;
+        for (uint32_t b = 0; b < bounces; ++b) {
+            uint32_t n = *current.count;
+            counts[b] = n;
+            if (written + n > ray_capacity) return ~0u;
+            for (uint32_t i = 0; i < n; ++i) {
+                const Ray& ray = current.items[i].ray;
+                wf_ray& out = rays[written + i];
+                out.origin[0] = ray.origin.x; out.origin[1] = ray.origin.y; out.origin[2] = ray.origin.z;
+                out.direction[0] = ray.direction.x; out.direction[1] = ray.direction.y;
+                out.direction[2] = ray.direction.z;
+            }
+            written += n;
+            if (b + 1 == bounces) break;
+            *next.count = 0;
+            parallel_for(n, threads, [&](uint32_t) { intersectScene(current, results.data(), scene); });
+            parallel_for(n, threads, [&](uint32_t) {
+                shadePaths(current, results.data(), next, paths.data(), scene, c->max_depth, c->rr_start_depth,
+                           false, false, sampleBuffer.data(), PhotonGrid{}, c->gather_radius);
+            });
+            std::swap(current, next);
+        }
+        return written;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "wfref_path_rays: %s\n", e.what());
+        return ~0u;
+    }
+}
+
 float wfref_dielectric_reflectance(float cosine, float eta) { return dielectricReflectance(cosine, eta); }
 
 // The reference's checkpoint reader/writer (render_checkpoint.cpp), for

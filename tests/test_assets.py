@@ -20,7 +20,11 @@ import oracle
 from wfpt import abi, assets
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "assets"
-REFERENCE_SCENES = Path(os.environ.get("WF_REFERENCE", "/root/reference")) / "assets" / "scenes"
+# The reference's asset presets: $WF_REFERENCE, or a checkout named
+# "reference" beside this repository; the preset comparisons skip without it.
+REFERENCE_ROOT = (Path(os.environ["WF_REFERENCE"]) if os.environ.get("WF_REFERENCE")
+                  else Path(__file__).resolve().parents[2] / "reference")
+REFERENCE_SCENES = REFERENCE_ROOT / "assets" / "scenes"
 KIND = {"sponza": "gltf", "deer": "obj", "demo": "demo", "rtweek": "rtweek"}
 
 needs_oracle = pytest.mark.skipif(not oracle.available(det=True), reason="oracle/_ref/libwfref_det.so not built")

@@ -168,3 +168,19 @@ def test_reference_twins_images_close():
     a, _, _ = oracle.RefScene(scene).render(cam, cfg, sample_count=8)
     b, _, _ = oracle.RefScene(scene, det=True).render(cam, cfg, sample_count=8)
     assert relative_rmse(a, b) < 0.05
+
+
+def test_reference_config_matches_library_defaults():
+    """oracle.reference_config (the CPU reference arm's config, built without
+    the B200 library) equals wf_render_config_default field by field."""
+    import ctypes
+    import wfpt
+    from wfpt import abi
+    a = oracle.reference_config(1920, 1080)
+    b = wfpt.render_config(1920, 1080)
+    assert ctypes.string_at(ctypes.addressof(a), ctypes.sizeof(a)) == \
+        ctypes.string_at(ctypes.addressof(b), ctypes.sizeof(b))
+    a = oracle.reference_config(64, 32, max_depth=5, caustics=1, photon_grid_min=(0, 0, 0))
+    b = wfpt.render_config(64, 32, max_depth=5, caustics=1, photon_grid_min=(0, 0, 0))
+    assert bytes(a) == bytes(b)
+    assert ctypes.sizeof(a) == ctypes.sizeof(abi.RenderConfig)

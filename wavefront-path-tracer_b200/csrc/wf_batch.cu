@@ -325,7 +325,7 @@ __global__ void k_batch_condition(cudaGraphConditionalHandle handle, Counters* c
 
 template <typename T>
 cudaError_t batch_alloc(wf_batch* b, T** p, size_t count) {
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * std::max<size_t>(count, 1));
+    cudaError_t e = device_alloc(reinterpret_cast<void**>(p), sizeof(T) * std::max<size_t>(count, 1));
     if (e == cudaSuccess) b->allocations.push_back(*p);
     return e;
 }
@@ -449,6 +449,8 @@ RenderParams job_params(const wf_batch_job& j) {
     return rp;
 }
 
+wf_status batch_destroy(wf_batch* b);
+
 wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_config* cfg, void* stream,
                        wf_batch** out) {
     if (!jobs || !out || count == 0) return fail(WF_ERR_INVALID_ARG, "empty batch");
@@ -462,7 +464,8 @@ wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_
     for (uint32_t i = 0; i < count; ++i)
         if (wf_status e = validate_job(jobs[i], i)) return e;
 
-    auto b = std::make_unique<wf_batch>();
+    // A creation that fails part way frees what it had made.
+    std::unique_ptr<wf_batch, wf_status (*)(wf_batch*)> b(new wf_batch(), batch_destroy);
     wf_batch* bp = b.get();
     b->jobs.assign(jobs, jobs + count);
     b->block = config.block_size ? config.block_size : 128u;
@@ -569,7 +572,7 @@ wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_
 
 wf_status batch_destroy(wf_batch* b) {
     if (!b) return WF_OK;
-    cudaStreamSynchronize(b->stream);
+    if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     for (void* p : b->allocations) cudaFree(p);

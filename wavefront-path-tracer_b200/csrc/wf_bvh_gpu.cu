@@ -22,6 +22,7 @@
 // left == kInvalidChild and right == primitive, the root last.
 #include "bvh_build.h"
 #include "wf_bvh_gpu.h"
+#include "wf_internal.h"
 
 #include <cuda_runtime.h>
 
@@ -219,7 +220,7 @@ struct Scratch {
     template <typename T>
     T* alloc(size_t count) {
         void* p = nullptr;
-        if (error == cudaSuccess) error = cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1));
+        if (error == cudaSuccess) error = device_alloc(&p, sizeof(T) * std::max<size_t>(count, 1));
         if (error == cudaSuccess) blocks.push_back(p);
         return static_cast<T*>(p);
     }

@@ -1,6 +1,7 @@
 // C ABI entry points (include/wavefront.h).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <algorithm>
@@ -14,7 +15,29 @@
 
 namespace wf {
 const char* last_error_text();
+
+namespace {
+// wf_test_fail_allocation: allocations left before the injected failure
+// (-1 = none armed).
+std::atomic<long long> g_fail_allocation{-1};
+}  // namespace
+
+cudaError_t device_alloc(void** p, size_t bytes) {
+    long long left = g_fail_allocation.load();
+    while (left >= 0) {
+        if (g_fail_allocation.compare_exchange_weak(left, left - 1)) {
+            if (left == 0) {
+                *p = nullptr;
+                return cudaErrorMemoryAllocation;
+            }
+            break;
+        }
+    }
+    return cudaMalloc(p, bytes);
 }
+}  // namespace wf
+
+extern "C" void wf_test_fail_allocation(int64_t after) { wf::g_fail_allocation.store(after < 0 ? -1 : after); }
 
 using namespace wf;
 
@@ -32,7 +55,7 @@ cudaError_t upload(wf_scene* s, std::vector<void*>& list, uint64_t& bytes, const
     if (v.empty()) return cudaSuccess;
     void* p = nullptr;
     size_t n = sizeof(T) * v.size();
-    cudaError_t e = cudaMalloc(&p, n);
+    cudaError_t e = device_alloc(&p, n);
     if (e != cudaSuccess) return e;
     list.push_back(p);
     bytes += n;
@@ -370,6 +393,10 @@ wf_status wf_synchronize(wf_renderer* r) {
         uint32_t f[2] = {0, 0};
         WF_CUDA(cudaMemcpy(&f[0], &parts[i]->counters->overflow, sizeof(uint32_t), cudaMemcpyDeviceToHost));
         WF_CUDA(cudaMemcpy(&f[1], &parts[i]->counters->error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        if (f[0] || f[1]) {  // reported once: the next render starts clean
+            WF_CUDA(cudaMemset(&parts[i]->counters->overflow, 0, sizeof(uint32_t)));
+            WF_CUDA(cudaMemset(&parts[i]->counters->error, 0, sizeof(uint32_t)));
+        }
         flags[0] |= f[0];
         flags[1] = flags[1] ? flags[1] : f[1];
     }
@@ -377,6 +404,21 @@ wf_status wf_synchronize(wf_renderer* r) {
         return fail(WF_ERR_TIMEOUT, "streaming loop exceeded samples x max_depth iterations");
     if (flags[1]) return fail(WF_ERR_TIMEOUT, "persistent kernel grid barrier timed out");
     if (flags[0]) return fail(WF_ERR_CAPACITY, "shadow queue or term buffer overflow (flags %u)", flags[0]);
+    return WF_OK;
+}
+
+wf_status wf_renderer_set_watchdog(wf_renderer* r, uint64_t barrier_cycles, uint32_t loop_iterations) {
+    if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
+    wf_renderer* parts[2];
+    for (int i = 0, n = renderer_parts(r, parts); i < n; ++i) {
+        Counters* c = parts[i]->counters;
+        unsigned long long cycles = barrier_cycles;
+        WF_CUDA(cudaMemcpyAsync(&c->barrier_limit, &cycles, sizeof(cycles), cudaMemcpyHostToDevice,
+                                parts[i]->stream));
+        WF_CUDA(cudaMemcpyAsync(&c->stream_limit, &loop_iterations, sizeof(loop_iterations), cudaMemcpyHostToDevice,
+                                parts[i]->stream));
+        WF_CUDA(cudaStreamSynchronize(parts[i]->stream));  // the host values are on this stack
+    }
     return WF_OK;
 }
 

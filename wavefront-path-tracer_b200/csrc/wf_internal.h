@@ -15,6 +15,11 @@ namespace wf {
 // Records the thread-local error text returned by wf_last_error().
 wf_status fail(wf_status status, const char* format, ...);
 
+// Every device allocation of the library goes through device_alloc, so a
+// test can make one of them fail (wf_test_fail_allocation) and check that
+// the entry point frees what it allocated and reports WF_ERR_OOM.
+cudaError_t device_alloc(void** p, size_t bytes);
+
 // The scene after the host build, in device layout (see wf_device.cuh).
 struct HostScene {
     std::vector<float4> triangles;  // 3 per triangle

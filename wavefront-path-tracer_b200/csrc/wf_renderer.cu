@@ -19,6 +19,8 @@
 #include "wf_lane_traverse.cuh"
 #include "wf_wavefront.cuh"
 
+#include <cuda.h>
+
 #include <algorithm>
 #include <cstring>
 #include <type_traits>
@@ -26,7 +28,7 @@
 namespace wf {
 
 wf_status cuda_fail(cudaError_t e, const char* what) {
-    return fail(WF_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return fail(e == cudaErrorMemoryAllocation ? WF_ERR_OOM : WF_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
 #define WF_CUDA(call)                                          \
@@ -450,6 +452,7 @@ __global__ void k_stream_condition(cudaGraphConditionalHandle handle, Counters* 
     uint32_t it = ++c->stream_iterations;
     bool live = c->queue_count[0] > 0;
     uint64_t bound = (uint64_t(tile->samples) * max_depth + 1) / 2 + 1;
+    if (c->stream_limit && c->stream_limit < bound) bound = c->stream_limit;
     if (live && it >= bound) {
         c->error = kErrorStreamBound;
         live = false;
@@ -463,13 +466,15 @@ __global__ void k_advance(Counters* c, const TileDev* tile) {
 }
 
 // Grid barrier with a bounded wait.  All blocks are co-resident (cooperative
-// launch).  A wait that exceeds ~2^31 cycles records an error and gives up;
-// callers then return and the host reports WF_ERR_TIMEOUT.
+// launch).  A wait that exceeds ~2^31 cycles (or the watchdog's bound)
+// records an error and gives up; callers then return and the host reports
+// WF_ERR_TIMEOUT.
 WF_DEV bool grid_barrier(Counters* c, uint32_t blocks) {
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile uint32_t* gen = &c->barrier_generation;
         uint32_t g = *gen;
+        long long limit = c->barrier_limit ? (long long)min(c->barrier_limit, 1ull << 62) : (1ll << 31);
         __threadfence();
         uint32_t arrived = atomicAdd(&c->barrier_count, 1u);
         if (arrived == blocks - 1) {
@@ -480,7 +485,7 @@ WF_DEV bool grid_barrier(Counters* c, uint32_t blocks) {
             long long start = clock64();
             while (*gen == g) {
                 if (*(volatile uint32_t*)&c->error) break;
-                if (clock64() - start > (1ll << 31)) {
+                if (clock64() - start > limit) {
                     atomicExch(&c->error, kErrorBarrierTimeout);
                     break;
                 }
@@ -837,7 +842,7 @@ __global__ void k_cell_counts(const uint32_t* start, uint32_t* end_to_count, uin
 template <typename T>
 cudaError_t alloc(wf_renderer* r, T** p, size_t count) {
     size_t bytes = sizeof(T) * std::max<size_t>(count, 1);
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+    cudaError_t e = device_alloc(reinterpret_cast<void**>(p), bytes);
     if (e == cudaSuccess) {
         r->allocations.push_back(*p);
         r->device_bytes += bytes;
@@ -1149,6 +1154,30 @@ wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
 
 }  // namespace
 
+// The config checks of RenderDriver::validateConfiguration and prepare
+// (render_driver.cu:104-147,429-437) that every render entry point makes,
+// plus this renderer's own fields.
+wf_status check_render_config(const wf_scene* scene, const wf_render_config& c) {
+    if (!std::isfinite(c.indirect_clamp) || c.indirect_clamp < 0.0f)
+        return fail(WF_ERR_INVALID_ARG, "Indirect radiance clamp must be finite and nonnegative");
+    if (c.width == 0 || c.height == 0) return fail(WF_ERR_INVALID_ARG, "Render dimensions must be greater than zero");
+    if (uint64_t(c.width) * c.height > 0xffffffffull)
+        return fail(WF_ERR_INVALID_ARG, "Render dimensions exceed the supported queue index range");
+    if (c.max_depth == 0) return fail(WF_ERR_INVALID_ARG, "maximum depth must be greater than zero");
+    if (c.max_depth > kMaxBounces) return fail(WF_ERR_INVALID_ARG, "maximum depth above %d", kMaxBounces);
+    if (c.block_size > 1024) return fail(WF_ERR_INVALID_ARG, "CUDA block size must be between 1 and 1024");
+    if (c.mode > WF_MODE_STREAM || c.rng > WF_RNG_PCG32 || c.debug > WF_DEBUG_SHADING_NORMAL)
+        return fail(WF_ERR_INVALID_ARG, "unknown mode, rng strategy or debug view");
+    if (c.caustics && c.photon_count == 0)
+        return fail(WF_ERR_INVALID_ARG, "Photon count must be greater than zero when caustics are enabled");
+    if (!(c.gather_radius > 0.0f))
+        return fail(WF_ERR_INVALID_ARG, "Caustic gather radius must be greater than zero");
+    if (c.refill_threshold > 32) return fail(WF_ERR_INVALID_ARG, "refill threshold must be between 0 and 32");
+    if (scene->view.punctual_count - scene->view.directional_count > 0 && scene->view.directional_count > 2)
+        return fail(WF_ERR_UNSUPPORTED, "more than two directional lights");
+    return WF_OK;
+}
+
 namespace {
 // external_framebuffer: render into this buffer instead of allocating one;
 // photon_source: reuse that renderer's photon map instead of building one.
@@ -1158,25 +1187,15 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
     if (!scene || !camera || !cfg || !out) return fail(WF_ERR_INVALID_ARG, "null argument");
     *out = nullptr;
     const wf_render_config& c = *cfg;
-    if (!std::isfinite(c.indirect_clamp) || c.indirect_clamp < 0.0f)
-        return fail(WF_ERR_INVALID_ARG, "Indirect radiance clamp must be finite and nonnegative");
-    if (c.width == 0 || c.height == 0) return fail(WF_ERR_INVALID_ARG, "Render dimensions must be greater than zero");
-    if (c.max_depth == 0) return fail(WF_ERR_INVALID_ARG, "maximum depth must be greater than zero");
-    if (c.max_depth > kMaxBounces) return fail(WF_ERR_INVALID_ARG, "maximum depth above %d", kMaxBounces);
-    if (c.block_size > 1024) return fail(WF_ERR_INVALID_ARG, "CUDA block size must be between 1 and 1024");
-    if (c.mode > WF_MODE_STREAM || c.rng > WF_RNG_PCG32 || c.debug > WF_DEBUG_SHADING_NORMAL)
-        return fail(WF_ERR_INVALID_ARG, "unknown mode, rng strategy or debug view");
-    if (c.caustics && c.photon_count == 0)
-        return fail(WF_ERR_INVALID_ARG, "Photon count must be greater than zero when caustics are enabled");
-    if (c.gather_radius <= 0.0f) return fail(WF_ERR_INVALID_ARG, "Caustic gather radius must be greater than zero");
-    if (scene->view.punctual_count - scene->view.directional_count > 0 && scene->view.directional_count > 2)
-        return fail(WF_ERR_UNSUPPORTED, "more than two directional lights");
+    if (wf_status e = check_render_config(scene, c)) return e;
     uint64_t pixels = uint64_t(c.width) * c.height;
     uint64_t capacity = (c.tile_width && c.tile_height) ? uint64_t(c.tile_width) * c.tile_height : pixels;
-    if (pixels > 0xffffffffull || capacity > 0xffffffffull)
+    if (capacity > 0xffffffffull)
         return fail(WF_ERR_INVALID_ARG, "Render dimensions exceed the supported queue index range");
 
-    auto r = std::make_unique<wf_renderer>();
+    // A creation that fails part way frees what it had made: renderer_destroy
+    // takes a partly built renderer.
+    std::unique_ptr<wf_renderer, wf_status (*)(wf_renderer*)> r(new wf_renderer(), renderer_destroy);
     r->scene = scene;
     r->config = c;
     r->capacity = uint32_t(std::min(capacity, pixels));
@@ -1184,7 +1203,6 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
     WF_CUDA(cudaDeviceGetAttribute(&r->sm_count, cudaDevAttrMultiProcessorCount, r->device));
     r->grid_cap = uint32_t(r->sm_count) * 64;
     if (c.block_size) r->block_trace = r->block_shade = c.block_size;
-    if (c.refill_threshold > 32) return fail(WF_ERR_INVALID_ARG, "refill threshold must be between 0 and 32");
     r->refill = c.refill_threshold ? c.refill_threshold : 8u;
     r->opaque = !scene->alpha_textures;
     r->textured = scene->textured;
@@ -1234,6 +1252,7 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
     if (c.mode != WF_MODE_PERSISTENT) {
         uint32_t requests_per_path = 5u + scene->view.directional_count;
         uint64_t shadow = uint64_t(cap) * requests_per_path;
+        if (c.shadow_queue_capacity && c.shadow_queue_capacity < shadow) shadow = c.shadow_queue_capacity;
         if (shadow > 0xffffffffull) shadow = 0xffffffffull;
         r->shadow_capacity = uint32_t(shadow);
         WF_CUDA(alloc(rr, &r->hit_a, cap));
@@ -1331,7 +1350,7 @@ wf_status renderer_destroy(wf_renderer* r) {
     if (r->twin) renderer_destroy(r->twin);
     if (r->twin_fork) cudaEventDestroy(r->twin_fork);
     if (r->twin_join) cudaEventDestroy(r->twin_join);
-    cudaStreamSynchronize(r->stream);
+    if (r->stream) cudaStreamSynchronize(r->stream);
     for (auto& slot : r->slots) {
         if (slot->writer.joinable()) slot->writer.join();
         if (slot->pixels) cudaFreeHost(slot->pixels);
@@ -1731,7 +1750,39 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 constexpr int kStaticMaxDevices = 64;
 std::mutex g_static_mutex;
 unsigned char* g_static_base[kStaticMaxDevices] = {};
+unsigned long long g_static_context[kStaticMaxDevices] = {};  // context the address belongs to
 uint32_t g_static_resident[kStaticMaxDevices][3] = {};  // per persistent-kernel variant
+
+// Unique id of the calling thread's current context (cuCtxGetId), or 0 when
+// none is current.  A device whose context is re-created (cudaDeviceReset,
+// then any runtime call) loads the module again, and the array may move: the
+// id changes with it, so the set-up runs again for the new context.  The
+// driver functions come from cudaGetDriverEntryPoint, so the library needs no
+// link against libcuda.
+cudaError_t current_context_id(unsigned long long& id) {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    id = 0;
+    if (!get_current || !get_id) {
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa{}, qb{};
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa);
+        if (e == cudaSuccess) e = cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb);
+        if (e != cudaSuccess) return e;
+        if (qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b)
+            return cudaErrorNotSupported;
+        get_current = reinterpret_cast<GetCurrent>(a);
+        get_id = reinterpret_cast<GetId>(b);
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS) return cudaErrorContextIsDestroyed;
+    if (!ctx) return cudaSuccess;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return cudaErrorContextIsDestroyed;
+    return cudaSuccess;
+}
 
 // Zeroes the counters at the start of a call (the array keeps the previous
 // call's contents) and writes the tile and the first sample index.
@@ -1762,17 +1813,9 @@ extern "C" wf_status wf_render_tile_static(const wf_scene* scene, const wf_camer
     using namespace wf;
     if (!scene || !camera || !config || !framebuffer) return fail(WF_ERR_INVALID_ARG, "null argument");
     const wf_render_config& c = *config;
-    if (!std::isfinite(c.indirect_clamp) || c.indirect_clamp < 0.0f)
-        return fail(WF_ERR_INVALID_ARG, "Indirect radiance clamp must be finite and nonnegative");
-    if (c.width == 0 || c.height == 0) return fail(WF_ERR_INVALID_ARG, "Render dimensions must be greater than zero");
-    if (c.max_depth == 0) return fail(WF_ERR_INVALID_ARG, "maximum depth must be greater than zero");
-    if (c.max_depth > kMaxBounces) return fail(WF_ERR_INVALID_ARG, "maximum depth above %d", kMaxBounces);
-    if (c.rng > WF_RNG_PCG32 || c.debug > WF_DEBUG_SHADING_NORMAL)
-        return fail(WF_ERR_INVALID_ARG, "unknown rng strategy or debug view");
+    if (wf_status e = check_render_config(scene, c)) return e;
     if (c.caustics)
         return fail(WF_ERR_UNSUPPORTED, "wf_render_tile_static does not build photon maps (caustics must be 0)");
-    if (scene->view.punctual_count - scene->view.directional_count > 0 && scene->view.directional_count > 2)
-        return fail(WF_ERR_UNSUPPORTED, "more than two directional lights");
     if (width == 0 || height == 0 || x >= c.width || y >= c.height || width > c.width - x || height > c.height - y)
         return fail(WF_ERR_INVALID_ARG, "Render task tile is outside the framebuffer");
     if (uint64_t(width) * height > kStaticMaxPixels)
@@ -1793,14 +1836,21 @@ extern "C" wf_status wf_render_tile_static(const wf_scene* scene, const wf_camer
     const int variant = !opaque ? 0 : (scene->textured ? 1 : 2);
     {
         std::lock_guard<std::mutex> lock(g_static_mutex);
-        if (!g_static_base[device]) {
+        unsigned long long context = 0;
+        WF_CUDA(current_context_id(context));
+        if (!g_static_base[device] || context == 0 || context != g_static_context[device]) {
+            // Set-up for this device's current context, with that device
+            // current: the runtime binds its primary context here if no
+            // context was current yet.
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
             if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+            WF_CUDA(current_context_id(context));
             int cooperative = 0;
             WF_CUDA(cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, device));
             if (!cooperative) return fail(WF_ERR_UNSUPPORTED, "device does not support cooperative launches");
             g_static_base[device] = static_cast<unsigned char*>(p);
+            g_static_context[device] = context;
         }
         if (!g_static_resident[device][variant]) {
             int sms = 0, per_sm = 0;

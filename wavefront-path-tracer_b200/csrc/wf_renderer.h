@@ -50,6 +50,9 @@ struct Counters {
     uint32_t profile[kMaxBounces];          // per-bounce queue sizes (latest sample)
     uint32_t persistent_count[kMaxBounces + 1];
     uint32_t persistent_work[kMaxBounces + 1];
+    // Bounds of the device-side waits (wf_renderer_set_watchdog); 0 = default.
+    unsigned long long barrier_limit;  // cycles a grid-barrier wait may take (default 2^31)
+    uint32_t stream_limit;             // streaming-loop passes per launch (default: samples x depth bound)
 };
 
 // Traversal work totals of one profiling pass: node visits, triangle tests,

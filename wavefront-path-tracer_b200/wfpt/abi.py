@@ -9,6 +9,8 @@ import ctypes as C
 import numpy as np
 
 WF_OK = 0
+(WF_ERR_INVALID_ARG, WF_ERR_OOM, WF_ERR_CUDA, WF_ERR_TIMEOUT, WF_ERR_FINGERPRINT, WF_ERR_CAPACITY, WF_ERR_IO,
+ WF_ERR_FORMAT, WF_ERR_UNSUPPORTED, WF_ERR_STATE) = range(1, 11)
 STATUS_NAMES = {
     0: "WF_OK", 1: "WF_ERR_INVALID_ARG", 2: "WF_ERR_OOM", 3: "WF_ERR_CUDA", 4: "WF_ERR_TIMEOUT",
     5: "WF_ERR_FINGERPRINT", 6: "WF_ERR_CAPACITY", 7: "WF_ERR_IO", 8: "WF_ERR_FORMAT",
@@ -140,6 +142,7 @@ class RenderConfig(C.Structure):
         ("photon_grid_min", C.c_float * 3), ("photon_grid_max", C.c_float * 3),
         ("photon_grid_resolution", C.c_uint32), ("photon_seed", C.c_uint32), ("spectral", C.c_uint32),
         ("profile_queues", C.c_uint32), ("refill_threshold", C.c_uint32), ("concurrent_tiles", C.c_uint32),
+        ("shadow_queue_capacity", C.c_uint32),
     ]
 
 
@@ -222,6 +225,8 @@ def declare(lib):
         "wf_framebuffer_download": (S, [P, U32, U32, U32, U32, P]),
         "wf_framebuffer_device": (S, [P, C.POINTER(P)]),
         "wf_synchronize": (S, [P]),
+        "wf_renderer_set_watchdog": (S, [P, U64, U32]),
+        "wf_test_fail_allocation": (None, [C.c_int64]),
         "wf_queue_counts": (S, [P, P, U32]),
         "wf_render_stats_get": (S, [P, C.POINTER(RenderStats), U32]),
         "wf_profile_sample": (S, [P, C.POINTER(KernelProfile)]),

@@ -14,10 +14,18 @@ i mod world.  Each rank renders its tasks through its own Renderer (the task
 call, wf_render of the tile and sample range) and merges them as the
 coordinator does.  One reduce sums the ranks' contributions onto rank 0
 (NCCL between GPUs, gloo on CPU), and one more ORs their completion flags.
-Rank 0 then holds the same state a reference coordinator would, and writes
-the same checkpoint file byte for byte in layout: a job can resume from
-either side's checkpoint.  Rendering needs no communication; only the merge
-at the end (or at a checkpoint) crosses ranks.
+Rank 0 then holds the coordinator's state and writes a checkpoint in the
+reference's file layout: a job can resume from either side's checkpoint.
+Rendering needs no communication; only the merge at the end (or at a
+checkpoint) crosses ranks.
+
+Which bytes match the reference: the header, task table, sample counts and
+completion flags always do.  The radiance bytes match a reference
+coordinator's only for one rank on a fresh job.  The coordinator adds each
+task into its running FP32 total as the task arrives; here each rank first
+sums its own tasks, the ranks' sums are reduced, and a resumed job adds the
+total to the restored radiance, so with several ranks or a resume the FP32
+additions are rounded in a different order.
 """
 from __future__ import annotations
 
@@ -245,7 +253,10 @@ def run_job(job: JobConfig, render, rank=0, world=1, resume=None, checkpoint_pat
     stops each rank after that many tasks (a partial run to checkpoint).
     Rank 0 returns its Coordinator (and writes `checkpoint_path` when given);
     other ranks return None.  With world > 1, torch.distributed must be
-    initialised; the two collectives run on every rank in the same order."""
+    initialised; the three reduces run on every rank in the same order.
+    The merged radiance equals a reference coordinator's bit for bit only
+    for world == 1 without `resume` (the sums are grouped per rank and added
+    to the restored total last, so the FP32 rounding order differs)."""
     coordinator = Coordinator(job)
     base_sequence = 0
     if resume is not None:

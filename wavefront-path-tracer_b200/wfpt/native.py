@@ -333,6 +333,10 @@ class Renderer:
     def synchronize(self):
         check(library().wf_synchronize(self.handle))
 
+    def set_watchdog(self, barrier_cycles=0, loop_iterations=0):
+        """wf_renderer_set_watchdog: bounds of the device-side waits (0 = default)."""
+        check(library().wf_renderer_set_watchdog(self.handle, int(barrier_cycles), int(loop_iterations)))
+
     def reset(self):
         check(library().wf_framebuffer_reset(self.handle))
 

@@ -496,6 +496,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--mode", default=None, choices=sorted(MODES), help="default: per workload")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: per workload)")
+    ap.add_argument("--regenerate-percent", type=int, default=0,
+                    help="streaming mode: share of idle slots (%%) at which waiting slots start their next "
+                         "samples together (0 = the renderer's default)")
     ap.add_argument("--concurrent-tiles", type=int, default=0,
                     help="graph mode: 1 = one wavefront, 2 = two on two streams (default)")
     ap.add_argument("--bvh-builder", default="host", choices=["host", "gpu"],
@@ -534,7 +537,8 @@ def main():
     dev_scene = wfpt.DeviceScene(scene)
     scene_info = dev_scene.info()
     args.mode = args.mode or DEFAULT_MODE[args.workload]
-    cfg = wfpt.render_config(width, height, mode=MODES[args.mode], concurrent_tiles=args.concurrent_tiles, **rkw)
+    cfg = wfpt.render_config(width, height, mode=MODES[args.mode], concurrent_tiles=args.concurrent_tiles,
+                             regenerate_percent=args.regenerate_percent, **rkw)
     spp = args.spp or SPP_PER_STEP[args.workload]
     renderer = wfpt.Renderer(dev_scene, cam, cfg, stream=stream.cuda_stream)
     setup_s = time.perf_counter() - t_setup
@@ -653,6 +657,7 @@ def main():
                        "max_depth": cfg.max_depth, "rr_start_depth": cfg.rr_start_depth,
                        "triangles": int(scene.triangle_count()), "instances": int(len(scene.instances)),
                        "photons": int(cfg.photon_count) if cfg.caustics else 0, "mode": args.mode,
+                       "regenerate_percent": (args.regenerate_percent or None) if args.mode == "stream" else None,
                        "wavefronts": 1 if args.mode != "graph" or args.concurrent_tiles == 1 else 2,
                        "scene_device_bytes": int(scene_bytes),
                        "bvh_builder": args.bvh_builder, "bvh_build_ms": round(float(scene_info.bvh_build_ms), 1),

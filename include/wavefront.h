@@ -397,6 +397,12 @@ typedef struct wf_render_config {
                                   terms count as unoccluded) and wf_synchronize reports
                                   WF_ERR_CAPACITY, as the reference's bounded appendWarpCompacted
                                   drops items beyond a queue's capacity (queue_compaction.cuh:8-29). */
+    uint32_t regenerate_percent; /* streaming mode: a slot whose path ended starts its pixel's next sample
+                                  once fewer than this percentage of the tile's slots still carry a
+                                  path; all waiting slots then start together, in slot order, and
+                                  their camera rays are traced coherently.  1..100 (100 = after every
+                                  bounce); 0 = the tuned default.  Each pixel still takes its samples
+                                  in order, so the sums do not depend on it. */
 } wf_render_config;
 
 /* Defaults of RenderConfig (config.hpp:11-41) at the given resolution. */

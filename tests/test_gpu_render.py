@@ -75,6 +75,19 @@ def test_stream_mode_bit_exact(cuda, name):
     assert 0 < stats["kernel_launches"] <= graph_stats["kernel_launches"]
 
 
+@pytest.mark.parametrize("percent", [1, 25, 100])
+@pytest.mark.parametrize("name", ["cornell", "large_mesh"])
+def test_stream_regeneration_threshold_keeps_sums(cuda, name, percent):
+    """Whatever share of the slots must be idle before waiting slots start
+    their next samples together (1 %: almost a sample at a time; 100 %: after
+    every bounce), each pixel takes its samples in order, so the sums equal
+    the reference's bit for bit."""
+    got, _, stats, want, want_counts, _ = render_both(name, abi.MODE_STREAM, regenerate_percent=percent)
+    diff = np.nonzero(got.view(np.uint32) != want.view(np.uint32))
+    assert diff[0].size == 0, f"{diff[0].size} channels differ"
+    assert stats["extension_rays"] == int(want_counts.sum())
+
+
 def test_stream_mode_tiles_and_long_ranges(cuda):
     """Tile-major frames, split ranges and a 16-sample range in streaming mode
     match the per-sample graph."""

@@ -554,6 +554,7 @@ wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_
     WF_BATCH_CUDA(cudaMemsetAsync(b->view.framebuffer, 0, sizeof(float) * fb, b->stream));
     WF_BATCH_CUDA(cudaMemsetAsync(b->counters, 0, sizeof(Counters), b->stream));
     b->paths.slot_sample = nullptr;
+    b->paths.wait = nullptr;
     b->view.jobs = b->jobs_dev;
     b->view.unit_job = b->unit_job;
     b->view.units = b->units;

@@ -70,9 +70,13 @@ __global__ void k_raygen_stream(RenderParams rp, const TileDev* tile_ptr, Counte
     uint32_t sample = c->sample_index;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
-        c->queue_count[0] = n;
+        // every slot starts with a camera ray: queue 0 holds no survivors yet
+        c->queue_count[0] = 0;
+        c->camera_count[0] = n;
+        c->camera_count[1] = 0;
         c->paths += uint64_t(n) * tile.samples;
         c->work_trace = 0;
+        c->work_camera = 0;
         c->stream_iterations = 0;
     }
     for (uint32_t lp = gid; lp < n; lp += gridDim.x * blockDim.x) {
@@ -81,6 +85,7 @@ __global__ void k_raygen_stream(RenderParams rp, const TileDev* tile_ptr, Counte
         store_path(ps, lp, path);
         ps.radiance[lp] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         ps.slot_sample[lp] = 0;
+        ps.wait[lp] = 0;
         queue[lp] = lp;
     }
 }
@@ -91,27 +96,37 @@ __global__ void k_raygen_stream(RenderParams rp, const TileDev* tile_ptr, Counte
 // The per-ray visit order and arithmetic are the same either way.
 // The closest-hit stage of one bounce; the kernels below differ only in
 // their register bounds.
+// `start` (nullable): the stage covers queue entries [*start, *start +
+// *count) instead of [0, *count) -- the streaming loop's camera rays, queued
+// after the survivors and traced beside them by a second launch -- and then
+// takes its work from `work` and leaves the per-bounce resets to the launch
+// over the survivors.
 template <typename Tally, bool kLanes>
 WF_DEV void trace_stage(const DeviceScene& s, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
-                        uint32_t* hit_inst, Counters* c, uint32_t bounce, TallyTotals* totals, uint32_t refill_at) {
+                        uint32_t* hit_inst, Counters* c, uint32_t bounce, TallyTotals* totals, uint32_t refill_at,
+                        const uint32_t* start, uint32_t* work) {
     count_launch(c);
     uint32_t n = *count;
+    uint32_t first = start ? *start : 0u;
+    uint32_t* counter = start ? work : &c->work_trace;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
-        c->shadow_count = 0;
-        c->gather_count = 0;
-        c->dense_count = 0;
-        c->work_shade = 0;
-        for (int k = 0; k < 8; ++k) c->shade_bucket[k] = c->shade_cursor[k] = 0;
-        if (bounce < kMaxBounces) c->profile[bounce] = n;
-        c->extension_rays += n;
+        if (!start) {
+            c->shadow_count = 0;
+            c->gather_count = 0;
+            c->dense_count = 0;
+            c->work_shade = 0;
+            for (int k = 0; k < 8; ++k) c->shade_bucket[k] = c->shade_cursor[k] = 0;
+            if (bounce < kMaxBounces) c->profile[bounce] = n;
+        }
+        atomicAdd(&c->extension_rays, (unsigned long long)n);
     }
     Tally tally;
     if constexpr (!kLanes) {
         uint32_t base;
-        while (next_chunk(&c->work_trace, n, base)) {
-            uint32_t i = base + (threadIdx.x & 31);
-            if (i >= n) continue;
+        while (next_chunk(counter, n, base)) {
+            uint32_t i = first + base + (threadIdx.x & 31);
+            if (i >= first + n) continue;
             uint32_t p = queue[i];
             float4 o = ps.origin[p], d = ps.direction[p];
             TraceState h;
@@ -128,9 +143,9 @@ WF_DEV void trace_stage(const DeviceScene& s, PathSoA ps, const uint32_t* queue,
     bool more = true;
     for (;;) {
         bool idle = L.stage == kStageDone;
-        uint32_t slot = refill(&c->work_trace, n, idle, refill_at, more);
+        uint32_t slot = refill(counter, n, idle, refill_at, more);
         if (slot != kInvalid) {
-            i = slot;
+            i = first + slot;
             uint32_t p = queue[i];
             float4 o = ps.origin[p], d = ps.direction[p];
             closest_begin(L, s, f4xyz(o), f4xyz(d), tally);
@@ -162,8 +177,9 @@ WF_DEV void trace_stage(const DeviceScene& s, PathSoA ps, const uint32_t* queue,
 template <typename Tally, bool kLanes = true>
 __global__ void __maxnreg__(72) k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const uint32_t* count,
                                         float4* hit_a, uint32_t* hit_inst, Counters* c, uint32_t bounce,
-                                        TallyTotals* totals, uint32_t refill_at) {
-    trace_stage<Tally, kLanes>(s, ps, queue, count, hit_a, hit_inst, c, bounce, totals, refill_at);
+                                        TallyTotals* totals, uint32_t refill_at, const uint32_t* start,
+                                        uint32_t* work) {
+    trace_stage<Tally, kLanes>(s, ps, queue, count, hit_a, hit_inst, c, bounce, totals, refill_at, start, work);
 }
 
 // Camera rays (one traversal per thread, coherent): bounded to 8 CTAs of 128
@@ -174,8 +190,8 @@ template <typename Tally>
 __global__ void __launch_bounds__(128, 8) k_trace_camera(DeviceScene s, PathSoA ps, const uint32_t* queue,
                                                          const uint32_t* count, float4* hit_a, uint32_t* hit_inst,
                                                          Counters* c, uint32_t bounce, TallyTotals* totals,
-                                                         uint32_t refill_at) {
-    trace_stage<Tally, false>(s, ps, queue, count, hit_a, hit_inst, c, bounce, totals, refill_at);
+                                                         uint32_t refill_at, const uint32_t* start, uint32_t* work) {
+    trace_stage<Tally, false>(s, ps, queue, count, hit_a, hit_inst, c, bounce, totals, refill_at, start, work);
 }
 
 // Shading categories: warps of k_shade take entries of one category at a
@@ -382,9 +398,9 @@ __global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float
 // Adds each path's accepted terms in emission order, applies the kill rule,
 // adds ended paths to the framebuffer and compacts survivors into `next`
 // (appendWarpCompacted, queue_compaction.cuh:8-29).  With kRegenerate (the
-// streaming mode) an ended path's slot starts its pixel's next sample, which
-// joins `next` like a survivor; the framebuffer add comes first, so every
-// pixel still accumulates its samples in sample order.
+// streaming mode) an ended path's slot is marked to start its pixel's next
+// sample (k_regenerate); the framebuffer add comes first, so every pixel
+// still accumulates its samples in sample order.
 template <bool kRegenerate>
 __global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* count, const float4* terms,
                            const int4* shade_out, const uint8_t* shadow_result, uint32_t* next, uint32_t* next_count,
@@ -420,16 +436,8 @@ __global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* co
                 f[1] += rad.y;
                 f[2] += rad.z;
                 if constexpr (kRegenerate) {
-                    TileDev tile = *tile_ptr;
-                    uint32_t started = ps.slot_sample[p] + 1;
-                    if (started < tile.samples) {
-                        Path path;
-                        init_path(rp, tile, c->sample_index + started, p, path);
-                        store_path(ps, p, path);
-                        ps.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        ps.slot_sample[p] = started;
-                        alive = true;
-                    }
+                    // the slot's next sample starts in k_regenerate
+                    if (ps.slot_sample[p] + 1 < tile_ptr->samples) ps.wait[p] = 1;
                 }
             }
         }
@@ -443,15 +451,18 @@ __global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* co
 }
 
 // Streaming loop condition: run the body again while paths remain.  Each
-// body pass advances every live path by two bounces, and a slot runs at most
-// samples * max_depth bounces, so a loop that exceeds that bound records an
+// body pass advances every live path by two bounces.  A slot's path takes at
+// most max_depth bounces, and a slot waits at most max_depth bounces for its
+// next sample (within that many bounces every path in flight has ended, and
+// an empty queue always regenerates), so a slot finishes within
+// samples * 2 * max_depth bounces; a loop that exceeds that bound records an
 // error and stops instead of spinning.
 __global__ void k_stream_condition(cudaGraphConditionalHandle handle, Counters* c, const TileDev* tile,
                                    uint32_t max_depth) {
     count_launch(c);
     uint32_t it = ++c->stream_iterations;
-    bool live = c->queue_count[0] > 0;
-    uint64_t bound = (uint64_t(tile->samples) * max_depth + 1) / 2 + 1;
+    bool live = c->queue_count[0] + c->camera_count[0] > 0;
+    uint64_t bound = uint64_t(tile->samples) * max_depth + 2;
     if (c->stream_limit && c->stream_limit < bound) bound = c->stream_limit;
     if (live && it >= bound) {
         c->error = kErrorStreamBound;
@@ -463,6 +474,52 @@ __global__ void k_stream_condition(cudaGraphConditionalHandle handle, Counters* 
 __global__ void k_advance(Counters* c, const TileDev* tile) {
     count_launch(c);
     if (tile->advance_sample) c->sample_index += tile->samples;
+}
+
+// Streaming mode: once fewer than `percent` % of the tile's slots carry a
+// path (or none does), every slot whose path ended and whose pixel has
+// samples left starts its next sample.  Warps take 32 consecutive slots and
+// append theirs with one atomic, so the camera rays queue after the
+// survivors in runs of neighbouring pixels, which k_trace_camera traces
+// coherently.  Per pixel the samples still run one after another.
+__global__ void k_regenerate(const __grid_constant__ RenderParams rp, const TileDev* tile_ptr, Counters* c,
+                             PathSoA ps, uint32_t* next, const uint32_t* next_count, uint32_t* camera_count,
+                             uint32_t capacity, uint32_t percent) {
+    count_launch(c);
+    TileDev tile = *tile_ptr;
+    uint32_t n = min(tile.width * tile.height, capacity);
+    uint32_t alive = *next_count;
+    if (alive != 0 && uint64_t(alive) * 100 >= uint64_t(n) * percent) return;
+    uint32_t lane = threadIdx.x & 31;
+    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t sample = c->sample_index;
+    for (uint32_t base = warp * 32; base < n; base += warps * 32) {
+        uint32_t p = base + lane;
+        bool waiting = p < n && ps.wait[p];
+        unsigned mask = __ballot_sync(0xffffffffu, waiting);
+        if (!mask) continue;
+        uint32_t out = 0;
+        if (lane == 0) out = atomicAdd(camera_count, uint32_t(__popc(mask)));
+        out = __shfl_sync(0xffffffffu, out, 0);
+        if (!waiting) continue;
+        uint32_t started = ps.slot_sample[p] + 1;
+        Path path;
+        init_path(rp, tile, sample + started, p, path);
+        store_path(ps, p, path);
+        ps.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        ps.slot_sample[p] = started;
+        ps.wait[p] = 0;
+        next[alive + out + __popc(mask & ((1u << lane) - 1u))] = p;
+    }
+}
+
+// Streaming mode, after both traces of a bounce: the camera rays join the
+// survivors, and their work counter is ready for the next bounce.
+__global__ void k_merge_camera(Counters* c, uint32_t q) {
+    count_launch(c);
+    c->queue_count[q] += c->camera_count[q];
+    c->camera_count[q] = 0;
+    c->work_camera = 0;
 }
 
 // Grid barrier with a bounded wait.  All blocks are co-resident (cooperative
@@ -1002,10 +1059,12 @@ wf_status capture_graph(wf_renderer* r) {
         uint32_t* next_count = &r->counters->queue_count[nxt];
         if (b == 0)
             launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st, 
-                s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill);
+                s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill,
+                nullptr, nullptr);
         else
             launch_trace<NoTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st, 
-                s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill);
+                s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill,
+                nullptr, nullptr);
         k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
                                                           r->counters);
         k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order, r->counters);
@@ -1073,8 +1132,19 @@ wf_status capture_stream_graph(wf_renderer* r) {
         uint32_t nxt = cur ^ 1;
         uint32_t* cur_count = &r->counters->queue_count[cur];
         uint32_t* next_count = &r->counters->queue_count[nxt];
-        launch_trace<NoTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st, 
-            s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, kMaxBounces, nullptr, r->refill);
+        // The camera rays of slots that started a sample (queued after the
+        // survivors) one per thread on a branch, the survivors by lane refill.
+        WF_CUDA(cudaEventRecord(r->fork_event, st));
+        WF_CUDA(cudaStreamWaitEvent(r->side, r->fork_event, 0));
+        launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, r->side,
+            s, r->paths, r->queue[cur], &r->counters->camera_count[cur], r->hit_a, r->hit_inst, r->counters,
+            kMaxBounces, nullptr, r->refill, cur_count, &r->counters->work_camera);
+        WF_CUDA(cudaEventRecord(r->join_event, r->side));
+        launch_trace<NoTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st,
+            s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, kMaxBounces, nullptr, r->refill,
+            nullptr, nullptr);
+        WF_CUDA(cudaStreamWaitEvent(st, r->join_event, 0));
+        k_merge_camera<<<1, 1, 0, st>>>(r->counters, cur);
         k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
                                                           r->counters);
         k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order, r->counters);
@@ -1097,6 +1167,9 @@ wf_status capture_stream_graph(wf_renderer* r) {
         k_finalize<true><<<grid(r, 3, cap, r->block_finalize), r->block_finalize, 0, st>>>(
             r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result, r->queue[nxt], next_count,
             cap, r->framebuffer, &r->counters->work_trace, r->params, r->tile, r->counters);
+        k_regenerate<<<grid(r, 3, cap, 256), 256, 0, st>>>(r->params, r->tile, r->counters, r->paths, r->queue[nxt],
+                                                           next_count, &r->counters->camera_count[nxt], cap,
+                                                           r->regenerate_percent);
     }
     k_stream_condition<<<1, 1, 0, st>>>(handle, r->counters, r->tile, r->config.max_depth);
     e = cudaStreamEndCapture(st, &captured);
@@ -1204,6 +1277,7 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
     r->grid_cap = uint32_t(r->sm_count) * 64;
     if (c.block_size) r->block_trace = r->block_shade = c.block_size;
     r->refill = c.refill_threshold ? c.refill_threshold : 8u;
+    r->regenerate_percent = c.regenerate_percent ? std::min(c.regenerate_percent, 100u) : kDefaultRegeneratePercent;
     r->opaque = !scene->alpha_textures;
     r->textured = scene->textured;
     if (stream) {
@@ -1264,7 +1338,10 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
         WF_CUDA(alloc(rr, &r->shadow_origin, r->shadow_capacity));
         WF_CUDA(alloc(rr, &r->shadow_dir, r->shadow_capacity));
         WF_CUDA(alloc(rr, &r->shadow_result, r->shadow_capacity));
-        if (c.mode == WF_MODE_STREAM) WF_CUDA(alloc(rr, &r->paths.slot_sample, cap));
+        if (c.mode == WF_MODE_STREAM) {
+            WF_CUDA(alloc(rr, &r->paths.slot_sample, cap));
+            WF_CUDA(alloc(rr, &r->paths.wait, cap));
+        }
         if (c.caustics) {
             WF_CUDA(alloc(rr, &r->gathers.position, cap));
             WF_CUDA(alloc(rr, &r->gathers.normal, cap));
@@ -1580,19 +1657,19 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                         if (count && b == 0)
                             launch_trace<CountTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st, 
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
-                                r->tally, r->refill);
+                                r->tally, r->refill, nullptr, nullptr);
                         else if (count)
                             launch_trace<CountTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st, 
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
-                                r->tally, r->refill);
+                                r->tally, r->refill, nullptr, nullptr);
                         else if (b == 0)
                             launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st, 
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
-                                nullptr, r->refill);
+                                nullptr, r->refill, nullptr, nullptr);
                         else
                             launch_trace<NoTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st, 
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
-                                nullptr, r->refill);
+                                nullptr, r->refill, nullptr, nullptr);
                     };
                     auto shade = [&] {  // with the category sort it feeds on
                         k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst,
@@ -1895,6 +1972,7 @@ extern "C" wf_status wf_render_tile_static(const wf_scene* scene, const wf_camer
     ps.info = reinterpret_cast<uint4*>(base + kStaticInfoOffset);
     ps.rng = reinterpret_cast<unsigned long long*>(base + kStaticRngOffset);
     ps.slot_sample = nullptr;
+    ps.wait = nullptr;
     uint32_t* q0 = reinterpret_cast<uint32_t*>(base + kStaticQueueOffset);
     uint32_t* q1 = q0 + kStaticMaxPixels;
 

@@ -22,6 +22,7 @@ struct TileDev {
 
 // Device counters of one renderer (one allocation, zeroed at creation).
 constexpr int kMaxBounces = 64;
+constexpr uint32_t kDefaultRegeneratePercent = 25;  // streaming mode (wf_render_config::regenerate_percent)
 constexpr uint32_t kErrorBarrierTimeout = 1;  // a persistent-kernel grid barrier wait gave up
 constexpr uint32_t kErrorStreamBound = 2;     // the streaming loop exceeded samples * max_depth bounces
 struct Counters {
@@ -50,6 +51,11 @@ struct Counters {
     uint32_t profile[kMaxBounces];          // per-bounce queue sizes (latest sample)
     uint32_t persistent_count[kMaxBounces + 1];
     uint32_t persistent_work[kMaxBounces + 1];
+    // Streaming mode: camera rays of slots that started a new sample, queued
+    // after queue_count[q] survivors of queue q (traced per thread, then
+    // merged into the queue), and the camera-ray trace's work counter.
+    uint32_t camera_count[2];
+    uint32_t work_camera;
     // Bounds of the device-side waits (wf_renderer_set_watchdog); 0 = default.
     unsigned long long barrier_limit;  // cycles a grid-barrier wait may take (default 2^31)
     uint32_t stream_limit;             // streaming-loop passes per launch (default: samples x depth bound)
@@ -69,6 +75,7 @@ struct PathSoA {
     uint4* info;        // pixel, depth, medium, flags (1 = specular, 2 = active)
     unsigned long long* rng;
     uint32_t* slot_sample;  // streaming mode: sample of the slot's path, relative to the launch's first
+    uint8_t* wait;          // streaming mode: 1 = the slot's path ended and its next sample has not started
 };
 
 struct AsyncCheckpointSlot {
@@ -121,6 +128,7 @@ struct wf_renderer {
     uint32_t persistent_block_size = 128;
     uint32_t chunk = 1;
     uint32_t refill = 8;  // trace/shadow kernels: idle lanes of a warp that trigger a refill
+    uint32_t regenerate_percent = 25;  // streaming mode: see wf_render_config::regenerate_percent
     // photon map
     uint32_t photons_emitted = 0, photons_stored = 0;
     float4* photon_raw = nullptr;  // 4 float4 per photon: pos(.w valid), dir, flux, rng/meta

@@ -142,7 +142,7 @@ class RenderConfig(C.Structure):
         ("photon_grid_min", C.c_float * 3), ("photon_grid_max", C.c_float * 3),
         ("photon_grid_resolution", C.c_uint32), ("photon_seed", C.c_uint32), ("spectral", C.c_uint32),
         ("profile_queues", C.c_uint32), ("refill_threshold", C.c_uint32), ("concurrent_tiles", C.c_uint32),
-        ("shadow_queue_capacity", C.c_uint32),
+        ("shadow_queue_capacity", C.c_uint32), ("regenerate_percent", C.c_uint32),
     ]
 
 

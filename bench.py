@@ -496,6 +496,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--mode", default=None, choices=sorted(MODES), help="default: per workload")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: per workload)")
+    ap.add_argument("--build", default="exact", choices=["exact", "fast"],
+                    help="exact: the bit-exact library (default); fast: multiply-adds contracted and CUDA's own "
+                         "elementary functions (make -C wavefront-path-tracer_b200 fast)")
     ap.add_argument("--regenerate-percent", type=int, default=0,
                     help="streaming mode: share of idle slots (%%) at which waiting slots start their next "
                          "samples together (0 = the renderer's default)")
@@ -507,6 +510,8 @@ def main():
                     help="skip timing the reference's own CUDA renderer built for sm_100a (make -C oracle cuda) "
                          "beside this one after the timed region (the `reference_cuda` object of the line)")
     args = ap.parse_args()
+    if args.build == "fast":
+        os.environ["WF_BUILD"] = "fast"  # read when wfpt loads the library
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
@@ -658,6 +663,7 @@ def main():
                        "triangles": int(scene.triangle_count()), "instances": int(len(scene.instances)),
                        "photons": int(cfg.photon_count) if cfg.caustics else 0, "mode": args.mode,
                        "regenerate_percent": (args.regenerate_percent or None) if args.mode == "stream" else None,
+                       "build": args.build,
                        "wavefronts": 1 if args.mode != "graph" or args.concurrent_tiles == 1 else 2,
                        "scene_device_bytes": int(scene_bytes),
                        "bvh_builder": args.bvh_builder, "bvh_build_ms": round(float(scene_info.bvh_build_ms), 1),

@@ -120,7 +120,19 @@ void writePpm(const char*, const std::vector<Vec3>&, uint32_t, uint32_t) {}
 namespace {
 struct CudaRefScene {
     DeviceScene device;
+    bool probe = false;
+    uint32_t original_material_count = 0;
 };
+
+// The reference's traceRayExternal (device_traversal.cuh:1196) over a batch
+// of rays, one per thread.
+__global__ void k_ref_trace(Scene scene, const wf_ray* rays, uint32_t count, TraceResult* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    Ray ray(Vec3(rays[i].origin[0], rays[i].origin[1], rays[i].origin[2]),
+            Vec3(rays[i].direction[0], rays[i].direction[1], rays[i].direction[2]));
+    out[i] = traceRayExternal(ray, scene);
+}
 }  // namespace
 
 namespace {
@@ -200,16 +212,72 @@ double build_photon_map(RenderDriver& driver, const wf_render_config* c) {
 }
 }  // namespace
 
+namespace {
+Camera reference_camera(const wf_camera* cam) {
+    Camera camera;
+    camera.position = wfref::v3(cam->position);
+    camera.forward = wfref::v3(cam->forward);
+    camera.right = wfref::v3(cam->right);
+    camera.up = wfref::v3(cam->up);
+    camera.verticalFov = cam->vertical_fov;
+    camera.aspectRatio = cam->aspect_ratio;
+    return camera;
+}
+
+// The reference's RenderConfig for a wf_render_config.  A config with a tile
+// size renders tiled (the queues hold one tile), which keeps the launches of
+// a small task small.
+RenderConfig reference_config(const wf_render_config* c, int persistent, bool profile_queues) {
+    RenderConfig config;
+    config.width = c->width;
+    config.height = c->height;
+    config.maxDepth = c->max_depth;
+    config.russianRouletteStartDepth = c->rr_start_depth;
+    config.samplesPerPixel = 1u << 30;  // bounds the absolute sample ranges of tasks
+    config.persistentWavefront = persistent != 0;
+    config.indirectRadianceClamp = c->indirect_clamp;
+    config.rngStrategy = RngStrategy(c->rng);
+    config.blockSize = 256;
+    if (c->tile_width && c->tile_height) {
+        config.tiledRendering = true;
+        config.tileWidth = c->tile_width;
+        config.tileHeight = c->tile_height;
+    }
+    // The Demo preset is not a caustic preset, so prepare() builds no photon
+    // map of its own; a caustic render gets the one build_photon_map makes.
+    config.enableCaustics = c->caustics != 0;
+    config.enableCausticGather = c->caustic_gather != 0;
+    config.causticPhotonCount = c->caustics ? c->photon_count : config.causticPhotonCount;
+    config.causticMaxDepth = c->photon_max_depth;
+    config.causticGatherRadius = c->gather_radius;
+    config.profileQueues = profile_queues;
+    config.distributedRole = DistributedRole::Worker;  // no local checkpoint writer
+    return config;
+}
+}  // namespace
+
 extern "C" {
 
-void* wfcuda_scene_create(const wf_scene_desc* d, const wf_environment* env) {
+// probe != 0: the hit-identity probe copy of the scene (ref_scene_convert.h;
+// instance lightOffset = index << 24), for wfcuda_trace.
+void* wfcuda_scene_create_probe(const wf_scene_desc* d, const wf_environment* env, int probe) {
     try {
         HostScene h;
-        wfref::host_scene_from_desc(d, false, h);
+        wfref::host_scene_from_desc(d, probe != 0, h);
         auto r = std::make_unique<CudaRefScene>();
+        r->probe = probe != 0;
+        r->original_material_count = d->material_count;
         r->device = uploadScene(h);
         r->device.scene.ignoreDirectLightOcclusion = d->ignore_direct_light_occlusion != 0;
         wfref::apply_normal_map_settings(r->device.scene, d);
+        if (probe && r->device.scene.instanceCount) {
+            std::vector<MeshInstance> inst(r->device.scene.instanceCount);
+            WFCUDA_CHECK(cudaMemcpy(inst.data(), r->device.instances, sizeof(MeshInstance) * inst.size(),
+                                    cudaMemcpyDeviceToHost));
+            for (uint32_t i = 0; i < inst.size(); ++i) inst[i].lightOffset = i << 24;
+            WFCUDA_CHECK(cudaMemcpy(r->device.instances, inst.data(), sizeof(MeshInstance) * inst.size(),
+                                    cudaMemcpyHostToDevice));
+        }
         if (env && env->width && env->height) {
             HostEnvironment map;
             map.width = env->width;
@@ -226,6 +294,75 @@ void* wfcuda_scene_create(const wf_scene_desc* d, const wf_environment* env) {
     } catch (const std::exception& e) {
         std::fprintf(stderr, "wfcuda_scene_create: %s\n", e.what());
         return nullptr;
+    }
+}
+
+void* wfcuda_scene_create(const wf_scene_desc* d, const wf_environment* env) {
+    return wfcuda_scene_create_probe(d, env, 0);
+}
+
+// Closest hits of `count` host rays with the reference's traversal on the
+// GPU, as wf_hit records (the probe copy fills kind / primitive / instance
+// from its identity codes, as oracle/ref_harness.cpp's wfref_trace does).
+int wfcuda_trace(void* handle, const wf_ray* rays, uint32_t count, wf_hit* hits) {
+    try {
+        CudaRefScene* r = static_cast<CudaRefScene*>(handle);
+        if (!r) return 1;
+        if (count == 0) return 0;
+        wf_ray* d_rays = nullptr;
+        TraceResult* d_out = nullptr;
+        WFCUDA_CHECK(cudaMalloc(&d_rays, sizeof(wf_ray) * count));
+        WFCUDA_CHECK(cudaMalloc(&d_out, sizeof(TraceResult) * count));
+        WFCUDA_CHECK(cudaMemcpy(d_rays, rays, sizeof(wf_ray) * count, cudaMemcpyHostToDevice));
+        k_ref_trace<<<(count + 127) / 128, 128>>>(r->device.scene, d_rays, count, d_out);
+        WFCUDA_CHECK(cudaGetLastError());
+        std::vector<TraceResult> res(count);
+        WFCUDA_CHECK(cudaMemcpy(res.data(), d_out, sizeof(TraceResult) * count, cudaMemcpyDeviceToHost));
+        cudaFree(d_rays);
+        cudaFree(d_out);
+        for (uint32_t i = 0; i < count; ++i) {
+            wf_hit& o = hits[i];
+            std::memset(&o, 0, sizeof(o));
+            o.instance = 0xffffffffu;
+            o.primitive = 0xffffffffu;
+            if (!res[i].didHit) {
+                o.material = WF_NO_MATERIAL;
+                o.light_index = 0xffffffffu;
+                o.kind = WF_HIT_NONE;
+                o.t = 1e30f;
+                continue;
+            }
+            const Hit& h = res[i].hit;
+            o.t = h.t;
+            o.position[0] = h.position.x; o.position[1] = h.position.y; o.position[2] = h.position.z;
+            o.geometric_normal[0] = h.geometricNormal.x;
+            o.geometric_normal[1] = h.geometricNormal.y;
+            o.geometric_normal[2] = h.geometricNormal.z;
+            o.normal[0] = h.normal.x; o.normal[1] = h.normal.y; o.normal[2] = h.normal.z;
+            o.material = h.material;
+            o.light_index = h.lightIndex;
+            o.kind = WF_HIT_NONE;
+            if (r->probe) {
+                if (h.material >= r->original_material_count) {
+                    o.kind = WF_HIT_SPHERE;
+                    o.primitive = h.material - r->original_material_count;
+                } else if (h.lightIndex & 0x80000000u) {
+                    o.kind = WF_HIT_TRIANGLE;
+                    o.primitive = h.lightIndex & 0x3fffffffu;
+                } else if (h.lightIndex & 0x40000000u) {
+                    o.kind = WF_HIT_STATIC_TRIANGLE;
+                    o.primitive = h.lightIndex & 0x3fffffffu;
+                } else {
+                    o.kind = WF_HIT_MESH;
+                    o.instance = h.lightIndex >> 24;
+                    o.primitive = h.lightIndex & 0xffffffu;
+                }
+            }
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "wfcuda_trace: %s\n", e.what());
+        return 3;
     }
 }
 
@@ -252,32 +389,8 @@ int wfcuda_render(void* handle, const wf_camera* cam, const wf_render_config* c,
     try {
         CudaRefScene* r = static_cast<CudaRefScene*>(handle);
         if (!r || spp == 0) return 1;
-        Camera camera;
-        camera.position = wfref::v3(cam->position);
-        camera.forward = wfref::v3(cam->forward);
-        camera.right = wfref::v3(cam->right);
-        camera.up = wfref::v3(cam->up);
-        camera.verticalFov = cam->vertical_fov;
-        camera.aspectRatio = cam->aspect_ratio;
-        RenderConfig config;
-        config.width = c->width;
-        config.height = c->height;
-        config.maxDepth = c->max_depth;
-        config.russianRouletteStartDepth = c->rr_start_depth;
-        config.samplesPerPixel = 1u << 30;  // bounds the absolute sample ranges of tasks
-        config.persistentWavefront = persistent != 0;
-        config.indirectRadianceClamp = c->indirect_clamp;
-        config.rngStrategy = RngStrategy(c->rng);
-        config.blockSize = 256;
-        // The Demo preset is not a caustic preset, so prepare() builds no
-        // photon map of its own; a caustic render gets the one built below.
-        config.enableCaustics = c->caustics != 0;
-        config.enableCausticGather = c->caustic_gather != 0;
-        config.causticPhotonCount = c->caustics ? c->photon_count : config.causticPhotonCount;
-        config.causticMaxDepth = c->photon_max_depth;
-        config.causticGatherRadius = c->gather_radius;
-        config.profileQueues = persistent && queue_counts != nullptr;
-        config.distributedRole = DistributedRole::Worker;  // no local checkpoint writer
+        Camera camera = reference_camera(cam);
+        RenderConfig config = reference_config(c, persistent, persistent && queue_counts != nullptr);
         SceneConfig scene_config;
         scene_config.preset = ScenePreset::Demo;
         RenderDriver driver(r->device, camera, config, scene_config);
@@ -303,6 +416,45 @@ int wfcuda_render(void* handle, const wf_camera* cam, const wf_render_config* c,
         return 0;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "wfcuda_render: %s\n", e.what());
+        return 3;
+    }
+}
+
+// The converged-image accumulator: renders `tasks` tasks of the tile
+// (x, y, w, h), each `spp` samples from sample_start + i * spp on, through
+// RenderTaskRenderer::render, and adds every task's FP32 sums into `sum`
+// (w * h * 3 doubles) on the host.  The driver, and with c->caustics its
+// photon map, is made once.
+int wfcuda_render_sum(void* handle, const wf_camera* cam, const wf_render_config* c, int persistent, uint32_t x,
+                      uint32_t y, uint32_t w, uint32_t h, uint32_t sample_start, uint32_t spp, uint32_t tasks,
+                      double* sum) {
+    try {
+        CudaRefScene* r = static_cast<CudaRefScene*>(handle);
+        if (!r || spp == 0 || !sum) return 1;
+        Camera camera = reference_camera(cam);
+        RenderConfig config = reference_config(c, persistent, false);
+        SceneConfig scene_config;
+        scene_config.preset = ScenePreset::Demo;
+        RenderDriver driver(r->device, camera, config, scene_config);
+        if (!driver.prepare()) return 4;
+        if (c->caustics) build_photon_map(driver, c);
+        RenderTaskRenderer renderer(driver);
+        RenderTask task;
+        task.jobFingerprint = computeRenderFingerprint(config, scene_config);
+        task.tile = DistributedTile{x, y, w, h};
+        for (uint32_t i = 0; i < tasks; ++i) {
+            task.id = RenderTaskId{0, sample_start + i * spp, spp};
+            RenderTaskResult result = renderer.render(task);
+            if (!result.success) return 2;
+            for (size_t k = 0; k < result.radiance.size(); ++k) {
+                sum[3 * k] += result.radiance[k].x;
+                sum[3 * k + 1] += result.radiance[k].y;
+                sum[3 * k + 2] += result.radiance[k].z;
+            }
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "wfcuda_render_sum: %s\n", e.what());
         return 3;
     }
 }

@@ -20,6 +20,7 @@ reference's exit-on-error cannot end the test session.  Skipped when the
 library has not been built.
 """
 import json
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -33,18 +34,27 @@ pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not LIB.exists(), reason="reference CUDA build absent (make -C oracle cuda)")]
 
 
-@pytest.mark.parametrize("workload,mode,caustics,tolerance", [
-    ("cornell", "graph", False, 0.01),
-    ("cornell", "persistent", False, 0.01),
-    ("large_mesh_small", "graph", False, 0.02),
-    ("large_mesh_small", "graph", True, 0.03),
+@pytest.mark.parametrize("workload,mode,caustics,tolerance,build", [
+    ("cornell", "graph", False, 0.01, "exact"),
+    ("cornell", "persistent", False, 0.01, "exact"),
+    ("large_mesh_small", "graph", False, 0.02, "exact"),
+    ("large_mesh_small", "graph", True, 0.03, "exact"),
+    ("cornell", "graph", False, 0.01, "fast"),
+    ("large_mesh_small", "graph", True, 0.03, "fast"),
 ])
-def test_image_matches_reference_cuda_renderer(cuda, workload, mode, caustics, tolerance):
+def test_image_matches_reference_cuda_renderer(cuda, workload, mode, caustics, tolerance, build):
+    """`build` fast: this renderer's fast build (libwavefront_b200_fast.so)."""
+    fast = ROOT / "wavefront-path-tracer_b200" / "libwavefront_b200_fast.so"
+    if build == "fast" and not fast.exists():
+        pytest.skip("fast build absent (make fast)")
     cmd = [sys.executable, str(ROOT / "oracle" / "ref_cuda_bench.py"), "--workload", workload, "--mode", mode,
            "--steps", "1"]
     if not caustics:
         cmd.append("--no-caustics")
-    run = subprocess.run(cmd, capture_output=True, text=True, timeout=900, cwd=ROOT)
+    env = dict(os.environ)
+    if build == "fast":
+        env["WF_BUILD"] = "fast"
+    run = subprocess.run(cmd, capture_output=True, text=True, timeout=900, cwd=ROOT, env=env)
     assert run.returncode == 0, run.stdout[-2000:] + run.stderr[-2000:]
     line = json.loads(run.stdout.strip().splitlines()[-1])
     ref = line["reference_cuda"][mode]

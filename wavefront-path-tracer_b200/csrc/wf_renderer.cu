@@ -96,22 +96,37 @@ __global__ void k_raygen_stream(RenderParams rp, const TileDev* tile_ptr, Counte
 // The per-ray visit order and arithmetic are the same either way.
 // The closest-hit stage of one bounce; the kernels below differ only in
 // their register bounds.
-// `start` (nullable): the stage covers queue entries [*start, *start +
-// *count) instead of [0, *count) -- the streaming loop's camera rays, queued
-// after the survivors and traced beside them by a second launch -- and then
-// takes its work from `work` and leaves the per-bounce resets to the launch
-// over the survivors.
+// `camera` (nullable, streaming mode): the number of camera rays of slots
+// that started a sample, queued after the *count survivors.  Two launches
+// share the bounce: when survivors exist, the lane-refill launch traces them
+// and the camera rays behind them (a warp that holds a long survivor keeps
+// refilling its other lanes with camera rays, which sit in runs of
+// neighbouring pixels), and the per-thread launch (kLanes false) has nothing
+// to do; when no path survived (the first pass, or a drained queue) the
+// per-thread launch traces the camera rays alone, taking its work from
+// `work`.  The lane-refill launch makes the per-bounce resets.
 template <typename Tally, bool kLanes>
 WF_DEV void trace_stage(const DeviceScene& s, PathSoA ps, const uint32_t* queue, const uint32_t* count, float4* hit_a,
                         uint32_t* hit_inst, Counters* c, uint32_t bounce, TallyTotals* totals, uint32_t refill_at,
-                        const uint32_t* start, uint32_t* work) {
+                        const uint32_t* camera, uint32_t* work) {
     count_launch(c);
     uint32_t n = *count;
-    uint32_t first = start ? *start : 0u;
-    uint32_t* counter = start ? work : &c->work_trace;
+    uint32_t* counter = &c->work_trace;
+    bool resets = true;
+    if (camera) {
+        uint32_t survivors = n, rays = *camera;
+        if constexpr (kLanes) {
+            n = survivors ? survivors + rays : 0u;
+        } else {
+            n = survivors ? 0u : rays;
+            counter = work;
+            resets = false;
+        }
+    }
+    constexpr uint32_t first = 0;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
-        if (!start) {
+        if (resets) {
             c->shadow_count = 0;
             c->gather_count = 0;
             c->dense_count = 0;
@@ -177,9 +192,9 @@ WF_DEV void trace_stage(const DeviceScene& s, PathSoA ps, const uint32_t* queue,
 template <typename Tally, bool kLanes = true>
 __global__ void __maxnreg__(72) k_trace(DeviceScene s, PathSoA ps, const uint32_t* queue, const uint32_t* count,
                                         float4* hit_a, uint32_t* hit_inst, Counters* c, uint32_t bounce,
-                                        TallyTotals* totals, uint32_t refill_at, const uint32_t* start,
+                                        TallyTotals* totals, uint32_t refill_at, const uint32_t* camera,
                                         uint32_t* work) {
-    trace_stage<Tally, kLanes>(s, ps, queue, count, hit_a, hit_inst, c, bounce, totals, refill_at, start, work);
+    trace_stage<Tally, kLanes>(s, ps, queue, count, hit_a, hit_inst, c, bounce, totals, refill_at, camera, work);
 }
 
 // Camera rays (one traversal per thread, coherent): bounded to 8 CTAs of 128
@@ -190,8 +205,8 @@ template <typename Tally>
 __global__ void __launch_bounds__(128, 8) k_trace_camera(DeviceScene s, PathSoA ps, const uint32_t* queue,
                                                          const uint32_t* count, float4* hit_a, uint32_t* hit_inst,
                                                          Counters* c, uint32_t bounce, TallyTotals* totals,
-                                                         uint32_t refill_at, const uint32_t* start, uint32_t* work) {
-    trace_stage<Tally, false>(s, ps, queue, count, hit_a, hit_inst, c, bounce, totals, refill_at, start, work);
+                                                         uint32_t refill_at, const uint32_t* camera, uint32_t* work) {
+    trace_stage<Tally, false>(s, ps, queue, count, hit_a, hit_inst, c, bounce, totals, refill_at, camera, work);
 }
 
 // Shading categories: warps of k_shade take entries of one category at a
@@ -1132,18 +1147,17 @@ wf_status capture_stream_graph(wf_renderer* r) {
         uint32_t nxt = cur ^ 1;
         uint32_t* cur_count = &r->counters->queue_count[cur];
         uint32_t* next_count = &r->counters->queue_count[nxt];
-        // The camera rays of slots that started a sample (queued after the
-        // survivors) one per thread on a branch, the survivors by lane refill.
-        WF_CUDA(cudaEventRecord(r->fork_event, st));
-        WF_CUDA(cudaStreamWaitEvent(r->side, r->fork_event, 0));
-        launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, r->side,
-            s, r->paths, r->queue[cur], &r->counters->camera_count[cur], r->hit_a, r->hit_inst, r->counters,
-            kMaxBounces, nullptr, r->refill, cur_count, &r->counters->work_camera);
-        WF_CUDA(cudaEventRecord(r->join_event, r->side));
+        // The survivors and the camera rays of slots that started a sample
+        // (see trace_stage): lane refill over both, or per thread over the
+        // camera rays when nothing survived.  The launch with nothing to do
+        // exits at once.
+        uint32_t* camera = &r->counters->camera_count[cur];
+        launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st,
+            s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, kMaxBounces, nullptr,
+            r->refill, camera, &r->counters->work_camera);
         launch_trace<NoTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st,
             s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, kMaxBounces, nullptr, r->refill,
-            nullptr, nullptr);
-        WF_CUDA(cudaStreamWaitEvent(st, r->join_event, 0));
+            camera, nullptr);
         k_merge_camera<<<1, 1, 0, st>>>(r->counters, cur);
         k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
                                                           r->counters);

@@ -52,8 +52,8 @@ struct Counters {
     uint32_t persistent_count[kMaxBounces + 1];
     uint32_t persistent_work[kMaxBounces + 1];
     // Streaming mode: camera rays of slots that started a new sample, queued
-    // after queue_count[q] survivors of queue q (traced per thread, then
-    // merged into the queue), and the camera-ray trace's work counter.
+    // after queue_count[q] survivors of queue q (merged into the queue once
+    // traced), and the work counter of the per-thread camera-ray trace.
     uint32_t camera_count[2];
     uint32_t work_camera;
     // Bounds of the device-side waits (wf_renderer_set_watchdog); 0 = default.

@@ -15,7 +15,11 @@ import numpy as np
 from . import abi
 
 PACKAGE_DIR = Path(__file__).resolve().parents[1]
-LIB_PATH = PACKAGE_DIR / "libwavefront_b200.so"
+# WF_BUILD=fast selects the fast build (multiply-adds contracted, CUDA's own
+# elementary functions: images within an RMSE of the reference instead of bit
+# for bit); the default is the bit-exact build.
+LIB_PATH = PACKAGE_DIR / ("libwavefront_b200_fast.so" if os.environ.get("WF_BUILD") == "fast"
+                          else "libwavefront_b200.so")
 _lib = None
 
 

@@ -151,13 +151,24 @@ def algorithmic_bytes(profile, kernel):
     return 48 * rays + 32 * nodes + 48 * tris + 16 * sph + 64 * inst
 
 
-def ncu_traffic(kernel, workload):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+def ncu_summary(kernel, workload):
+    """The committed ncu summary of `kernel` on `workload` (profiles/), or {}."""
     p = ROOT / "profiles" / f"{kernel}_{workload}.json"
-    if p.exists():
-        data = json.loads(p.read_text())
-        return data.get("dram_bytes_per_launch_full_size")
-    return None
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
+def l2_term(kernel, workload, rays_per_launch, avg_ms):
+    """L2 traffic of one launch from the ncu summary's L2 bytes per ray
+    (lts__t_bytes of a captured launch over its rays), scaled to this
+    launch's rays and divided by its live CUDA-event time."""
+    data = ncu_summary(kernel, workload)
+    per_ray = data.get("l2_bytes_per_ray")
+    if not per_ray or not rays_per_launch:
+        return None
+    b = per_ray * rays_per_launch
+    return {"bytes_per_launch": b, "achieved_gbs": b / (avg_ms / 1e3) / 1e9,
+            "ncu_l2_throughput_pct_of_peak": data.get("l2_throughput_pct"),
+            "ncu_l2_hit_rate_pct": data.get("l2_hit_rate_pct"), "source": data.get("l2_source")}
 
 
 def cpu_reference_rate(ref, cam, width, height, render_kwargs, seconds_target=15.0, threads=0):
@@ -617,9 +628,11 @@ def main():
         bytes_per_launch = algorithmic_bytes(profile, dominant) / launches
         peak, peak_kind = measured_peak()
         achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+        rays_key = "extension_rays" if dominant == "trace" else "shadow_rays"
         roofline = {"bound": "hbm", "kernel": f"k_{dominant}", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": peak_kind,
-                    "traffic": ncu_traffic(f"k_{dominant}", args.workload),
+                    "traffic": ncu_summary(f"k_{dominant}", args.workload).get("dram_bytes_per_launch_full_size"),
+                    "l2": l2_term(f"k_{dominant}", args.workload, profile[rays_key] / launches, avg_ms),
                     "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
                     "kernel_share": {k: v["ms"] / total_ms for k, v in kernels.items()}}
     else:

@@ -503,6 +503,36 @@ wf_status wf_render_tile_static(const wf_scene* scene, const wf_camera* camera,
                                 uint32_t width, uint32_t height, uint32_t sample_start,
                                 uint32_t sample_count, float* framebuffer, void* stream);
 
+/* Candidate settings of wf_renderer_autotune.  Each list comes with its
+ * length; a length of 0 keeps the base config's value.  Settings that a mode
+ * does not read are not varied for it (concurrent_tiles: graph mode only;
+ * regenerate_percents: streaming mode only; chunks: persistent mode only). */
+typedef struct wf_tune_space {
+    const uint32_t* modes;               uint32_t mode_count;               /* WF_MODE_* */
+    const uint32_t* block_sizes;         uint32_t block_size_count;         /* trace / shade CTA size */
+    const uint32_t* refill_thresholds;   uint32_t refill_threshold_count;   /* lane refill (1..32) */
+    const uint32_t* concurrent_tiles;    uint32_t concurrent_tiles_count;   /* wavefronts per tile */
+    const uint32_t* regenerate_percents; uint32_t regenerate_percent_count; /* streaming regeneration */
+    const uint32_t* chunks;              uint32_t chunk_count;              /* persistent work chunk */
+    const uint32_t* tile_sizes;          uint32_t tile_size_count;          /* square tile edge = queue
+                                                                               capacity; 0 = full frame */
+    uint32_t samples;  /* samples per pixel of each timed frame (0 = 1) */
+} wf_tune_space;
+
+/* Single-scene autotuner (no counterpart in the reference, whose block size
+ * and schedule are fixed settings of config.hpp).  For every combination of
+ * the candidate settings it creates a renderer from `base` (same scene,
+ * camera and image), renders one untimed frame of space->samples samples per
+ * pixel, then one timed frame (CUDA events on the renderer stream), and
+ * keeps the fastest.  `best` receives that config; times_ms[i] (optional,
+ * times_capacity entries) the frame time of candidate i in loop order
+ * (modes outermost, then block sizes, refill thresholds, tile sizes, and the
+ * mode's own setting); *evaluated the number of candidates.  All candidates
+ * render the same image, so the choice does not change any result. */
+wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, const wf_render_config* base,
+                               const wf_tune_space* space, void* stream, wf_render_config* best,
+                               float* times_ms, uint32_t times_capacity, uint32_t* evaluated);
+
 /* Kernel-level profile of one sample pass over the whole frame. */
 enum { WF_KERNEL_RAYGEN = 0, WF_KERNEL_TRACE = 1, WF_KERNEL_SHADE = 2, WF_KERNEL_SHADOW = 3,
        WF_KERNEL_FINALIZE = 4, WF_KERNEL_PERSISTENT = 5, WF_KERNEL_GATHER = 6, WF_KERNEL_KINDS = 7 };

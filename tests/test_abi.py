@@ -55,7 +55,7 @@ def test_struct_sizes_compiled_from_header(tmp_path):
              "wf_batch_job": abi.BatchJob, "wf_batch_config": abi.BatchConfig, "wf_scene_info": abi.SceneInfo,
              "wf_environment": abi.Environment, "wf_diff_config": abi.DiffConfig,
              "wf_frame_guide": abi.FRAME_GUIDE_DTYPE, "wf_hit": abi.HIT_DTYPE, "wf_ray": abi.RAY_DTYPE,
-             "wf_material_textures": abi.MATERIAL_TEXTURES_DTYPE}
+             "wf_material_textures": abi.MATERIAL_TEXTURES_DTYPE, "wf_tune_space": abi.TuneSpace}
     src = tmp_path / "sizes.c"
     body = "".join(f'    printf("%zu\\n", sizeof({name}));\n' for name in pairs)
     src.write_text('#include <stdio.h>\n#include "wavefront.h"\nint main(void) {\n' + body + "    return 0;\n}\n")

@@ -75,3 +75,24 @@ def test_static_entry_rejects_oversized_tiles_and_caustics(cuda):
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     finally:
         dev.close()
+
+
+@pytest.mark.parametrize("alpha", [True, False], ids=["alpha-textured", "textured-opaque"])
+def test_static_entry_textured_kernel_variants(cuda, alpha):
+    """The two other persistent-kernel variants the entry point picks per
+    scene: with the texture alpha test (an alpha-masked, albedo-textured
+    card) and with textures but no alpha test (the same room with alpha
+    masking turned off).  Two calls in a row, each against wf_render."""
+    scene, cam = scenes.textured_room(64, 64)
+    if not alpha:
+        scene.materials["alpha_masked"] = 0
+    cfg = wfpt.render_config(64, 64, max_depth=6, rr_start_depth=3, mode=abi.MODE_PERSISTENT)
+    dev = wfpt.DeviceScene(scene)
+    try:
+        for tile, start, count in (((0, 0, 64, 64), 40, 2), ((8, 16, 48, 40), 3, 1)):
+            want = _reference_tile(dev, cam, cfg, tile, start, count)
+            got = _static_tile(cuda, dev, cam, cfg, tile, start, count)
+            assert got.mean() > 0
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    finally:
+        dev.close()

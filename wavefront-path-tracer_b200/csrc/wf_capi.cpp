@@ -350,6 +350,76 @@ wf_status wf_render_frame(wf_renderer* r, uint32_t sample_count) {
     return renderer_render_frame(r, sample_count);
 }
 
+wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, const wf_render_config* base,
+                               const wf_tune_space* space, void* stream, wf_render_config* best, float* times_ms,
+                               uint32_t times_capacity, uint32_t* evaluated) {
+    if (!scene || !camera || !base || !space || !best) return fail(WF_ERR_INVALID_ARG, "null argument");
+    auto values = [](const uint32_t* list, uint32_t count, uint32_t keep) {
+        std::vector<uint32_t> v;
+        for (uint32_t i = 0; list && i < count; ++i) v.push_back(list[i]);
+        if (v.empty()) v.push_back(keep);
+        return v;
+    };
+    std::vector<uint32_t> modes = values(space->modes, space->mode_count, base->mode);
+    std::vector<uint32_t> blocks = values(space->block_sizes, space->block_size_count, base->block_size);
+    std::vector<uint32_t> refills =
+        values(space->refill_thresholds, space->refill_threshold_count, base->refill_threshold);
+    std::vector<uint32_t> tiles = values(space->tile_sizes, space->tile_size_count,
+                                         base->tile_width == base->tile_height ? base->tile_width : 0u);
+    uint32_t samples = space->samples ? space->samples : 1u;
+    uint32_t count = 0;
+    float best_ms = 0.0f;
+    for (uint32_t mode : modes) {
+        std::vector<uint32_t> own = mode == WF_MODE_GRAPH
+                                        ? values(space->concurrent_tiles, space->concurrent_tiles_count,
+                                                 base->concurrent_tiles)
+                                    : mode == WF_MODE_STREAM
+                                        ? values(space->regenerate_percents, space->regenerate_percent_count,
+                                                 base->regenerate_percent)
+                                        : values(space->chunks, space->chunk_count, base->chunk);
+        for (uint32_t block : blocks)
+            for (uint32_t refill : refills)
+                for (uint32_t tile : tiles)
+                    for (uint32_t setting : own) {
+                        wf_render_config c = *base;
+                        c.mode = mode;
+                        c.block_size = block;
+                        c.refill_threshold = refill;
+                        c.tile_width = c.tile_height = tile;
+                        if (mode == WF_MODE_GRAPH) c.concurrent_tiles = setting;
+                        else if (mode == WF_MODE_STREAM) c.regenerate_percent = setting;
+                        else c.chunk = setting;
+                        wf_renderer* r = nullptr;
+                        if (wf_status e = renderer_create(scene, camera, &c, stream, &r)) return e;
+                        cudaEvent_t e0 = nullptr, e1 = nullptr;
+                        float ms = 0.0f;
+                        wf_status st = renderer_render_frame(r, samples);
+                        cudaError_t err = cudaSuccess;
+                        if (st == WF_OK) err = cudaEventCreate(&e0);
+                        if (st == WF_OK && err == cudaSuccess) err = cudaEventCreate(&e1);
+                        if (st == WF_OK && err == cudaSuccess) err = cudaEventRecord(e0, r->stream);
+                        if (st == WF_OK && err == cudaSuccess) st = renderer_render_frame(r, samples);
+                        if (st == WF_OK && err == cudaSuccess) err = cudaEventRecord(e1, r->stream);
+                        if (st == WF_OK && err == cudaSuccess) err = cudaEventSynchronize(e1);
+                        if (st == WF_OK && err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+                        if (st == WF_OK && err == cudaSuccess) st = wf_synchronize(r);
+                        if (e0) cudaEventDestroy(e0);
+                        if (e1) cudaEventDestroy(e1);
+                        renderer_destroy(r);
+                        if (st != WF_OK) return st;
+                        if (err != cudaSuccess) return cuda_fail(err, "autotune timing");
+                        if (times_ms && count < times_capacity) times_ms[count] = ms;
+                        if (count == 0 || ms < best_ms) {
+                            best_ms = ms;
+                            *best = c;
+                        }
+                        ++count;
+                    }
+    }
+    if (evaluated) *evaluated = count;
+    return WF_OK;
+}
+
 wf_status wf_profile_sample(wf_renderer* r, wf_kernel_profile* profile) {
     if (!r || !profile) return fail(WF_ERR_INVALID_ARG, "null argument");
     return renderer_profile(r, profile);

@@ -39,9 +39,7 @@ wf_status cuda_fail(cudaError_t e, const char* what) {
 
 namespace {
 
-__global__ void k_raygen(RenderParams rp, const TileDev* tile_ptr, Counters* c, PathSoA ps, uint32_t* queue,
-                         uint32_t capacity) {
-    count_launch(c);
+WF_DEV void raygen_stage(RenderParams rp, const TileDev* tile_ptr, Counters* c, PathSoA ps, uint32_t* queue, uint32_t capacity) {
     TileDev tile = *tile_ptr;
     uint32_t n = min(tile.width * tile.height, capacity);
     uint32_t sample = c->sample_index;
@@ -58,6 +56,12 @@ __global__ void k_raygen(RenderParams rp, const TileDev* tile_ptr, Counters* c, 
         ps.radiance[lp] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         queue[lp] = lp;
     }
+}
+
+__global__ void k_raygen(RenderParams rp, const TileDev* tile_ptr, Counters* c, PathSoA ps, uint32_t* queue,
+                         uint32_t capacity) {
+    count_launch(c);
+    raygen_stage(rp, tile_ptr, c, ps, queue, capacity);
 }
 
 // Streaming mode: every slot (= pixel of the tile) starts the launch's first
@@ -240,9 +244,7 @@ WF_DEV uint32_t shade_category(const DeviceScene& s, float4 ha, uint32_t inst) {
     }
 }
 
-__global__ void k_classify(const __grid_constant__ DeviceScene s, const uint32_t* count, const float4* hit_a,
-                           const uint32_t* hit_inst, uint8_t* key, Counters* c) {
-    count_launch(c);
+WF_DEV void classify_stage(const DeviceScene& s, const uint32_t* count, const float4* hit_a, const uint32_t* hit_inst, uint8_t* key, Counters* c) {
     __shared__ uint32_t histogram[kShadeCategories];
     if (threadIdx.x < kShadeCategories) histogram[threadIdx.x] = 0;
     __syncthreads();
@@ -257,10 +259,15 @@ __global__ void k_classify(const __grid_constant__ DeviceScene s, const uint32_t
         atomicAdd(&c->shade_bucket[threadIdx.x], histogram[threadIdx.x]);
 }
 
+__global__ void k_classify(const __grid_constant__ DeviceScene s, const uint32_t* count, const float4* hit_a,
+                           const uint32_t* hit_inst, uint8_t* key, Counters* c) {
+    count_launch(c);
+    classify_stage(s, count, hit_a, hit_inst, key, c);
+}
+
 // Counting-sort scatter: within a warp, entries of one category keep their
 // order (ballot rank); warps reserve runs of each bucket with one atomic.
-__global__ void k_scatter(const uint32_t* count, const uint8_t* key, uint32_t* order, Counters* c) {
-    count_launch(c);
+WF_DEV void scatter_stage(const uint32_t* count, const uint8_t* key, uint32_t* order, Counters* c) {
     uint32_t n = *count;
     uint32_t offset[kShadeCategories];
     uint32_t run = 0;
@@ -282,13 +289,14 @@ __global__ void k_scatter(const uint32_t* count, const uint8_t* key, uint32_t* o
     }
 }
 
+__global__ void k_scatter(const uint32_t* count, const uint8_t* key, uint32_t* order, Counters* c) {
+    count_launch(c);
+    scatter_stage(count, key, order, c);
+}
+
 // 128 registers: 4 CTAs per SM; the few spills cost less than the lost warps.
 template <bool kTextures>
-__global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ RenderParams rp, PathSoA ps, const uint32_t* queue, const uint32_t* count,
-                        const float4* hit_a, const uint32_t* hit_inst, float4* terms, int4* shade_out,
-                        float4* shadow_origin, float4* shadow_dir, uint32_t shadow_capacity, Counters* c,
-                        uint32_t* next_count, GatherQueue gathers, const uint32_t* order) {
-    count_launch(c);
+WF_DEV void shade_stage(const DeviceScene& s, const RenderParams& rp, PathSoA ps, const uint32_t* queue, const uint32_t* count, const float4* hit_a, const uint32_t* hit_inst, float4* terms, int4* shade_out, float4* shadow_origin, float4* shadow_dir, uint32_t shadow_capacity, Counters* c, uint32_t* next_count, GatherQueue gathers, const uint32_t* order) {
     uint32_t n = *count;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
@@ -327,6 +335,15 @@ __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ Device
     }
 }
 
+template <bool kTextures>
+__global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ RenderParams rp, PathSoA ps, const uint32_t* queue, const uint32_t* count,
+                        const float4* hit_a, const uint32_t* hit_inst, float4* terms, int4* shade_out,
+                        float4* shadow_origin, float4* shadow_dir, uint32_t shadow_capacity, Counters* c,
+                        uint32_t* next_count, GatherQueue gathers, const uint32_t* order) {
+    count_launch(c);
+    shade_stage<kTextures>(s, rp, ps, queue, count, hit_a, hit_inst, terms, shade_out, shadow_origin, shadow_dir, shadow_capacity, c, next_count, gathers, order);
+}
+
 // Caustic gathers queued by k_shade (gatherCaustics, photon_mapping.cu:91-163),
 // written into the term slots their paths reserved.  A request whose cells
 // hold many photons (near a caustic) would scan them serially while the rest
@@ -341,8 +358,7 @@ WF_DEV void write_gather_term(const RenderParams& rp, const GatherQueue& q, floa
     terms[__float_as_uint(pos.w)] = make_float4(col.x, col.y, col.z, __int_as_float(kUnconditional));
 }
 
-__global__ void k_gather(const __grid_constant__ RenderParams rp, GatherQueue q, float4* terms, Counters* c) {
-    count_launch(c);
+WF_DEV void gather_stage(const RenderParams& rp, GatherQueue q, float4* terms, Counters* c) {
     uint32_t n = min(*q.count, q.capacity);
     uint32_t base;
     while (next_chunk(&c->work_gather, n, base)) {
@@ -360,8 +376,12 @@ __global__ void k_gather(const __grid_constant__ RenderParams rp, GatherQueue q,
     }
 }
 
-__global__ void k_gather_dense(const __grid_constant__ RenderParams rp, GatherQueue q, float4* terms, Counters* c) {
+__global__ void k_gather(const __grid_constant__ RenderParams rp, GatherQueue q, float4* terms, Counters* c) {
     count_launch(c);
+    gather_stage(rp, q, terms, c);
+}
+
+WF_DEV void gather_dense_stage(const RenderParams& rp, GatherQueue q, float4* terms, Counters* c) {
     uint32_t n = min(*q.dense_count, q.capacity);
     uint32_t lane = threadIdx.x & 31;
     for (;;) {
@@ -376,10 +396,13 @@ __global__ void k_gather_dense(const __grid_constant__ RenderParams rp, GatherQu
     }
 }
 
-template <typename Tally>
-__global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float4* shadow_dir, uint8_t* result,
-                         Counters* c, uint32_t capacity, TallyTotals* totals, uint32_t refill_at) {
+__global__ void k_gather_dense(const __grid_constant__ RenderParams rp, GatherQueue q, float4* terms, Counters* c) {
     count_launch(c);
+    gather_dense_stage(rp, q, terms, c);
+}
+
+template <typename Tally>
+WF_DEV void shadow_stage(DeviceScene s, const float4* shadow_origin, const float4* shadow_dir, uint8_t* result, Counters* c, uint32_t capacity, TallyTotals* totals, uint32_t refill_at) {
     uint32_t n = min(c->shadow_count, capacity);
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) c->shadow_rays += n;
@@ -410,6 +433,13 @@ __global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float
     if constexpr (Tally::kCounts) flush_tally(tally, totals);
 }
 
+template <typename Tally>
+__global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float4* shadow_dir, uint8_t* result,
+                         Counters* c, uint32_t capacity, TallyTotals* totals, uint32_t refill_at) {
+    count_launch(c);
+    shadow_stage<Tally>(s, shadow_origin, shadow_dir, result, c, capacity, totals, refill_at);
+}
+
 // Adds each path's accepted terms in emission order, applies the kill rule,
 // adds ended paths to the framebuffer and compacts survivors into `next`
 // (appendWarpCompacted, queue_compaction.cuh:8-29).  With kRegenerate (the
@@ -417,11 +447,7 @@ __global__ void k_shadow(DeviceScene s, const float4* shadow_origin, const float
 // sample (k_regenerate); the framebuffer add comes first, so every pixel
 // still accumulates its samples in sample order.
 template <bool kRegenerate>
-__global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* count, const float4* terms,
-                           const int4* shade_out, const uint8_t* shadow_result, uint32_t* next, uint32_t* next_count,
-                           uint32_t capacity, float* framebuffer, uint32_t* work_trace, RenderParams rp,
-                           const TileDev* tile_ptr, Counters* c) {
-    count_launch(c);
+WF_DEV void finalize_stage(PathSoA ps, const uint32_t* queue, const uint32_t* count, const float4* terms, const int4* shade_out, const uint8_t* shadow_result, uint32_t* next, uint32_t* next_count, uint32_t capacity, float* framebuffer, uint32_t* work_trace, RenderParams rp, const TileDev* tile_ptr, Counters* c) {
     uint32_t n = *count;
     uint32_t lane = threadIdx.x & 31;
     uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -463,6 +489,15 @@ __global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* co
         uint32_t rank = __popc(mask & ((1u << lane) - 1u));
         if (alive && out + rank < capacity) next[out + rank] = p;
     }
+}
+
+template <bool kRegenerate>
+__global__ void k_finalize(PathSoA ps, const uint32_t* queue, const uint32_t* count, const float4* terms,
+                           const int4* shade_out, const uint8_t* shadow_result, uint32_t* next, uint32_t* next_count,
+                           uint32_t capacity, float* framebuffer, uint32_t* work_trace, RenderParams rp,
+                           const TileDev* tile_ptr, Counters* c) {
+    count_launch(c);
+    finalize_stage<kRegenerate>(ps, queue, count, terms, shade_out, shadow_result, next, next_count, capacity, framebuffer, work_trace, rp, tile_ptr, c);
 }
 
 // Streaming loop condition: run the body again while paths remain.  Each
@@ -670,6 +705,127 @@ const void* persistent_kernel(bool opaque, bool textured) {
     if (!opaque) return reinterpret_cast<const void*>(k_persistent<NoTally, true>);
     return textured ? reinterpret_cast<const void*>(k_persistent<Opaque<NoTally>, true>)
                     : reinterpret_cast<const void*>(k_persistent<Opaque<NoTally>, false>);
+}
+
+// The phased persistent kernel (WF_MODE_PERSISTENT renderers): one
+// cooperative launch renders one sample of a tile, running the wavefront
+// stages -- camera rays, closest hit (per thread at bounce 0, lane refill
+// after), material classification and sort, shading with deferred shadow
+// rays and caustic gathers, any-hit shadow rays, ordered finalize -- one
+// after another over the whole grid, with a bounded grid barrier between
+// stages.  The reference's persistent kernel (persistentWavefrontTrace,
+// renderer.cu:55-125) instead traces, shades and tests the shadow rays of
+// one path in a single fused body; fused, that body needs ~244 registers,
+// and bounded for occupancy it spills ~1.6 KB per thread.  Staged, every
+// path still sees the same arithmetic in the same order (the stages are
+// those of the captured graph), so the sums are unchanged.
+struct PhasedBuffers {
+    PathSoA ps;
+    uint32_t* queue[2];
+    float4* hit_a;
+    uint32_t* hit_inst;
+    float4* terms;
+    int4* shade_out;
+    float4* shadow_origin;
+    float4* shadow_dir;
+    uint8_t* shadow_result;
+    uint32_t shadow_capacity;
+    uint8_t* shade_key;
+    uint32_t* shade_order;
+    GatherQueue gathers;
+    float* framebuffer;
+    uint32_t capacity;
+    uint32_t refill;
+};
+
+// Each stage is an out-of-line call, so the register allocator sees one
+// stage at a time instead of every stage's live ranges at once.
+#define WF_STAGE static __device__ __noinline__
+template <typename Tally, bool kLanes>
+WF_STAGE void phased_trace(const DeviceScene& s, const PhasedBuffers& b, uint32_t cur, Counters* c, uint32_t bounce) {
+    trace_stage<Tally, kLanes>(s, b.ps, b.queue[cur], &c->queue_count[cur], b.hit_a, b.hit_inst, c, bounce, nullptr,
+                               b.refill, nullptr, nullptr);
+}
+WF_STAGE void phased_classify(const DeviceScene& s, const PhasedBuffers& b, uint32_t cur, Counters* c) {
+    classify_stage(s, &c->queue_count[cur], b.hit_a, b.hit_inst, b.shade_key, c);
+}
+WF_STAGE void phased_scatter(const PhasedBuffers& b, uint32_t cur, Counters* c) {
+    scatter_stage(&c->queue_count[cur], b.shade_key, b.shade_order, c);
+}
+template <bool kTextures>
+WF_STAGE void phased_shade(const DeviceScene& s, const RenderParams& rp, const PhasedBuffers& b, uint32_t cur,
+                           Counters* c) {
+    shade_stage<kTextures>(s, rp, b.ps, b.queue[cur], &c->queue_count[cur], b.hit_a, b.hit_inst, b.terms,
+                           b.shade_out, b.shadow_origin, b.shadow_dir, b.shadow_capacity, c,
+                           &c->queue_count[cur ^ 1], b.gathers, b.shade_order);
+}
+WF_STAGE void phased_gather(const RenderParams& rp, const PhasedBuffers& b, Counters* c, bool dense) {
+    if (dense)
+        gather_dense_stage(rp, b.gathers, b.terms, c);
+    else
+        gather_stage(rp, b.gathers, b.terms, c);
+}
+template <typename Tally>
+WF_STAGE void phased_shadow(const DeviceScene& s, const PhasedBuffers& b, Counters* c) {
+    shadow_stage<Tally>(s, b.shadow_origin, b.shadow_dir, b.shadow_result, c, b.shadow_capacity, nullptr, b.refill);
+}
+WF_STAGE void phased_finalize(const RenderParams& rp, const PhasedBuffers& b, uint32_t cur, Counters* c,
+                              const TileDev* tile_ptr) {
+    finalize_stage<false>(b.ps, b.queue[cur], &c->queue_count[cur], b.terms, b.shade_out, b.shadow_result,
+                          b.queue[cur ^ 1], &c->queue_count[cur ^ 1], b.capacity, b.framebuffer, &c->work_trace, rp,
+                          tile_ptr, c);
+}
+
+// CTAs of 128 per SM the phased kernel is bounded to (registers per thread
+// = 65536 / (128 x this)); a build setting (make PHASED_CTAS=n).
+#ifndef WF_PHASED_CTAS
+#define WF_PHASED_CTAS 6
+#endif
+template <typename Tally, bool kTextures>
+__global__ void __launch_bounds__(128, WF_PHASED_CTAS) k_persistent_phased(const __grid_constant__ DeviceScene s,
+                                                           const __grid_constant__ RenderParams rp,
+                                                           const TileDev* tile_ptr, Counters* c,
+                                                           const __grid_constant__ PhasedBuffers b) {
+    count_launch(c);
+    uint32_t blocks = gridDim.x;
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    raygen_stage(rp, tile_ptr, c, b.ps, b.queue[0], b.capacity);
+    if (!grid_barrier(c, blocks)) return;
+    uint32_t depth = min(rp.max_depth, uint32_t(kMaxBounces));
+    for (uint32_t bounce = 0; bounce < depth; ++bounce) {
+        uint32_t cur = bounce & 1;
+        if (*(volatile uint32_t*)&c->queue_count[cur] == 0) {  // every path ended: the rest are empty
+            if (gid == 0)
+                for (uint32_t r = bounce; r < depth; ++r) c->profile[r] = 0;
+            break;
+        }
+        if (bounce == 0)
+            phased_trace<Tally, false>(s, b, cur, c, bounce);
+        else
+            phased_trace<Tally, true>(s, b, cur, c, bounce);
+        if (!grid_barrier(c, blocks)) return;
+        phased_classify(s, b, cur, c);
+        if (!grid_barrier(c, blocks)) return;
+        phased_scatter(b, cur, c);
+        if (!grid_barrier(c, blocks)) return;
+        phased_shade<kTextures>(s, rp, b, cur, c);
+        if (!grid_barrier(c, blocks)) return;
+        if (rp.photons.enabled) {
+            phased_gather(rp, b, c, false);
+            if (!grid_barrier(c, blocks)) return;
+            phased_gather(rp, b, c, true);
+        }
+        phased_shadow<Tally>(s, b, c);
+        if (!grid_barrier(c, blocks)) return;
+        phased_finalize(rp, b, cur, c, tile_ptr);
+        if (!grid_barrier(c, blocks)) return;
+    }
+}
+
+const void* phased_kernel(bool opaque, bool textured) {
+    if (!opaque) return reinterpret_cast<const void*>(k_persistent_phased<NoTally, true>);
+    return textured ? reinterpret_cast<const void*>(k_persistent_phased<Opaque<NoTally>, true>)
+                    : reinterpret_cast<const void*>(k_persistent_phased<Opaque<NoTally>, false>);
 }
 
 // ---------------------------------------------------------------- batch API
@@ -1209,6 +1365,40 @@ uint32_t persistent_grid(uint32_t configured, uint32_t resident, uint32_t sm_cou
     return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(wanted, resident)));
 }
 
+// One cooperative launch of the phased persistent kernel over `paths`
+// paths of the current tile (the tile record is already on the device).
+cudaError_t launch_phased(wf_renderer* r, cudaStream_t st, uint64_t paths) {
+    cudaError_t e = cudaMemsetAsync(&r->counters->barrier_count, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    DeviceScene s = r->scene->view;
+    RenderParams rp = r->params;
+    const TileDev* tp = r->tile;
+    Counters* c = r->counters;
+    PhasedBuffers b{};
+    b.ps = r->paths;
+    b.queue[0] = r->queue[0];
+    b.queue[1] = r->queue[1];
+    b.hit_a = r->hit_a;
+    b.hit_inst = r->hit_inst;
+    b.terms = r->terms;
+    b.shade_out = r->shade_out;
+    b.shadow_origin = r->shadow_origin;
+    b.shadow_dir = r->shadow_dir;
+    b.shadow_result = r->shadow_result;
+    b.shadow_capacity = r->shadow_capacity;
+    b.shade_key = r->shade_key;
+    b.shade_order = r->shade_order;
+    b.gathers = r->gathers;
+    b.framebuffer = r->framebuffer;
+    b.capacity = r->capacity;
+    b.refill = r->refill;
+    void* args[] = {&s, &rp, &tp, &c, &b};
+    uint32_t blocks = persistent_grid(r->config.persistent_blocks, r->persistent_blocks, r->sm_count,
+                                      std::min<uint64_t>(paths, r->capacity));
+    return cudaLaunchCooperativeKernel(phased_kernel(r->opaque, r->textured), dim3(blocks),
+                                       dim3(r->persistent_block_size), args, 0, st);
+}
+
 wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
     WF_CUDA(cudaMemcpyAsync(r->tile, &tile, sizeof(TileDev), cudaMemcpyHostToDevice, r->stream));
     r->last_tile_width = tile.width;
@@ -1217,23 +1407,7 @@ wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
         WF_CUDA(cudaGraphLaunch(r->graph_exec, r->stream));
         return WF_OK;
     }
-    WF_CUDA(cudaMemsetAsync(r->counters->persistent_count, 0, sizeof(uint32_t) * 2 * (kMaxBounces + 1), r->stream));
-    WF_CUDA(cudaMemsetAsync(&r->counters->barrier_count, 0, sizeof(uint32_t), r->stream));
-    DeviceScene s = r->scene->view;
-    RenderParams rp = r->params;
-    const TileDev* tp = r->tile;
-    Counters* c = r->counters;
-    PathSoA ps = r->paths;
-    uint32_t* q0 = r->queue[0];
-    uint32_t* q1 = r->queue[1];
-    uint32_t cap = r->capacity;
-    float* fb = r->framebuffer;
-    uint32_t chunk = r->chunk;
-    void* args[] = {&s, &rp, &tp, &c, &ps, &q0, &q1, &cap, &fb, &chunk};
-    uint32_t blocks = persistent_grid(r->config.persistent_blocks, r->persistent_blocks, r->sm_count,
-                                      std::min<uint64_t>(uint64_t(tile.width) * tile.height, r->capacity));
-    WF_CUDA(cudaLaunchCooperativeKernel(persistent_kernel(r->opaque, r->textured), dim3(blocks),
-                                        dim3(r->persistent_block_size), args, 0, r->stream));
+    WF_CUDA(launch_phased(r, r->stream, uint64_t(tile.width) * tile.height));
     k_advance<<<1, 1, 0, r->stream>>>(r->counters, r->tile);
     WF_CUDA(cudaGetLastError());
     return WF_OK;
@@ -1337,7 +1511,7 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
         WF_CUDA(alloc(rr, &r->framebuffer, size_t(pixels) * 3));
         WF_CUDA(cudaMemsetAsync(r->framebuffer, 0, sizeof(float) * 3 * size_t(pixels), r->stream));
     }
-    if (c.mode != WF_MODE_PERSISTENT) {
+    {  // stage buffers: every schedule runs the wavefront stages
         uint32_t requests_per_path = 5u + scene->view.directional_count;
         uint64_t shadow = uint64_t(cap) * requests_per_path;
         if (c.shadow_queue_capacity && c.shadow_queue_capacity < shadow) shadow = c.shadow_queue_capacity;
@@ -1367,6 +1541,8 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
             r->gathers.dense_count = &r->counters->dense_count;
             WF_CUDA(resident_grid(rr, 4, k_gather, r->block_gather));
         }
+    }
+    if (c.mode != WF_MODE_PERSISTENT) {
         WF_CUDA(r->opaque ? resident_grid(rr, 0, k_trace<Opaque<NoTally>>, r->block_trace)
                           : resident_grid(rr, 0, k_trace<NoTally>, r->block_trace));
         WF_CUDA(r->opaque ? resident_grid(rr, 5, k_trace_camera<Opaque<NoTally>>, r->block_trace)
@@ -1382,7 +1558,7 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
         if (!cooperative) return fail(WF_ERR_UNSUPPORTED, "device does not support cooperative launches");
         r->persistent_block_size = 128;
         int per_sm = 0;
-        WF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel(r->opaque, r->textured),
+        WF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, phased_kernel(r->opaque, r->textured),
                                                               int(r->persistent_block_size), 0));
         if (per_sm <= 0) return fail(WF_ERR_UNSUPPORTED, "the persistent kernel cannot be resident");
         uint32_t resident = uint32_t(per_sm) * uint32_t(r->sm_count);
@@ -1622,28 +1798,9 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
     if (r->config.mode == WF_MODE_PERSISTENT) {
         for (const TileDev& tile : tiles) {
             WF_CUDA(cudaMemcpyAsync(r->tile, &tile, sizeof(TileDev), cudaMemcpyHostToDevice, st));
-            WF_CUDA(cudaMemsetAsync(r->counters->persistent_count, 0, sizeof(uint32_t) * 2 * (kMaxBounces + 1), st));
-            WF_CUDA(cudaMemsetAsync(&r->counters->barrier_count, 0, sizeof(uint32_t), st));
-            DeviceScene s = r->scene->view;
-            RenderParams rp = r->params;
-            const TileDev* tp = r->tile;
-            Counters* c = r->counters;
-            PathSoA ps = r->paths;
-            uint32_t *q0 = r->queue[0], *q1 = r->queue[1];
-            uint32_t cap = r->capacity;
-            float* fb = r->framebuffer;
-            uint32_t chunk = r->chunk;
-            void* args[] = {&s, &rp, &tp, &c, &ps, &q0, &q1, &cap, &fb, &chunk};
             cudaError_t launch_error = cudaSuccess;
             if (wf_status e = timed(WF_KERNEL_PERSISTENT, [&] {
-                    launch_error = cudaLaunchCooperativeKernel(persistent_kernel(r->opaque, r->textured),
-                                                               dim3(persistent_grid(
-                                                                   r->config.persistent_blocks, r->persistent_blocks,
-                                                                   r->sm_count,
-                                                                   std::min<uint64_t>(uint64_t(r->last_tile_width) *
-                                                                                          r->last_tile_height,
-                                                                                      r->capacity))),
-                                                               dim3(r->persistent_block_size), args, 0, st);
+                    launch_error = launch_phased(r, st, uint64_t(tile.width) * tile.height);
                 }))
                 return e;
             WF_CUDA(launch_error);

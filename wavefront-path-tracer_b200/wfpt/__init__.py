@@ -6,8 +6,8 @@ that ABI.  See native.py for the entry points and scenes.py for the
 synthetic workloads.
 """
 from . import abi
-from .native import (Batch, DeviceScene, Renderer, Scene, WavefrontError, camera_struct, check, library, material,
-                     render_config)
+from .native import (Batch, DeviceScene, Renderer, Scene, WavefrontError, autotune, camera_struct, check, library,
+                     material, render_config)
 
-__all__ = ["abi", "Batch", "DeviceScene", "Renderer", "Scene", "WavefrontError", "camera_struct", "check", "library",
-           "material", "render_config"]
+__all__ = ["abi", "Batch", "DeviceScene", "Renderer", "Scene", "WavefrontError", "autotune", "camera_struct", "check",
+           "library", "material", "render_config"]

@@ -146,6 +146,17 @@ class RenderConfig(C.Structure):
     ]
 
 
+class TuneSpace(C.Structure):
+    _fields_ = [("modes", C.c_void_p), ("mode_count", C.c_uint32),
+                ("block_sizes", C.c_void_p), ("block_size_count", C.c_uint32),
+                ("refill_thresholds", C.c_void_p), ("refill_threshold_count", C.c_uint32),
+                ("concurrent_tiles", C.c_void_p), ("concurrent_tiles_count", C.c_uint32),
+                ("regenerate_percents", C.c_void_p), ("regenerate_percent_count", C.c_uint32),
+                ("chunks", C.c_void_p), ("chunk_count", C.c_uint32),
+                ("tile_sizes", C.c_void_p), ("tile_size_count", C.c_uint32),
+                ("samples", C.c_uint32)]
+
+
 class BatchJob(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("camera", Camera), ("config", RenderConfig),
                 ("sample_start", C.c_uint32), ("sample_count", C.c_uint32)]
@@ -207,6 +218,8 @@ def declare(lib):
         "wf_render_frame": (S, [P, U32]),
         "wf_diff_forward": (S, [P, C.POINTER(Camera), C.POINTER(DiffConfig), P, P, F, P, P]),
         "wf_diff_backward": (S, [P, C.POINTER(Camera), C.POINTER(DiffConfig), P, P, F, P, P, P, P, P]),
+        "wf_renderer_autotune": (S, [P, C.POINTER(Camera), C.POINTER(RenderConfig), C.POINTER(TuneSpace), P,
+                                     C.POINTER(RenderConfig), P, U32, C.POINTER(U32)]),
         "wf_batch_config_default": (None, [C.POINTER(BatchConfig)]),
         "wf_batch_create": (S, [C.POINTER(BatchJob), U32, C.POINTER(BatchConfig), P, C.POINTER(P)]),
         "wf_batch_run": (S, [P]),

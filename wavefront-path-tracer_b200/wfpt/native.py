@@ -414,6 +414,87 @@ class Renderer:
         return s.value
 
 
+_TUNED = {}
+
+
+def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREAM), block_sizes=(128,),
+             refill_thresholds=(4, 8, 16), concurrent_tiles=(1, 2), regenerate_percents=(10, 25),
+             chunks=(), tile_sizes=(), samples=1, stream=None, key=None, cache_path=None):
+    """wf_renderer_autotune: times one frame per candidate setting and
+    returns (best RenderConfig, [(candidate settings, ms), ...]).
+
+    The choice is cached for the process under `key` (default: the scene
+    handle, camera, base config and candidate lists) and, with `cache_path`,
+    in that JSON file, so a later call with the same key returns the stored
+    settings without rendering (the table is then empty)."""
+    import json
+    fields = ("mode", "block_size", "refill_threshold", "tile_width", "tile_height", "concurrent_tiles",
+              "regenerate_percent", "chunk")
+    if key is None:
+        key = repr((device_scene.handle.value, sorted((k, tuple(v) if hasattr(v, "__len__") else v)
+                                                      for k, v in camera.items()),
+                    bytes(config), modes, block_sizes, refill_thresholds, concurrent_tiles, regenerate_percents,
+                    chunks, tile_sizes, samples))
+    stored = _TUNED.get(key)
+    if stored is None and cache_path is not None and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            stored = json.load(f).get(key)
+    if stored is not None:
+        best = abi.RenderConfig.from_buffer_copy(bytes(config))
+        for k in fields:
+            setattr(best, k, stored[k])
+        return best, []
+
+    def arr(v):
+        a = (C.c_uint32 * max(1, len(v)))(*v)
+        return a, len(v)
+    lists = {}
+    space = abi.TuneSpace()
+    for name, vals in (("modes", modes), ("block_sizes", block_sizes), ("refill_thresholds", refill_thresholds),
+                       ("concurrent_tiles", concurrent_tiles), ("regenerate_percents", regenerate_percents),
+                       ("chunks", chunks), ("tile_sizes", tile_sizes)):
+        a, n = arr(list(vals))
+        lists[name] = a
+        setattr(space, name, C.cast(a, C.c_void_p))
+        count_field = {"modes": "mode_count", "block_sizes": "block_size_count",
+                       "refill_thresholds": "refill_threshold_count", "concurrent_tiles": "concurrent_tiles_count",
+                       "regenerate_percents": "regenerate_percent_count", "chunks": "chunk_count",
+                       "tile_sizes": "tile_size_count"}[name]
+        setattr(space, count_field, n)
+    space.samples = samples
+    capacity = 4096
+    times = (C.c_float * capacity)()
+    evaluated = C.c_uint32()
+    best = abi.RenderConfig()
+    cam = camera_struct(camera)
+    check(library().wf_renderer_autotune(device_scene.handle, C.byref(cam), C.byref(config), C.byref(space), stream,
+                                         C.byref(best), times, capacity, C.byref(evaluated)))
+    # candidate settings in the tuner's loop order
+    table = []
+    base_tile = config.tile_width if config.tile_width == config.tile_height else 0
+    for mode in (modes or (config.mode,)):
+        own = (concurrent_tiles or (config.concurrent_tiles,)) if mode == abi.MODE_GRAPH else \
+            (regenerate_percents or (config.regenerate_percent,)) if mode == abi.MODE_STREAM else \
+            (chunks or (config.chunk,))
+        for b in (block_sizes or (config.block_size,)):
+            for rf in (refill_thresholds or (config.refill_threshold,)):
+                for t in (tile_sizes or (base_tile,)):
+                    for o in own:
+                        table.append({"mode": mode, "block_size": b, "refill_threshold": rf, "tile": t, "setting": o})
+    table = [(cand, times[i]) for i, cand in enumerate(table[:evaluated.value])]
+    chosen = {k: getattr(best, k) for k in fields}
+    _TUNED[key] = chosen
+    if cache_path is not None:
+        data = {}
+        if os.path.exists(cache_path):
+            with open(cache_path) as f:
+                data = json.load(f)
+        data[key] = chosen
+        with open(cache_path, "w") as f:
+            json.dump(data, f)
+    return best, table
+
+
 class Batch:
     """Many render jobs in one captured graph (wf_batch_*).  `jobs` is a list
     of dicts: scene (DeviceScene), camera (camera dict), config

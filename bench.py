@@ -396,7 +396,7 @@ def run_batch(args):
         return ms
 
     tune = None
-    if args.no_autotune:
+    if not args.autotune:
         batch = wfpt.Batch(jobs, stream=stream.cuda_stream)
     else:
         best, times = wfpt.Batch.autotune(jobs, slot_capacities=(1 << 20, 2 << 20, 4 << 20), block_sizes=(128, 256),
@@ -502,14 +502,18 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="large_mesh", choices=sorted(WORKLOADS) + ["batch", "inverse"])
     ap.add_argument("--batch-jobs", type=int, default=64, help="batch workload: number of jobs")
-    ap.add_argument("--no-autotune", action="store_true", help="batch workload: default batch configuration")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--mode", default=None, choices=sorted(MODES), help="default: per workload")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: per workload)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="scene workloads: skip wf_renderer_autotune and render with the given or default settings "
+                         "(batch workload: skip the batch tuner)")
     ap.add_argument("--build", default="exact", choices=["exact", "fast"],
                     help="exact: the bit-exact library (default); fast: multiply-adds contracted and CUDA's own "
                          "elementary functions (make -C wavefront-path-tracer_b200 fast)")
+    ap.add_argument("--persistent-kernel", default="auto", choices=["auto", "fused", "staged"],
+                    help="persistent mode: the fused per-path kernel, the staged kernel, or by tile size (default)")
     ap.add_argument("--regenerate-percent", type=int, default=0,
                     help="streaming mode: share of idle slots (%%) at which waiting slots start their next "
                          "samples together (0 = the renderer's default)")
@@ -552,10 +556,32 @@ def main():
     scene.bvh_builder = wfpt.abi.BVH_GPU_PLOC if args.bvh_builder == "gpu" else wfpt.abi.BVH_HOST_SAH
     dev_scene = wfpt.DeviceScene(scene)
     scene_info = dev_scene.info()
+    mode_given = args.mode is not None
     args.mode = args.mode or DEFAULT_MODE[args.workload]
+    stages = {"auto": wfpt.abi.PERSISTENT_AUTO, "fused": wfpt.abi.PERSISTENT_FUSED,
+              "staged": wfpt.abi.PERSISTENT_STAGED}[args.persistent_kernel]
     cfg = wfpt.render_config(width, height, mode=MODES[args.mode], concurrent_tiles=args.concurrent_tiles,
-                             regenerate_percent=args.regenerate_percent, **rkw)
+                             regenerate_percent=args.regenerate_percent, persistent_stages=stages, **rkw)
     spp = args.spp or SPP_PER_STEP[args.workload]
+    tune = None
+    if args.autotune:
+        # wf_renderer_autotune: one timed frame of `spp` samples per candidate
+        # (schedule, CTA size, refill threshold and the schedule's own
+        # setting); options given on the command line stay fixed
+        modes = (MODES[args.mode],) if mode_given else (MODES["graph"], MODES["stream"])
+        t_tune = time.perf_counter()
+        best, table = wfpt.autotune(
+            dev_scene, cam, cfg, modes=modes, block_sizes=(128, 256), refill_thresholds=(8, 16),
+            concurrent_tiles=(args.concurrent_tiles,) if args.concurrent_tiles else (1, 2),
+            regenerate_percents=(args.regenerate_percent,) if args.regenerate_percent else (10, 25),
+            samples=spp, stream=stream.cuda_stream, key=f"{args.workload}/{spp}/{args.build}/{modes}")
+        cfg = best
+        args.mode = {v: k for k, v in MODES.items()}[cfg.mode]
+        args.concurrent_tiles = cfg.concurrent_tiles
+        tune = {"seconds": round(time.perf_counter() - t_tune, 2), "candidates": len(table),
+                "chosen": {"mode": args.mode, "block_size": cfg.block_size, "refill_threshold": cfg.refill_threshold,
+                           "concurrent_tiles": cfg.concurrent_tiles, "regenerate_percent": cfg.regenerate_percent},
+                "frame_ms": [dict(c, ms=round(ms, 3)) for c, ms in table]}
     renderer = wfpt.Renderer(dev_scene, cam, cfg, stream=stream.cuda_stream)
     setup_s = time.perf_counter() - t_setup
     scene_bytes = dev_scene.info().device_bytes
@@ -675,9 +701,11 @@ def main():
                        "max_depth": cfg.max_depth, "rr_start_depth": cfg.rr_start_depth,
                        "triangles": int(scene.triangle_count()), "instances": int(len(scene.instances)),
                        "photons": int(cfg.photon_count) if cfg.caustics else 0, "mode": args.mode,
-                       "regenerate_percent": (args.regenerate_percent or None) if args.mode == "stream" else None,
+                       "regenerate_percent": (cfg.regenerate_percent or None) if args.mode == "stream" else None,
+                       "persistent_kernel": args.persistent_kernel if args.mode == "persistent" else None,
                        "build": args.build,
                        "wavefronts": 1 if args.mode != "graph" or args.concurrent_tiles == 1 else 2,
+                       "block_size": cfg.block_size or 128, "refill_threshold": cfg.refill_threshold or 8,
                        "scene_device_bytes": int(scene_bytes),
                        "bvh_builder": args.bvh_builder, "bvh_build_ms": round(float(scene_info.bvh_build_ms), 1),
                        "gpu_bvh_builds": int(scene_info.gpu_bvh_builds),
@@ -696,6 +724,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clock_record,
             "setup_seconds": setup_s,
+            "autotune": tune,
         }
         line["frame_guides"] = guides  # measured after the timed region
         if reference_cuda is not None:

@@ -368,7 +368,8 @@ typedef struct wf_render_config {
     float indirect_clamp;      /* 0 disables */
     uint32_t tile_width;       /* 0 = full frame; bounds queue memory */
     uint32_t tile_height;
-    uint32_t block_size;       /* 0 = tuned default */
+    uint32_t block_size;       /* CTA size of the lane-refill trace and shadow kernels: a multiple of
+                                  32 up to 1024; 0 = 128 */
     uint32_t persistent_blocks;/* 0 = the resident grid, trimmed for small tiles to
                                   max(4 x SMs, paths / 128) */
     uint32_t chunk;            /* persistent work chunk in paths, 0 = default */
@@ -403,7 +404,13 @@ typedef struct wf_render_config {
                                   their camera rays are traced coherently.  1..100 (100 = after every
                                   bounce); 0 = the tuned default.  Each pixel still takes its samples
                                   in order, so the sums do not depend on it. */
+    uint32_t persistent_stages; /* persistent mode: WF_PERSISTENT_AUTO (0) = staged from 262,144 paths
+                                  per tile, fused below; WF_PERSISTENT_FUSED = one body per path
+                                  (trace, shade, shadow rays inline, as persistentWavefrontTrace);
+                                  WF_PERSISTENT_STAGED = the wavefront stages between grid barriers.
+                                  Same sums either way. */
 } wf_render_config;
+enum { WF_PERSISTENT_AUTO = 0, WF_PERSISTENT_FUSED = 1, WF_PERSISTENT_STAGED = 2 };
 
 /* Defaults of RenderConfig (config.hpp:11-41) at the given resolution. */
 void wf_render_config_default(wf_render_config* config, uint32_t width, uint32_t height);
@@ -506,14 +513,16 @@ wf_status wf_render_tile_static(const wf_scene* scene, const wf_camera* camera,
 /* Candidate settings of wf_renderer_autotune.  Each list comes with its
  * length; a length of 0 keeps the base config's value.  Settings that a mode
  * does not read are not varied for it (concurrent_tiles: graph mode only;
- * regenerate_percents: streaming mode only; chunks: persistent mode only). */
+ * regenerate_percents: streaming mode only; persistent_stages: persistent
+ * mode only, with chunks varied for its fused kernel only). */
 typedef struct wf_tune_space {
     const uint32_t* modes;               uint32_t mode_count;               /* WF_MODE_* */
     const uint32_t* block_sizes;         uint32_t block_size_count;         /* trace / shade CTA size */
     const uint32_t* refill_thresholds;   uint32_t refill_threshold_count;   /* lane refill (1..32) */
     const uint32_t* concurrent_tiles;    uint32_t concurrent_tiles_count;   /* wavefronts per tile */
     const uint32_t* regenerate_percents; uint32_t regenerate_percent_count; /* streaming regeneration */
-    const uint32_t* chunks;              uint32_t chunk_count;              /* persistent work chunk */
+    const uint32_t* chunks;              uint32_t chunk_count;              /* persistent work chunk (fused) */
+    const uint32_t* persistent_stages;   uint32_t persistent_stage_count;   /* WF_PERSISTENT_* */
     const uint32_t* tile_sizes;          uint32_t tile_size_count;          /* square tile edge = queue
                                                                                capacity; 0 = full frame */
     uint32_t samples;  /* samples per pixel of each timed frame (0 = 1) */
@@ -527,7 +536,8 @@ typedef struct wf_tune_space {
  * keeps the fastest.  `best` receives that config; times_ms[i] (optional,
  * times_capacity entries) the frame time of candidate i in loop order
  * (modes outermost, then block sizes, refill thresholds, tile sizes, and the
- * mode's own setting); *evaluated the number of candidates.  All candidates
+ * mode's own settings: concurrent tiles; regenerate percents; persistent
+ * stages, each fused one by chunk); *evaluated the number of candidates.  All candidates
  * render the same image, so the choice does not change any result. */
 wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, const wf_render_config* base,
                                const wf_tune_space* space, void* stream, wf_render_config* best,

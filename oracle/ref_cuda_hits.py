@@ -74,10 +74,13 @@ def compare(workload):
     agree = same_prim & same_inst & hit
     rel_t = np.abs(got["t"][agree].astype(np.float64) - want["t"][agree]) / np.abs(want["t"][agree])
     exact_t = int((got["t"][agree].view(np.uint32) == want["t"][agree].view(np.uint32)).sum())
+    # e.g. a sphere whose near root lands just below the minimum distance on
+    # one side and just above on the other: same primitive, other root
+    t_differs = int((rel_t > 1e-4).sum())
     return {"workload": workload, "build": "fast" if "fast" in str(wfpt.native.LIB_PATH) else "exact",
             "rays": int(len(rays)), "per_bounce": [int(c) for c in counts], "hits": int(hit.sum()),
             "kind_differs": int((~same_kind).sum()), "primitive_differs": int((~same_prim).sum()),
-            "instance_differs": int((~same_inst).sum()), "t_bit_identical": exact_t,
+            "instance_differs": int((~same_inst).sum()), "t_bit_identical": exact_t, "t_differs": t_differs,
             "t_max_relative_difference": float(rel_t.max()) if rel_t.size else 0.0}
 
 

@@ -39,7 +39,7 @@ def test_struct_layouts_match_header():
     assert abi.MATERIAL_DTYPE.itemsize == 124
     assert abi.HIT_DTYPE.itemsize == 68
     assert ctypes.sizeof(abi.SceneDesc) == 184
-    assert ctypes.sizeof(abi.RenderConfig) == 128
+    assert ctypes.sizeof(abi.RenderConfig) == 132
     assert ctypes.sizeof(abi.Camera) == 56
 
 

@@ -19,10 +19,12 @@ def test_autotune_picks_a_schedule_with_identical_sums(cuda, tmp_path):
     cache = tmp_path / "tuned.json"
     best, table = wfpt.autotune(dev, cam, base, modes=(abi.MODE_GRAPH, abi.MODE_STREAM, abi.MODE_PERSISTENT),
                                 block_sizes=(128, 256), refill_thresholds=(8, 16), concurrent_tiles=(1, 2),
-                                regenerate_percents=(10, 50), chunks=(32, 64), samples=2, key="cornell64",
-                                cache_path=str(cache))
-    # graph: 2 x 2 x 2, stream: 2 x 2 x 2, persistent: 2 x 2 x 2
-    assert len(table) == 24 and all(ms > 0 for _, ms in table)
+                                regenerate_percents=(10, 50), chunks=(32, 64),
+                                persistent_stages=(abi.PERSISTENT_FUSED, abi.PERSISTENT_STAGED), samples=2,
+                                key="cornell64", cache_path=str(cache))
+    # graph: 2 x 2 x 2 wavefronts, stream: 2 x 2 x 2 percents,
+    # persistent: 2 x 2 x (fused x 2 chunks + staged)
+    assert len(table) == 28 and all(ms > 0 for _, ms in table)
     fastest = min(table, key=lambda row: row[1])[0]
     assert best.mode == fastest["mode"] and best.block_size == fastest["block_size"]
     again, empty = wfpt.autotune(dev, cam, base, key="cornell64", cache_path=str(cache))

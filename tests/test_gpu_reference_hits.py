@@ -4,8 +4,10 @@ sample-0 ray batch (65,536 camera rays and their bounce-1 continuations)
 and the reduced large mesh's.  The reference's sm_100a build contracts
 multiply-adds; the exact build here does not, the fast build does, so a ray
 that grazes an edge or meets two surfaces at nearly the same distance may
-resolve differently.  Bound: at most 1 ray in 10,000 with a different
-kind, primitive or instance, and t within 1e-4 relative where they agree."""
+resolve differently, and a ray that meets a primitive at a distance near
+the minimum may take the other root or face.  Bound: at most 1 ray in
+10,000 with a different kind, primitive or instance, and at most 1 in
+10,000 of the agreeing rays with t apart by more than 1e-4 relative."""
 import json
 import os
 import subprocess
@@ -37,4 +39,4 @@ def test_hit_identities_match_reference_cuda(cuda, workload, build):
     assert r["build"] == build and r["rays"] > 10_000 and r["hits"] > r["rays"] // 4, r
     differ = r["kind_differs"] + r["primitive_differs"] + r["instance_differs"]
     assert differ <= r["rays"] // 10_000, r
-    assert r["t_max_relative_difference"] <= 1e-4, r
+    assert r["t_differs"] <= r["rays"] // 10_000, r

@@ -565,7 +565,10 @@ wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_
     WF_BATCH_CUDA(b->opaque ? batch_resident(bp, 2, k_batch_shadow<Opaque<NoTally>>, b->block)
                             : batch_resident(bp, 2, k_batch_shadow<NoTally>, b->block));
     WF_BATCH_CUDA(batch_resident(bp, 3, k_batch_finalize, 256));
-    if (wf_status e = capture_batch(bp)) return e;
+    if (wf_status e = capture_batch(bp)) {
+        abandon_capture(b->stream);
+        return e;
+    }
     WF_BATCH_CUDA(cudaStreamSynchronize(b->stream));
     *out = b.release();
     return WF_OK;

@@ -370,25 +370,42 @@ wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, c
     uint32_t count = 0;
     float best_ms = 0.0f;
     for (uint32_t mode : modes) {
-        std::vector<uint32_t> own = mode == WF_MODE_GRAPH
-                                        ? values(space->concurrent_tiles, space->concurrent_tiles_count,
-                                                 base->concurrent_tiles)
-                                    : mode == WF_MODE_STREAM
-                                        ? values(space->regenerate_percents, space->regenerate_percent_count,
-                                                 base->regenerate_percent)
-                                        : values(space->chunks, space->chunk_count, base->chunk);
+        // the mode's own settings: (setting, fused-kernel chunk) pairs
+        std::vector<std::pair<uint32_t, uint32_t>> own;
+        if (mode == WF_MODE_GRAPH) {
+            for (uint32_t v : values(space->concurrent_tiles, space->concurrent_tiles_count, base->concurrent_tiles))
+                own.push_back({v, base->chunk});
+        } else if (mode == WF_MODE_STREAM) {
+            for (uint32_t v :
+                 values(space->regenerate_percents, space->regenerate_percent_count, base->regenerate_percent))
+                own.push_back({v, base->chunk});
+        } else {
+            for (uint32_t k :
+                 values(space->persistent_stages, space->persistent_stage_count, base->persistent_stages)) {
+                if (k == WF_PERSISTENT_STAGED) {
+                    own.push_back({k, base->chunk});
+                    continue;
+                }
+                for (uint32_t chunk : values(space->chunks, space->chunk_count, base->chunk)) own.push_back({k, chunk});
+            }
+        }
         for (uint32_t block : blocks)
             for (uint32_t refill : refills)
                 for (uint32_t tile : tiles)
-                    for (uint32_t setting : own) {
+                    for (const auto& setting : own) {
                         wf_render_config c = *base;
                         c.mode = mode;
                         c.block_size = block;
                         c.refill_threshold = refill;
                         c.tile_width = c.tile_height = tile;
-                        if (mode == WF_MODE_GRAPH) c.concurrent_tiles = setting;
-                        else if (mode == WF_MODE_STREAM) c.regenerate_percent = setting;
-                        else c.chunk = setting;
+                        if (mode == WF_MODE_GRAPH) {
+                            c.concurrent_tiles = setting.first;
+                        } else if (mode == WF_MODE_STREAM) {
+                            c.regenerate_percent = setting.first;
+                        } else {
+                            c.persistent_stages = setting.first;
+                            c.chunk = setting.second;
+                        }
                         wf_renderer* r = nullptr;
                         if (wf_status e = renderer_create(scene, camera, &c, stream, &r)) return e;
                         cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -1229,7 +1229,7 @@ wf_status capture_graph(wf_renderer* r) {
         uint32_t* cur_count = &r->counters->queue_count[cur];
         uint32_t* next_count = &r->counters->queue_count[nxt];
         if (b == 0)
-            launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st, 
+            launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_camera), r->block_camera, st, 
                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill,
                 nullptr, nullptr);
         else
@@ -1308,7 +1308,7 @@ wf_status capture_stream_graph(wf_renderer* r) {
         // camera rays when nothing survived.  The launch with nothing to do
         // exits at once.
         uint32_t* camera = &r->counters->camera_count[cur];
-        launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st,
+        launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_camera), r->block_camera, st,
             s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, kMaxBounces, nullptr,
             r->refill, camera, &r->counters->work_camera);
         launch_trace<NoTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st,
@@ -1393,10 +1393,43 @@ cudaError_t launch_phased(wf_renderer* r, cudaStream_t st, uint64_t paths) {
     b.capacity = r->capacity;
     b.refill = r->refill;
     void* args[] = {&s, &rp, &tp, &c, &b};
-    uint32_t blocks = persistent_grid(r->config.persistent_blocks, r->persistent_blocks, r->sm_count,
+    uint32_t blocks = persistent_grid(r->config.persistent_blocks, r->phased_blocks, r->sm_count,
                                       std::min<uint64_t>(paths, r->capacity));
     return cudaLaunchCooperativeKernel(phased_kernel(r->opaque, r->textured), dim3(blocks),
                                        dim3(r->persistent_block_size), args, 0, st);
+}
+
+// One cooperative launch of the fused persistent kernel (k_persistent).
+cudaError_t launch_fused(wf_renderer* r, cudaStream_t st, uint64_t paths) {
+    cudaError_t e = cudaMemsetAsync(r->counters->persistent_count, 0, sizeof(uint32_t) * 2 * (kMaxBounces + 1), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&r->counters->barrier_count, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    DeviceScene s = r->scene->view;
+    RenderParams rp = r->params;
+    const TileDev* tp = r->tile;
+    Counters* c = r->counters;
+    PathSoA ps = r->paths;
+    uint32_t* q0 = r->queue[0];
+    uint32_t* q1 = r->queue[1];
+    uint32_t cap = r->capacity;
+    float* fb = r->framebuffer;
+    uint32_t chunk = r->chunk;
+    void* args[] = {&s, &rp, &tp, &c, &ps, &q0, &q1, &cap, &fb, &chunk};
+    uint32_t blocks = persistent_grid(r->config.persistent_blocks, r->persistent_blocks, r->sm_count,
+                                      std::min<uint64_t>(paths, r->capacity));
+    return cudaLaunchCooperativeKernel(persistent_kernel(r->opaque, r->textured), dim3(blocks),
+                                       dim3(r->persistent_block_size), args, 0, st);
+}
+
+// The persistent schedule's launch for a tile of `paths` paths: the staged
+// kernel pays a grid barrier per stage, which a small tile does not amortise
+// (256x256 Cornell box: fused 127, staged 72 Mpaths/s), while on large tiles
+// the fused body's spills dominate (1080p large mesh: fused 47, staged 84).
+constexpr uint64_t kStagedMinPaths = 262144;
+cudaError_t launch_persistent(wf_renderer* r, cudaStream_t st, uint64_t paths) {
+    uint32_t k = r->config.persistent_stages;
+    bool staged = k == WF_PERSISTENT_STAGED || (k == WF_PERSISTENT_AUTO && paths >= kStagedMinPaths);
+    return staged ? launch_phased(r, st, paths) : launch_fused(r, st, paths);
 }
 
 wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
@@ -1407,7 +1440,7 @@ wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
         WF_CUDA(cudaGraphLaunch(r->graph_exec, r->stream));
         return WF_OK;
     }
-    WF_CUDA(launch_phased(r, r->stream, uint64_t(tile.width) * tile.height));
+    WF_CUDA(launch_persistent(r, r->stream, uint64_t(tile.width) * tile.height));
     k_advance<<<1, 1, 0, r->stream>>>(r->counters, r->tile);
     WF_CUDA(cudaGetLastError());
     return WF_OK;
@@ -1426,7 +1459,8 @@ wf_status check_render_config(const wf_scene* scene, const wf_render_config& c) 
         return fail(WF_ERR_INVALID_ARG, "Render dimensions exceed the supported queue index range");
     if (c.max_depth == 0) return fail(WF_ERR_INVALID_ARG, "maximum depth must be greater than zero");
     if (c.max_depth > kMaxBounces) return fail(WF_ERR_INVALID_ARG, "maximum depth above %d", kMaxBounces);
-    if (c.block_size > 1024) return fail(WF_ERR_INVALID_ARG, "CUDA block size must be between 1 and 1024");
+    if (c.block_size > 1024 || c.block_size % 32)
+        return fail(WF_ERR_INVALID_ARG, "CUDA block size must be a multiple of 32 up to 1024 (0 = default)");
     if (c.mode > WF_MODE_STREAM || c.rng > WF_RNG_PCG32 || c.debug > WF_DEBUG_SHADING_NORMAL)
         return fail(WF_ERR_INVALID_ARG, "unknown mode, rng strategy or debug view");
     if (c.caustics && c.photon_count == 0)
@@ -1463,7 +1497,10 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
     WF_CUDA(cudaGetDevice(&r->device));
     WF_CUDA(cudaDeviceGetAttribute(&r->sm_count, cudaDevAttrMultiProcessorCount, r->device));
     r->grid_cap = uint32_t(r->sm_count) * 64;
-    if (c.block_size) r->block_trace = r->block_shade = c.block_size;
+    // The CTA size setting applies to the lane-refill trace and shadow
+    // kernels; shading and camera rays keep the 128 their register bounds
+    // are written for.
+    if (c.block_size) r->block_trace = c.block_size;
     r->refill = c.refill_threshold ? c.refill_threshold : 8u;
     r->regenerate_percent = c.regenerate_percent ? std::min(c.regenerate_percent, 100u) : kDefaultRegeneratePercent;
     r->opaque = !scene->alpha_textures;
@@ -1545,8 +1582,8 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
     if (c.mode != WF_MODE_PERSISTENT) {
         WF_CUDA(r->opaque ? resident_grid(rr, 0, k_trace<Opaque<NoTally>>, r->block_trace)
                           : resident_grid(rr, 0, k_trace<NoTally>, r->block_trace));
-        WF_CUDA(r->opaque ? resident_grid(rr, 5, k_trace_camera<Opaque<NoTally>>, r->block_trace)
-                          : resident_grid(rr, 5, k_trace_camera<NoTally>, r->block_trace));
+        WF_CUDA(r->opaque ? resident_grid(rr, 5, k_trace_camera<Opaque<NoTally>>, r->block_camera)
+                          : resident_grid(rr, 5, k_trace_camera<NoTally>, r->block_camera));
         WF_CUDA(r->textured ? resident_grid(rr, 1, k_shade<true>, r->block_shade)
                             : resident_grid(rr, 1, k_shade<false>, r->block_shade));
         WF_CUDA(r->opaque ? resident_grid(rr, 2, k_shadow<Opaque<NoTally>>, r->block_trace)
@@ -1556,13 +1593,19 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
         int cooperative = 0;
         WF_CUDA(cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, r->device));
         if (!cooperative) return fail(WF_ERR_UNSUPPORTED, "device does not support cooperative launches");
+        if (c.persistent_stages > WF_PERSISTENT_STAGED)
+            return fail(WF_ERR_INVALID_ARG, "unknown persistent kernel %u", c.persistent_stages);
         r->persistent_block_size = 128;
         int per_sm = 0;
-        WF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, phased_kernel(r->opaque, r->textured),
+        WF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel(r->opaque, r->textured),
                                                               int(r->persistent_block_size), 0));
-        if (per_sm <= 0) return fail(WF_ERR_UNSUPPORTED, "the persistent kernel cannot be resident");
-        uint32_t resident = uint32_t(per_sm) * uint32_t(r->sm_count);
-        r->persistent_blocks = resident;  // the largest grid; persistent_grid picks each launch's
+        int phased_per_sm = 0;
+        WF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&phased_per_sm, phased_kernel(r->opaque, r->textured),
+                                                              int(r->persistent_block_size), 0));
+        if (per_sm <= 0 || phased_per_sm <= 0) return fail(WF_ERR_UNSUPPORTED, "the persistent kernel cannot be resident");
+        // the largest grids; persistent_grid picks each launch's
+        r->persistent_blocks = uint32_t(per_sm) * uint32_t(r->sm_count);
+        r->phased_blocks = uint32_t(phased_per_sm) * uint32_t(r->sm_count);
         r->chunk = c.chunk ? std::max(1u, c.chunk / 32) : 1u;
     }
     if (c.caustics && photon_source) {
@@ -1577,10 +1620,12 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
         WF_CUDA(cudaEventCreateWithFlags(&r->fork_event, cudaEventDisableTiming));
         WF_CUDA(cudaEventCreateWithFlags(&r->join_event, cudaEventDisableTiming));
     }
-    if (c.mode == WF_MODE_GRAPH) {
-        if (wf_status e = capture_graph(rr)) return e;
-    } else if (c.mode == WF_MODE_STREAM) {
-        if (wf_status e = capture_stream_graph(rr)) return e;
+    if (c.mode == WF_MODE_GRAPH || c.mode == WF_MODE_STREAM) {
+        wf_status e = c.mode == WF_MODE_GRAPH ? capture_graph(rr) : capture_stream_graph(rr);
+        if (e != WF_OK) {
+            abandon_capture(r->stream);
+            return e;
+        }
     }
     WF_CUDA(cudaStreamSynchronize(r->stream));
     *out = r.release();
@@ -1800,7 +1845,7 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
             WF_CUDA(cudaMemcpyAsync(r->tile, &tile, sizeof(TileDev), cudaMemcpyHostToDevice, st));
             cudaError_t launch_error = cudaSuccess;
             if (wf_status e = timed(WF_KERNEL_PERSISTENT, [&] {
-                    launch_error = launch_phased(r, st, uint64_t(tile.width) * tile.height);
+                    launch_error = launch_persistent(r, st, uint64_t(tile.width) * tile.height);
                 }))
                 return e;
             WF_CUDA(launch_error);
@@ -1826,7 +1871,7 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                     uint32_t* next_count = &r->counters->queue_count[nxt];
                     auto trace = [&] {
                         if (count && b == 0)
-                            launch_trace<CountTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st, 
+                            launch_trace<CountTally, false>(r, grid(r, 5, cap, r->block_camera), r->block_camera, st, 
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
                                 r->tally, r->refill, nullptr, nullptr);
                         else if (count)
@@ -1834,7 +1879,7 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
                                 r->tally, r->refill, nullptr, nullptr);
                         else if (b == 0)
-                            launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_trace), r->block_trace, st, 
+                            launch_trace<NoTally, false>(r, grid(r, 5, cap, r->block_camera), r->block_camera, st, 
                                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b,
                                 nullptr, r->refill, nullptr, nullptr);
                         else

@@ -98,7 +98,7 @@ struct wf_renderer {
     int device = 0;
     int sm_count = 148;
     uint32_t capacity = 0;
-    uint32_t block_trace = 128, block_shade = 128, block_finalize = 256, block_gather = 128;
+    uint32_t block_trace = 128, block_shade = 128, block_finalize = 256, block_gather = 128, block_camera = 128;
     uint32_t grid_cap = 0;
     std::vector<void*> allocations;
     uint64_t device_bytes = 0;
@@ -124,7 +124,8 @@ struct wf_renderer {
     uint8_t* shade_key = nullptr;     // shading category of each queue entry
     uint32_t* shade_order = nullptr;  // queue entries grouped by category (the order k_shade takes them)
     wf::GatherQueue gathers{};                      // caustic gather requests (graph and streaming modes)
-    uint32_t persistent_blocks = 0;
+    uint32_t persistent_blocks = 0;  // resident grid of the fused persistent kernel
+    uint32_t phased_blocks = 0;      // resident grid of the staged persistent kernel
     uint32_t persistent_block_size = 128;
     uint32_t chunk = 1;
     uint32_t refill = 8;  // trace/shadow kernels: idle lanes of a warp that trigger a refill
@@ -148,6 +149,19 @@ struct wf_renderer {
 };
 
 namespace wf {
+// After a failed graph capture: ends the capture if it is still open
+// (discarding its graph) and consumes the launch error it recorded, so
+// neither outlives the failed call on the calling thread.
+inline void abandon_capture(cudaStream_t st) {
+    cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &status) == cudaSuccess && status != cudaStreamCaptureStatusNone) {
+        cudaGraph_t partial = nullptr;
+        cudaStreamEndCapture(st, &partial);
+        if (partial) cudaGraphDestroy(partial);
+    }
+    cudaGetLastError();
+}
+
 wf_status renderer_create(const wf_scene* scene, const wf_camera* camera, const wf_render_config* config,
                           void* stream, wf_renderer** out);
 wf_status renderer_destroy(wf_renderer* r);

@@ -22,6 +22,7 @@ ACCEL_BVH, ACCEL_DIRECT = 0, 1
 LIGHT_POINT, LIGHT_SPOT, LIGHT_DIRECTIONAL = 0, 1, 2
 NO_MATERIAL = 0xFFFFFFFF
 MODE_GRAPH, MODE_PERSISTENT, MODE_STREAM = 0, 1, 2
+PERSISTENT_AUTO, PERSISTENT_FUSED, PERSISTENT_STAGED = 0, 1, 2
 RNG_XORSHIFT32, RNG_PCG32 = 0, 1
 DEBUG_NONE, DEBUG_INTERSECTION, DEBUG_SHADING_NORMAL = 0, 1, 2
 HIT_NONE, HIT_MESH, HIT_STATIC_TRIANGLE, HIT_TRIANGLE, HIT_SPHERE = 0, 1, 2, 3, 4
@@ -143,6 +144,7 @@ class RenderConfig(C.Structure):
         ("photon_grid_resolution", C.c_uint32), ("photon_seed", C.c_uint32), ("spectral", C.c_uint32),
         ("profile_queues", C.c_uint32), ("refill_threshold", C.c_uint32), ("concurrent_tiles", C.c_uint32),
         ("shadow_queue_capacity", C.c_uint32), ("regenerate_percent", C.c_uint32),
+        ("persistent_stages", C.c_uint32),
     ]
 
 
@@ -153,6 +155,7 @@ class TuneSpace(C.Structure):
                 ("concurrent_tiles", C.c_void_p), ("concurrent_tiles_count", C.c_uint32),
                 ("regenerate_percents", C.c_void_p), ("regenerate_percent_count", C.c_uint32),
                 ("chunks", C.c_void_p), ("chunk_count", C.c_uint32),
+                ("persistent_stages", C.c_void_p), ("persistent_stage_count", C.c_uint32),
                 ("tile_sizes", C.c_void_p), ("tile_size_count", C.c_uint32),
                 ("samples", C.c_uint32)]
 

@@ -419,7 +419,8 @@ _TUNED = {}
 
 def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREAM), block_sizes=(128,),
              refill_thresholds=(4, 8, 16), concurrent_tiles=(1, 2), regenerate_percents=(10, 25),
-             chunks=(), tile_sizes=(), samples=1, stream=None, key=None, cache_path=None):
+             chunks=(), persistent_stages=(abi.PERSISTENT_FUSED, abi.PERSISTENT_STAGED), tile_sizes=(), samples=1,
+             stream=None, key=None, cache_path=None):
     """wf_renderer_autotune: times one frame per candidate setting and
     returns (best RenderConfig, [(candidate settings, ms), ...]).
 
@@ -429,12 +430,12 @@ def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREA
     settings without rendering (the table is then empty)."""
     import json
     fields = ("mode", "block_size", "refill_threshold", "tile_width", "tile_height", "concurrent_tiles",
-              "regenerate_percent", "chunk")
+              "regenerate_percent", "chunk", "persistent_stages")
     if key is None:
         key = repr((device_scene.handle.value, sorted((k, tuple(v) if hasattr(v, "__len__") else v)
                                                       for k, v in camera.items()),
                     bytes(config), modes, block_sizes, refill_thresholds, concurrent_tiles, regenerate_percents,
-                    chunks, tile_sizes, samples))
+                    chunks, persistent_stages, tile_sizes, samples))
     stored = _TUNED.get(key)
     if stored is None and cache_path is not None and os.path.exists(cache_path):
         with open(cache_path) as f:
@@ -452,14 +453,14 @@ def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREA
     space = abi.TuneSpace()
     for name, vals in (("modes", modes), ("block_sizes", block_sizes), ("refill_thresholds", refill_thresholds),
                        ("concurrent_tiles", concurrent_tiles), ("regenerate_percents", regenerate_percents),
-                       ("chunks", chunks), ("tile_sizes", tile_sizes)):
+                       ("chunks", chunks), ("persistent_stages", persistent_stages), ("tile_sizes", tile_sizes)):
         a, n = arr(list(vals))
         lists[name] = a
         setattr(space, name, C.cast(a, C.c_void_p))
         count_field = {"modes": "mode_count", "block_sizes": "block_size_count",
                        "refill_thresholds": "refill_threshold_count", "concurrent_tiles": "concurrent_tiles_count",
                        "regenerate_percents": "regenerate_percent_count", "chunks": "chunk_count",
-                       "tile_sizes": "tile_size_count"}[name]
+                       "persistent_stages": "persistent_stage_count", "tile_sizes": "tile_size_count"}[name]
         setattr(space, count_field, n)
     space.samples = samples
     capacity = 4096
@@ -473,14 +474,22 @@ def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREA
     table = []
     base_tile = config.tile_width if config.tile_width == config.tile_height else 0
     for mode in (modes or (config.mode,)):
-        own = (concurrent_tiles or (config.concurrent_tiles,)) if mode == abi.MODE_GRAPH else \
-            (regenerate_percents or (config.regenerate_percent,)) if mode == abi.MODE_STREAM else \
-            (chunks or (config.chunk,))
+        if mode == abi.MODE_GRAPH:
+            own = [{"concurrent_tiles": v} for v in (concurrent_tiles or (config.concurrent_tiles,))]
+        elif mode == abi.MODE_STREAM:
+            own = [{"regenerate_percent": v} for v in (regenerate_percents or (config.regenerate_percent,))]
+        else:
+            own = []
+            for k in (persistent_stages or (config.persistent_stages,)):
+                if k == abi.PERSISTENT_STAGED:
+                    own.append({"persistent_stages": k})
+                else:
+                    own += [{"persistent_stages": k, "chunk": ch} for ch in (chunks or (config.chunk,))]
         for b in (block_sizes or (config.block_size,)):
             for rf in (refill_thresholds or (config.refill_threshold,)):
                 for t in (tile_sizes or (base_tile,)):
                     for o in own:
-                        table.append({"mode": mode, "block_size": b, "refill_threshold": rf, "tile": t, "setting": o})
+                        table.append(dict({"mode": mode, "block_size": b, "refill_threshold": rf, "tile": t}, **o))
     table = [(cand, times[i]) for i, cand in enumerate(table[:evaluated.value])]
     chosen = {k: getattr(best, k) for k in fields}
     _TUNED[key] = chosen

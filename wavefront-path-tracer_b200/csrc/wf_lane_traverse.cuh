@@ -27,18 +27,46 @@ constexpr int kLaneStack = 128;
 
 enum : uint32_t { kStageTlas = 0, kStageBlas = 1, kStageDirect = 2, kStageDone = 3 };
 
+// The traversal stack keeps its most recent entry in registers (top_ref,
+// top_t) and the entries below it in local memory, one 8-byte (ref, entry
+// distance) pair each.  The usual pattern -- push the far child, descend
+// the near one to a leaf, pop the far child -- then resumes from a register
+// instead of waiting on a local-memory load; the refill of the register
+// from memory is issued at the pop and is ready by the next one.
 struct ClosestLane {
     V3 wo, wd;            // world ray
     V3 o, d, inv;         // ray of the current BVH (instance-local inside a BLAS)
     TraceState h;
     int ref;              // node (>= 0) or ~leaf to process next
     uint32_t stage;
-    int size, base;       // stack size; first entry of the current BVH
+    int size, base;       // stack size (the top included); first entry of the current BVH
     uint32_t inst, material_override;
     float previous;       // closestT when the current BLAS / direct BVH was entered
-    int stack_ref[kLaneStack];
-    float stack_t[kLaneStack];
+    int top_ref;          // entry size - 1 (valid when size > 0)
+    float top_t;
+    int2 stack[kLaneStack];  // entries 0 .. size - 2: (ref, entry distance bits)
 };
+
+WF_DEV void lane_push(ClosestLane& L, int ref, float t) {
+    if (L.size >= kLaneStack) return;  // TLAS + BLAS depth <= 2 * kMaxBvhDepth < kLaneStack
+    if (L.size > 0) L.stack[L.size - 1] = make_int2(L.top_ref, __float_as_int(L.top_t));
+    L.top_ref = ref;
+    L.top_t = t;
+    ++L.size;
+}
+
+// Removes the top entry (size > 0) into (ref, t) and brings the next one
+// into the registers.
+WF_DEV void lane_pop(ClosestLane& L, int& ref, float& t) {
+    ref = L.top_ref;
+    t = L.top_t;
+    --L.size;
+    if (L.size > 0) {
+        int2 e = L.stack[L.size - 1];
+        L.top_ref = e.x;
+        L.top_t = __int_as_float(e.y);
+    }
+}
 
 // Direct triangle list (last stage of traceRay): its BVH is traversed by the
 // lane; the no-BVH linear list runs at once.
@@ -137,9 +165,11 @@ WF_DEV void closest_pop(ClosestLane& L, const DeviceScene& s, Tally& tally) {
             L.stage = kStageDone;
             return;
         }
-        --L.size;
-        if (L.stack_t[L.size] < L.h.t) {
-            L.ref = L.stack_ref[L.size];
+        int ref;
+        float t;
+        lane_pop(L, ref, t);
+        if (t < L.h.t) {
+            L.ref = ref;
             return;
         }
     }
@@ -161,11 +191,7 @@ WF_DEV void closest_step(ClosestLane& L, const DeviceScene& s, Tally& tally) {
         bool hr = slab(L.o, L.inv, rxy.x, rxy.y, rxy.z, rxy.w, lrz.z, lrz.w, L.h.t, tr);
         if (hl && hr) {
             bool left_near = tl < tr;
-            if (L.size < kLaneStack) {  // TLAS + BLAS depth <= 2 * kMaxBvhDepth < kLaneStack
-                L.stack_ref[L.size] = left_near ? ch.y : ch.x;
-                L.stack_t[L.size] = left_near ? tr : tl;
-                ++L.size;
-            }
+            lane_push(L, left_near ? ch.y : ch.x, left_near ? tr : tl);
             L.ref = left_near ? ch.x : ch.y;
             return;
         }

@@ -464,6 +464,16 @@ def run_batch(args):
     for r in renderers:
         r.close()
     batch.close()
+    reference_sequential = None
+    if rank == 0 and world == 1 and args.reference_cuda:
+        # the reference's CUDA renderer, one job after another (after the timed regions)
+        if (ROOT / "oracle" / "_ref" / "libwfref_cuda.so").exists():
+            run = subprocess.run([sys.executable, str(ROOT / "oracle" / "ref_cuda_bench.py"), "--batch-jobs",
+                                  str(args.batch_jobs)], capture_output=True, text=True, timeout=1800, cwd=ROOT)
+            reference_sequential = (json.loads(run.stdout.strip().splitlines()[-1]) if run.returncode == 0
+                                    else {"failed": (run.stdout + run.stderr)[-400:]})
+        else:
+            reference_sequential = {"unavailable": "reference CUDA build absent (make -C oracle cuda)"}
     if rank == 0:
         line = {
             "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
@@ -479,6 +489,10 @@ def run_batch(args):
             "sequential": {"value": sequential, "unit": "Mpaths/s", "ms_per_step": s_ms / args.steps,
                            "how": "one graph-mode renderer per job, rendered one after another"},
             "speedup_vs_sequential": value / sequential,
+            "reference_cuda_sequential": reference_sequential,
+            "e2e_speedup_vs_reference_sequential": (e2e / reference_sequential["Mpaths/s"]
+                                                    if reference_sequential and "Mpaths/s" in reference_sequential
+                                                    else None),
             "parity_mismatched_jobs": mismatched,
             "autotune": tune,
             "gpu_launches": int(stats["kernel_launches"]),

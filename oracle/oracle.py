@@ -42,6 +42,8 @@ def ref_lib(det=False):
         lib.wfref_occluded.argtypes = [P, P, P, U32, P, I]
         lib.wfref_photons.restype = I
         lib.wfref_photons.argtypes = [P, P, P, P, P, I]
+        lib.wfref_load_environment.restype = I
+        lib.wfref_load_environment.argtypes = [C.c_char_p, P, P, P]
         lib.wfref_path_rays.restype = U32
         lib.wfref_path_rays.argtypes = [P, P, P, U32, U32, U32, U32, U32, U32, P, U32, P, I]
         lib.wfref_render.restype = I
@@ -217,6 +219,19 @@ class RefScene:
         if rc != 0:
             raise RuntimeError("reference render failed")
         return fb32, fb64, counts
+
+
+def load_environment(path, det=False):
+    """The reference's loadEnvironmentMap (stb_image's stbi_loadf) on a
+    Radiance .hdr file: float32 (h, w, 4) texels, or None when it throws."""
+    import os
+    lib = ref_lib(det)
+    w, h = C.c_uint32(), C.c_uint32()
+    if lib.wfref_load_environment(os.fsencode(path), C.byref(w), C.byref(h), None) != 0:
+        return None
+    out = np.zeros((h.value, w.value, 4), np.float32)
+    lib.wfref_load_environment(os.fsencode(path), C.byref(w), C.byref(h), out.ctypes.data)
+    return out
 
 
 def environment_distribution(rgba, det=False):

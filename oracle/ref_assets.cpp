@@ -10,6 +10,7 @@
 // layouts of include/wavefront.h so a test can compare it field by field with
 // the scene the product's loaders build; wfref_host_scene_upload turns it
 // into a renderable reference scene.
+#include "scene/environment.hpp"
 #include "scene/gltf_loader.hpp"
 #include "scene/obj_loader.hpp"
 #include "scene/scene_host.hpp"
@@ -83,6 +84,22 @@ const std::vector<Triangle>* triangle_list(const HostScene& h, int which, uint32
 }  // namespace
 
 extern "C" {
+
+// The reference's loadEnvironmentMap (src/scene/environment.cpp:66-82) on a
+// Radiance .hdr file: *width and *height always, and with rgba non-null the
+// width*height float4 texels.  Returns 0, or 1 when the reference throws.
+int wfref_load_environment(const char* path, uint32_t* width, uint32_t* height, float* rgba) {
+    try {
+        HostEnvironment map = loadEnvironmentMap(path);
+        *width = map.width;
+        *height = map.height;
+        if (rgba) std::memcpy(rgba, map.pixels.data(), sizeof(float) * 4 * map.pixels.size());
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "wfref_load_environment: %s\n", e.what());
+        return 1;
+    }
+}
 
 // The reference's preset assembly.  kind 0: assembleGltfScene(filename,
 // scale, add_top_light) (the sponza preset); kind 1:

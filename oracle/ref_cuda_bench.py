@@ -155,6 +155,40 @@ def compare(workload=None, modes=("graph", "persistent"), steps=5, spp=0, own_mo
     }
 
 
+def batch_sequential(job_count=64, seed=11):
+    """The batch workload's jobs (wfpt.scenes.batch_jobs) rendered by the
+    reference's CUDA renderer one after another, each as one task of its
+    whole sample count through RenderTaskRenderer::render (after one untimed
+    warm-up task): the "plain renderer once per job, sequentially" that
+    batching replaces.  Scene creation is not timed."""
+    import wfpt
+    from wfpt import native, scenes
+    lib = load()
+    specs = scenes.batch_jobs(job_count, seed)
+    total_ms, paths, setup_s = 0.0, 0, 0.0
+    for j in specs:
+        cfg = wfpt.render_config(j["width"], j["height"], max_depth=j["max_depth"])
+        cam_struct = native.camera_struct(j["camera"])
+        d, keep = j["scene"].desc()
+        t0 = time.perf_counter()
+        handle = lib.wfcuda_scene_create(C.addressof(d), None)
+        setup_s += time.perf_counter() - t0
+        del keep
+        if not handle:
+            raise SystemExit("reference scene creation failed")
+        ms = (C.c_double * 1)()
+        rc = lib.wfcuda_render(handle, C.addressof(cam_struct), C.addressof(cfg), 0, 0, j["spp"], 1, None, ms,
+                               None, None)
+        lib.wfcuda_scene_destroy(handle)
+        if rc != 0:
+            raise SystemExit(f"reference render failed ({rc})")
+        total_ms += ms[0]
+        paths += j["width"] * j["height"] * j["spp"]
+    return {"jobs": len(specs), "seed": seed, "paths": paths, "ms": total_ms, "Mpaths/s": paths / total_ms / 1e3,
+            "scene_setup_s": round(setup_s, 2),
+            "timing": "sum over jobs of the wall time of one whole-job task: render + download of the radiance"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="large_mesh")
@@ -168,7 +202,12 @@ def main():
     ap.add_argument("--manifest", default=None,
                     help="a scene manifest of the reference's presets, loaded by wfpt.assets, instead of a workload")
     ap.add_argument("--size", default="1280x720", help="image size for --manifest")
+    ap.add_argument("--batch-jobs", type=int, default=0,
+                    help="render the batch workload's jobs one after another with the reference instead")
     args = ap.parse_args()
+    if args.batch_jobs:
+        print(json.dumps(batch_sequential(args.batch_jobs)), flush=True)
+        return
     out = compare(args.workload, tuple(args.mode.split(",")), args.steps, args.spp, args.own_mode, args.sample_start,
                   args.manifest, args.size, caustics=not args.no_caustics)
     print(json.dumps(out), flush=True)

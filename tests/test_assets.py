@@ -10,6 +10,7 @@ levels, because the two JPEG decoders round their inverse DCTs differently.
 The fixtures under tests/golden/assets are made by
 tests/golden/make_asset_fixtures.py.  The reference's own asset presets are
 compared too when its asset tree is present."""
+import json
 import os
 from pathlib import Path
 
@@ -177,3 +178,82 @@ def test_preset_cameras_match_the_reference_formulas():
     assert cam["aspect_ratio"] == np.float32(2.0)
     demo = assets.camera("demo", 64, 64)
     assert abs(np.dot(demo["right"], demo["forward"])) < 1e-6 and demo["up"][1] > 0.9
+
+
+def _write_hdr(path, rgbe, rle=True, header=b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n"):
+    """A Radiance .hdr file from (h, w, 4) RGBE bytes: run-length encoded
+    scanlines (runs of repeated bytes and literals, per channel) or flat."""
+    h, w, _ = rgbe.shape
+    out = bytearray(header + b"\n" + f"-Y {h} +X {w}\n".encode())
+    if not rle:
+        out += rgbe.astype(np.uint8).tobytes()
+    else:
+        for y in range(h):
+            out += bytes([2, 2, w >> 8, w & 255])
+            for ch in range(4):
+                row = rgbe[y, :, ch].astype(np.uint8)
+                x = 0
+                while x < w:
+                    run = 1
+                    while x + run < w and run < 127 and row[x + run] == row[x]:
+                        run += 1
+                    if run >= 3:
+                        out += bytes([128 + run, int(row[x])])
+                        x += run
+                        continue
+                    lit = 1
+                    while x + lit < w and lit < 128 and not (x + lit + 2 < w and row[x + lit] == row[x + lit + 1]
+                                                             == row[x + lit + 2]):
+                        lit += 1
+                    out += bytes([lit]) + row[x:x + lit].tobytes()
+                    x += lit
+    path.write_bytes(bytes(out))
+
+
+@needs_oracle
+@pytest.mark.parametrize("rle,width", [(True, 64), (False, 64), (True, 8), (False, 5)])
+def test_hdr_environment_matches_reference_loader(tmp_path, rle, width):
+    """wfpt.assets.load_environment_map against the reference's
+    loadEnvironmentMap (stb_image) on run-length-encoded and flat files:
+    texels bit for bit, including zero-exponent texels and runs."""
+    rng = np.random.default_rng(width + rle)
+    h = 7
+    rgbe = rng.integers(0, 256, (h, width, 4)).astype(np.uint8)
+    rgbe[..., 3] = rng.integers(100, 160, (h, width))
+    rgbe[0, : width // 2] = (10, 20, 30, 130)   # a run in every channel
+    rgbe[1, 0] = (200, 100, 50, 0)              # exponent 0: black
+    path = tmp_path / "env.hdr"
+    _write_hdr(path, rgbe, rle=rle)
+    got = assets.load_environment_map(path)
+    want = oracle.load_environment(path)
+    assert got.shape == (h, width, 4) and want is not None
+    same_bits("environment texels", got, want)
+    assert got[1, 0, :3].sum() == 0 and (got[..., 3] == 1).all()
+
+
+@needs_oracle
+def test_hdr_environment_rejections(tmp_path):
+    bad = tmp_path / "bad.hdr"
+    _write_hdr(bad, np.zeros((2, 8, 4), np.uint8), header=b"#?RADIANCE\nFORMAT=32-bit_rle_xyze\n")
+    with pytest.raises(ValueError):
+        assets.load_environment_map(bad)
+    assert oracle.load_environment(bad) is None
+    notes = tmp_path / "notes.hdr"
+    notes.write_bytes(b"not an image\n")
+    with pytest.raises(ValueError):
+        assets.load_environment_map(notes)
+    assert oracle.load_environment(notes) is None
+
+
+def test_manifest_environment_becomes_the_scene_environment(tmp_path):
+    """A manifest's environment block (scene_manifest.cpp:146-168): the file,
+    resolved beside the manifest, its intensity and rotation."""
+    rgbe = np.full((4, 8, 4), (128, 128, 128, 129), np.uint8)
+    _write_hdr(tmp_path / "sky.hdr", rgbe)
+    manifest = tmp_path / "scene.json"
+    manifest.write_text(json.dumps({"name": "demo-sky", "preset": "demo",
+                                    "environment": {"file": "sky.hdr", "intensity": 2.5, "rotation_degrees": 30}}))
+    scene, cam = assets.preset_scene(manifest, 64, 48)
+    env = scene.environment
+    assert env["rgba"].shape == (4, 8, 4) and env["intensity"] == 2.5 and env["rotation"] == 30
+    assert np.allclose(env["rgba"][..., :3], 128 * 2.0 ** (129 - 136))

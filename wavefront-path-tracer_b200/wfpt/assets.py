@@ -1018,6 +1018,88 @@ def rtweek_scene(obj_path):
     return s
 
 
+def load_environment_map(path):
+    """loadEnvironmentMap (src/scene/environment.cpp:66-82): a Radiance .hdr
+    file as float RGBA texels (alpha 1), row 0 at the top, shape (h, w, 4).
+    The reference decodes it with stb_image's stbi_loadf; this is the same
+    decoding written from the file format: a text header that must start
+    with "#?RADIANCE" or "#?RGBE" and declare FORMAT=32-bit_rle_rgbe, the
+    resolution line "-Y height +X width", then scanlines that are either
+    flat RGBE or, for widths 8..32767, run-length encoded per channel
+    (2, 2, width >> 8, width & 255, then each channel as runs: a count above
+    128 repeats the next byte count - 128 times, otherwise count literal
+    bytes).  A texel is (r, g, b) * 2^(e - 136) in float32, or 0 when e is 0."""
+    data = Path(path).read_bytes()
+    pos = 0
+
+    def line():
+        nonlocal pos
+        end = data.find(b"\n", pos)
+        if end < 0:
+            raise ValueError(f"Could not decode HDR environment: {path}")
+        text = data[pos:end].decode("latin-1")
+        pos = end + 1
+        return text
+
+    magic = line()
+    if magic not in ("#?RADIANCE", "#?RGBE"):
+        raise ValueError(f"Environment must be a readable Radiance .hdr file: {path}")
+    valid = False
+    while True:
+        text = line()
+        if text == "":
+            break
+        if text == "FORMAT=32-bit_rle_rgbe":
+            valid = True
+    parts = line().split()
+    if not valid or len(parts) != 4 or parts[0] != "-Y" or parts[2] != "+X":
+        raise ValueError(f"Could not decode HDR environment: {path}")
+    height, width = int(parts[1]), int(parts[3])
+    if width <= 0 or height <= 0:
+        raise ValueError(f"Could not decode HDR environment: {path}")
+    rgbe = np.zeros((height, width, 4), np.uint8)
+    buf = np.frombuffer(data, np.uint8)
+    flat = width < 8 or width >= 32768
+    if not flat and pos + 4 <= len(buf):
+        c1, c2, c3 = int(buf[pos]), int(buf[pos + 1]), int(buf[pos + 2])
+        flat = c1 != 2 or c2 != 2 or (c3 & 0x80) != 0
+    if flat:  # the rest of the file is plain RGBE quadruples
+        need = width * height * 4
+        if pos + need > len(buf):
+            raise ValueError(f"Could not decode HDR environment: {path}")
+        rgbe[:] = buf[pos:pos + need].reshape(height, width, 4)
+    else:
+        for y in range(height):
+            if pos + 4 > len(buf) or buf[pos] != 2 or buf[pos + 1] != 2 or \
+                    (int(buf[pos + 2]) << 8 | int(buf[pos + 3])) != width:
+                raise ValueError(f"Could not decode HDR environment: {path}")
+            pos += 4
+            for ch in range(4):
+                x = 0
+                row = rgbe[y, :, ch]
+                while x < width:
+                    count = int(buf[pos])
+                    pos += 1
+                    if count > 128:
+                        count -= 128
+                        if x + count > width:
+                            raise ValueError(f"Could not decode HDR environment: {path}")
+                        row[x:x + count] = buf[pos]
+                        pos += 1
+                    else:
+                        if count == 0 or x + count > width:
+                            raise ValueError(f"Could not decode HDR environment: {path}")
+                        row[x:x + count] = buf[pos:pos + count]
+                        pos += count
+                    x += count
+    e = rgbe[..., 3].astype(np.int32)
+    scale = np.where(e != 0, np.ldexp(np.float32(1.0), e - 136).astype(np.float32), np.float32(0.0))
+    out = np.ones((height, width, 4), np.float32)
+    out[..., :3] = rgbe[..., :3].astype(np.float32) * scale[..., None]
+    out[..., :3][e == 0] = 0.0
+    return out
+
+
 def preset_scene(manifest, width, height):
     """The preset a manifest names, as RenderDriver builds it
     (createSceneFromConfig + applySceneConfig, src/scene/scene_factory.cpp:
@@ -1043,6 +1125,7 @@ def preset_scene(manifest, width, height):
         raise NotImplementedError(f"preset {c.preset} has no asset path")
     s.disable_normal_maps = not c.use_normal_maps
     s.normal_map_minimum_cosine = c.normal_map_minimum_cosine
-    if c.environment_file:
-        raise NotImplementedError("HDR environment files")
+    if c.environment_file:  # scene_factory.cpp:102-104
+        s.environment = dict(rgba=load_environment_map(c.environment_file), intensity=c.environment_intensity,
+                             rotation=c.environment_rotation_degrees)
     return s, cam

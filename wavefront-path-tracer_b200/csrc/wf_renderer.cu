@@ -178,7 +178,9 @@ WF_DEV void trace_stage(const DeviceScene& s, PathSoA ps, const uint32_t* queue,
             if (!more) break;
             continue;
         }
-        if (busy) {
+        uint32_t kind = lane_step_kind(busy, L.stage, L.ref);
+        uint32_t pick = warp_step_kind(kind);  // every lane of the warp takes part
+        if (busy && kind == pick) {
             closest_step(L, s, tally);
             if (L.stage == kStageDone) {
                 hit_a[i] = make_float4(L.h.t, L.h.u, L.h.v, __uint_as_float(L.h.prim));
@@ -425,7 +427,9 @@ WF_DEV void shadow_stage(DeviceScene s, const float4* shadow_origin, const float
             if (!more) break;
             continue;
         }
-        if (busy) {
+        uint32_t kind = lane_step_kind(busy, L.stage, L.ref);
+        uint32_t pick = warp_step_kind(kind);  // every lane of the warp takes part
+        if (busy && kind == pick) {
             any_step(L, s, tally);
             if (L.stage == kStageDone) result[j] = L.hit ? 1 : 0;
         }

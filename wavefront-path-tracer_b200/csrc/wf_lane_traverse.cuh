@@ -441,46 +441,6 @@ WF_DEV void any_step(AnyLane& L, const DeviceScene& s, Tally& tally) {
     any_pop(L, s, tally);
 }
 
-// Step types of a lane: 0 a BVH node, 1 a triangle leaf (BLAS or direct
-// BVH), 2 a TLAS leaf (instance entry or sphere), 3 nothing to do.
-WF_DEV uint32_t lane_step_kind(bool busy, uint32_t stage, int ref) {
-    if (!busy) return 3;
-    if (ref >= 0) return 0;
-    return stage == kStageTlas ? 2u : 1u;
-}
-
-// Which step type the warp runs this iteration (every lane of the warp
-// calls this).  The three types are separate branches of the step; a warp
-// that runs them all each iteration pays the triangle test and the instance
-// entry whenever one lane needs them, while most lanes wait at nodes.  So
-// the warp runs one type per iteration, and lanes at other types wait (Aila
-// and Laine's postponed leaves).  WF_LANE_GATE (a build setting) picks the
-// rule: 0 = every lane steps every iteration; 1 = the type with the most
-// lanes; n > 1 = nodes until fewer than n lanes need one, then the leaf
-// type with the most lanes.  Every lane's ray still takes its own steps in
-// its own order, so no result changes; only the interleaving of lanes does.
-#ifndef WF_LANE_GATE
-#define WF_LANE_GATE 1
-#endif
-WF_DEV uint32_t warp_step_kind(uint32_t kind) {
-#if WF_LANE_GATE == 0
-    return kind;  // every lane steps
-#else
-    uint32_t nodes = __popc(__ballot_sync(0xffffffffu, kind == 0));
-    uint32_t tris = __popc(__ballot_sync(0xffffffffu, kind == 1));
-    uint32_t tlas = __popc(__ballot_sync(0xffffffffu, kind == 2));
-#if WF_LANE_GATE == 1
-    // the type with the most lanes (ties to nodes, then triangles)
-    if (nodes >= tris && nodes >= tlas) return 0;
-    return tris >= tlas ? 1u : 2u;
-#else
-    // nodes until fewer than WF_LANE_GATE lanes need one
-    if (nodes >= WF_LANE_GATE || (nodes && !tris && !tlas)) return 0;
-    return tris >= tlas ? 1u : 2u;
-#endif
-#endif
-}
-
 // Lane refill: when at least `threshold` lanes of the warp are idle (or all
 // of them), the idle lanes take the next rays of [0, n) from `counter` with
 // one warp-aggregated atomic.  Returns the ray index for this lane, or

@@ -178,9 +178,7 @@ WF_DEV void trace_stage(const DeviceScene& s, PathSoA ps, const uint32_t* queue,
             if (!more) break;
             continue;
         }
-        uint32_t kind = lane_step_kind(busy, L.stage, L.ref);
-        uint32_t pick = warp_step_kind(kind);  // every lane of the warp takes part
-        if (busy && kind == pick) {
+        if (busy) {
             closest_step(L, s, tally);
             if (L.stage == kStageDone) {
                 hit_a[i] = make_float4(L.h.t, L.h.u, L.h.v, __uint_as_float(L.h.prim));
@@ -427,9 +425,7 @@ WF_DEV void shadow_stage(DeviceScene s, const float4* shadow_origin, const float
             if (!more) break;
             continue;
         }
-        uint32_t kind = lane_step_kind(busy, L.stage, L.ref);
-        uint32_t pick = warp_step_kind(kind);  // every lane of the warp takes part
-        if (busy && kind == pick) {
+        if (busy) {
             any_step(L, s, tally);
             if (L.stage == kStageDone) result[j] = L.hit ? 1 : 0;
         }
@@ -990,11 +986,12 @@ __global__ void __launch_bounds__(128, 8) k_trace_photons(const __grid_constant_
     }
 }
 
+// An order-preserving map of floats onto uint32, so the photon bounds can be
+// taken with integer atomicMin / atomicMax; build_photon_map decodes it.
 WF_DEV uint32_t float_order(float f) {
     uint32_t u = __float_as_uint(f);
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
-WF_DEV float order_float(uint32_t u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u); }
 
 __global__ void k_photon_bounds(const float4* photons, uint32_t count, uint32_t* bounds) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -498,12 +498,11 @@ wf_status wf_render_stats_get(wf_renderer* renderer, wf_render_stats* stats, uin
  * library holds until the process exits; tiles above 65,536 pixels return
  * WF_ERR_CAPACITY and configs with caustics return WF_ERR_UNSUPPORTED.
  * The first call on each device looks up the array's device address and the
- * kernel's resident grid (no allocation), so make that first call before any
- * stream capture; a device whose context was re-created (cudaDeviceReset)
- * gets the same set-up again on its next call.  Every call shares the one
- * array (it is reset at the start
- * of each call): calls whose GPU work overlaps, from several host threads or
- * streams, race and give wrong images.  The call returns after the work on
+ * kernel's resident grid (no allocation); a device whose context was
+ * re-created (cudaDeviceReset) gets the same set-up again on its next call.
+ * Every call shares the one array (it is reset at the start of each call):
+ * calls whose GPU work overlaps, from several host threads or streams, race
+ * and give wrong images.  The call returns after the work on
  * `stream` (cudaStream_t, may be NULL) has finished. */
 wf_status wf_render_tile_static(const wf_scene* scene, const wf_camera* camera,
                                 const wf_render_config* config, uint32_t x, uint32_t y,

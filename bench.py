@@ -637,17 +637,25 @@ def main():
     value = world * pixels * spp * args.steps / seconds / 1e6
     mrays = (stats["extension_rays"] + stats["shadow_rays"]) / seconds / 1e6
 
-    # End to end through the C-ABI task call with host buffers.
-    host = torch.empty((height, width, 3), dtype=torch.float32, pin_memory=True)
+    # End to end through the C-ABI task call with host buffers: every step
+    # renders its sample range and copies the frame's sums into pinned host
+    # memory; the copy of step i crosses PCIe while step i + 1 renders
+    # (wf_framebuffer_download_async), and the timed region ends when the
+    # last copy has arrived.
+    hosts = [torch.empty((height, width, 3), dtype=torch.float32, pin_memory=True) for _ in range(2)]
     lib = wfpt.library()
     renderer.render_task((0, 0, width, height), base + 999_000, spp)
+    wfpt.check(lib.wf_framebuffer_download_async(renderer.handle, 0, 0, width, height, hosts[0].data_ptr()))
+    wfpt.check(lib.wf_framebuffer_download_wait(renderer.handle))
     barrier()
     torch.cuda.synchronize()
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_start.record(stream)
     for i in range(args.steps):
         wfpt.check(lib.wf_render(renderer.handle, 0, 0, width, height, base + 1000 + i * spp, spp, 1))
-        wfpt.check(lib.wf_framebuffer_download(renderer.handle, 0, 0, width, height, host.data_ptr()))
+        wfpt.check(lib.wf_framebuffer_download_async(renderer.handle, 0, 0, width, height,
+                                                     hosts[i % 2].data_ptr()))
+    wfpt.check(lib.wf_framebuffer_download_wait(renderer.handle))
     e_end.record(stream)
     torch.cuda.synchronize()
     e_ms = e_start.elapsed_time(e_end)

@@ -450,6 +450,23 @@ wf_status wf_get_sample_index(wf_renderer* renderer, uint32_t* sample_index);
  * render_task.cu:101-108.) */
 wf_status wf_framebuffer_download(wf_renderer* renderer, uint32_t x, uint32_t y,
                                   uint32_t width, uint32_t height, float* rgb);
+/* Starts the copy of a tile's sums into host memory, as
+ * wf_framebuffer_download does, and returns without waiting.  The renderer
+ * first snapshots the tile on the device in stream order, so the wf_render
+ * calls made after this one run while the snapshot crosses PCIe (with
+ * page-locked `rgb` memory; pageable memory works, without the overlap).
+ * Two copies may be in flight; a third waits on the device for the oldest.
+ * `rgb` holds the data once wf_framebuffer_download_wait or wf_synchronize
+ * has returned.  The reference overlaps its checkpoint copies with
+ * rendering in the same way (enqueueAsyncCheckpoint, render_session.cuh:
+ * 22-26).  The first call allocates two framebuffer-sized device
+ * snapshots. */
+wf_status wf_framebuffer_download_async(wf_renderer* renderer, uint32_t x, uint32_t y,
+                                        uint32_t width, uint32_t height, float* rgb);
+/* Waits until every copy started by wf_framebuffer_download_async has
+ * arrived; work issued on the renderer's stream afterwards is ordered after
+ * those copies. */
+wf_status wf_framebuffer_download_wait(wf_renderer* renderer);
 /* Device address of the width*height*3 float framebuffer. */
 wf_status wf_framebuffer_device(wf_renderer* renderer, float** rgb);
 /* Waits for the renderer's work and reports the errors its kernels recorded:

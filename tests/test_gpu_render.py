@@ -189,6 +189,35 @@ def test_tiles_and_accumulation(cuda):
     r.close()
 
 
+@pytest.mark.parametrize("concurrent", [1, 2])
+def test_async_download_matches_each_step(cuda, concurrent):
+    """wf_framebuffer_download_async: each copy holds the framebuffer as it
+    stood when the call was made, although later renders (which clear and
+    rewrite the tile) were issued before the copies arrived; a third copy
+    reuses the first snapshot only after the first copy has left."""
+    scene, cam = scenes.cornell_box(64, 48)
+    cfg = wfpt.render_config(64, 48, max_depth=8, rr_start_depth=3, concurrent_tiles=concurrent)
+    dev = wfpt.DeviceScene(scene)
+    r = wfpt.Renderer(dev, cam, cfg)
+    want = []
+    for i in range(4):
+        r.render(0, 0, 64, 48, 10 + 2 * i, 2, True)
+        want.append(r.download())
+    got = [np.full((48, 64, 3), np.nan, np.float32) for _ in range(4)]
+    for i in range(4):
+        r.render(0, 0, 64, 48, 10 + 2 * i, 2, True)
+        r.download_async(got[i])
+    r.download_wait()
+    part = np.full((17, 24, 3), np.nan, np.float32)
+    r.download_async(part, 5, 7)
+    r.synchronize()
+    r.close()
+    dev.close()
+    for a, b in zip(got, want):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.array_equal(part.view(np.uint32), want[3][7:24, 5:29].view(np.uint32))
+
+
 def test_debug_views(cuda):
     scene, cam = scenes.cornell_box(32, 32)
     for debug in (abi.DEBUG_INTERSECTION, abi.DEBUG_SHADING_NORMAL):

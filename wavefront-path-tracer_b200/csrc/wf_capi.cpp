@@ -474,6 +474,7 @@ wf_status wf_get_sample_index(wf_renderer* r, uint32_t* sample_index) {
 wf_status wf_synchronize(wf_renderer* r) {
     if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
     uint32_t flags[2] = {0, 0};
+    if (r->copy_stream) WF_CUDA(cudaStreamSynchronize(r->copy_stream));
     wf_renderer* parts[2];
     for (int i = 0, n = renderer_parts(r, parts); i < n; ++i) {
         WF_CUDA(cudaStreamSynchronize(parts[i]->stream));
@@ -517,6 +518,49 @@ wf_status wf_framebuffer_download(wf_renderer* r, uint32_t x, uint32_t y, uint32
     WF_CUDA(cudaMemcpy2DAsync(rgb, size_t(w) * 12, r->framebuffer + (size_t(y) * c.width + x) * 3,
                               size_t(c.width) * 12, size_t(w) * 12, h, cudaMemcpyDeviceToHost, r->stream));
     return wf_synchronize(r);
+}
+
+wf_status wf_framebuffer_download_async(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, uint32_t h,
+                                        float* rgb) {
+    if (!r || !rgb) return fail(WF_ERR_INVALID_ARG, "null argument");
+    const wf_render_config& c = r->config;
+    if (w == 0 || h == 0 || x >= c.width || y >= c.height || w > c.width - x || h > c.height - y)
+        return fail(WF_ERR_INVALID_ARG, "download region outside the framebuffer");
+    if (!r->copy_stream) {
+        size_t full = size_t(c.width) * c.height * 3 * sizeof(float);
+        for (int k = 0; k < 2; ++k) {  // a call that failed half-way left some of these
+            if (!r->snapshot[k]) {
+                void* p = nullptr;
+                cudaError_t e = device_alloc(&p, full);
+                if (e != cudaSuccess) return cuda_fail(e, "framebuffer snapshot");
+                r->allocations.push_back(p);
+                r->device_bytes += full;
+                r->snapshot[k] = static_cast<float*>(p);
+            }
+            if (!r->snapshot_ready[k]) WF_CUDA(cudaEventCreateWithFlags(&r->snapshot_ready[k], cudaEventDisableTiming));
+            if (!r->copy_done[k]) WF_CUDA(cudaEventCreateWithFlags(&r->copy_done[k], cudaEventDisableTiming));
+        }
+        WF_CUDA(cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking));
+    }
+    uint32_t k = r->next_snapshot;
+    r->next_snapshot ^= 1u;
+    // the snapshot's previous copy must have left before it is overwritten
+    WF_CUDA(cudaStreamWaitEvent(r->stream, r->copy_done[k], 0));
+    WF_CUDA(cudaMemcpy2DAsync(r->snapshot[k], size_t(w) * 12, r->framebuffer + (size_t(y) * c.width + x) * 3,
+                              size_t(c.width) * 12, size_t(w) * 12, h, cudaMemcpyDeviceToDevice, r->stream));
+    WF_CUDA(cudaEventRecord(r->snapshot_ready[k], r->stream));
+    WF_CUDA(cudaStreamWaitEvent(r->copy_stream, r->snapshot_ready[k], 0));
+    WF_CUDA(cudaMemcpyAsync(rgb, r->snapshot[k], size_t(w) * h * 12, cudaMemcpyDeviceToHost, r->copy_stream));
+    WF_CUDA(cudaEventRecord(r->copy_done[k], r->copy_stream));
+    return WF_OK;
+}
+
+wf_status wf_framebuffer_download_wait(wf_renderer* r) {
+    if (!r) return fail(WF_ERR_INVALID_ARG, "null renderer");
+    if (!r->copy_stream) return WF_OK;
+    for (int k = 0; k < 2; ++k) WF_CUDA(cudaStreamWaitEvent(r->stream, r->copy_done[k], 0));
+    WF_CUDA(cudaStreamSynchronize(r->copy_stream));
+    return WF_OK;
 }
 
 wf_status wf_framebuffer_device(wf_renderer* r, float** rgb) {

@@ -1663,6 +1663,14 @@ wf_status renderer_destroy(wf_renderer* r) {
     if (r->twin) renderer_destroy(r->twin);
     if (r->twin_fork) cudaEventDestroy(r->twin_fork);
     if (r->twin_join) cudaEventDestroy(r->twin_join);
+    if (r->copy_stream) {
+        cudaStreamSynchronize(r->copy_stream);
+        cudaStreamDestroy(r->copy_stream);
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (r->snapshot_ready[k]) cudaEventDestroy(r->snapshot_ready[k]);
+        if (r->copy_done[k]) cudaEventDestroy(r->copy_done[k]);
+    }
     if (r->stream) cudaStreamSynchronize(r->stream);
     for (auto& slot : r->slots) {
         if (slot->writer.joinable()) slot->writer.join();

@@ -146,6 +146,12 @@ struct wf_renderer {
     bool external_framebuffer = false;
     uint32_t last_tile_parts = 1;  // which of {this, twin} rendered the last tile (bit 0, bit 1)
     cudaEvent_t twin_fork = nullptr, twin_join = nullptr;
+    // wf_framebuffer_download_async: two device snapshots of the framebuffer
+    // and the stream that copies them to the host
+    float* snapshot[2] = {nullptr, nullptr};
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t snapshot_ready[2] = {nullptr, nullptr}, copy_done[2] = {nullptr, nullptr};
+    uint32_t next_snapshot = 0;
 };
 
 namespace wf {

@@ -239,6 +239,8 @@ def declare(lib):
         "wf_set_sample_index": (S, [P, U32]),
         "wf_get_sample_index": (S, [P, C.POINTER(U32)]),
         "wf_framebuffer_download": (S, [P, U32, U32, U32, U32, P]),
+        "wf_framebuffer_download_async": (S, [P, U32, U32, U32, U32, P]),
+        "wf_framebuffer_download_wait": (S, [P]),
         "wf_framebuffer_device": (S, [P, C.POINTER(P)]),
         "wf_synchronize": (S, [P]),
         "wf_renderer_set_watchdog": (S, [P, U64, U32]),

@@ -351,6 +351,18 @@ class Renderer:
         check(library().wf_framebuffer_download(self.handle, x, y, w, h, out.ctypes.data))
         return out
 
+    def download_async(self, out, x=0, y=0):
+        """wf_framebuffer_download_async into `out`, a C-contiguous
+        (h, w, 3) float32 host array (numpy, or a torch CPU tensor, pinned
+        for the copy to overlap later renders); returns at once.  `out` holds
+        the tile once download_wait() has returned."""
+        h, w = int(out.shape[0]), int(out.shape[1])
+        ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+        check(library().wf_framebuffer_download_async(self.handle, x, y, w, h, ptr))
+
+    def download_wait(self):
+        check(library().wf_framebuffer_download_wait(self.handle))
+
     def sample_index(self):
         v = C.c_uint32()
         check(library().wf_get_sample_index(self.handle, C.byref(v)))

@@ -195,6 +195,7 @@ wf_status wf_scene_create(const wf_scene_desc* desc, wf_scene** out) {
     v.direct_instance_count = uint32_t(h.direct_instances.size());
     v.instance_count = uint32_t(h.instances.size());
     v.material_count = uint32_t(h.materials.size());
+    for (const Material& m : h.materials) s->material_categories |= 1u << material_category(m);
     v.light_count = uint32_t(h.lights.size());
     v.punctual_count = uint32_t(h.punctual.size());
     v.directional_count = h.directional_count;

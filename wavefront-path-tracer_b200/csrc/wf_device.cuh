@@ -161,6 +161,20 @@ struct Material {
 
 enum MaterialType : uint32_t { kDiffuse = 0, kMetal = 1, kDielectric = 2, kEmissive = 3, kSpecGloss = 4 };
 
+// Shading categories (the key of the material sort before shading):
+// 0 miss, 1 emissive, 2 diffuse, 3 metal, 4 dielectric, 5 other.
+constexpr uint32_t kShadeCategories = 6;
+WF_HDI uint32_t material_category(const Material& mat) {
+    if (mat.flags & kMatGltfPbr) return 5;
+    switch (mat.type) {
+    case kEmissive: return 1;
+    case kDiffuse: return mat.metallic > 0.5f ? 3 : 2;
+    case kMetal: return 3;
+    case kDielectric: return 4;
+    default: return 5;
+    }
+}
+
 // TextureBinding, include/scene/material.cuh:14-21.
 struct TexBinding {
     uint32_t texture;  // kInvalid: none

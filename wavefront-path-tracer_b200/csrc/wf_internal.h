@@ -97,6 +97,7 @@ struct wf_scene {
     double bvh_build_ms = 0.0;
     bool alpha_textures = false;  // some material is alpha-masked with an albedo texture
     bool textured = false;        // some material has a texture binding
+    uint32_t material_categories = 0;  // bit k: some material has shading category k (material_category)
     wf::Box bounds{};
     int device = 0;
 };

@@ -217,8 +217,6 @@ __global__ void __launch_bounds__(128, 8) k_trace_camera(DeviceScene s, PathSoA 
 // time, so they run one material branch instead of all of them.  Which warp
 // shades which path does not change any path's arithmetic: the outputs go to
 // the entry's own queue position.
-constexpr uint32_t kShadeCategories = 6;  // miss, emissive, diffuse, metal, dielectric, other
-
 WF_DEV uint32_t shade_category(const DeviceScene& s, float4 ha, uint32_t inst) {
     uint32_t prim = __float_as_uint(ha.w);
     uint32_t kind = hit_kind(prim), index = hit_index(prim);
@@ -233,15 +231,7 @@ WF_DEV uint32_t shade_category(const DeviceScene& s, float4 ha, uint32_t inst) {
             if (over != kInvalid) m = over;
         }
     }
-    const Material& mat = s.materials[m];
-    if (mat.flags & kMatGltfPbr) return 5;
-    switch (mat.type) {
-    case kEmissive: return 1;
-    case kDiffuse: return mat.metallic > 0.5f ? 3 : 2;
-    case kMetal: return 3;
-    case kDielectric: return 4;
-    default: return 5;
-    }
+    return material_category(s.materials[m]);
 }
 
 WF_DEV void classify_stage(const DeviceScene& s, const uint32_t* count, const float4* hit_a, const uint32_t* hit_inst, uint8_t* key, Counters* c) {
@@ -1237,12 +1227,15 @@ wf_status capture_graph(wf_renderer* r) {
             launch_trace<NoTally, true>(r, grid(r, 0, cap, r->block_trace), r->block_trace, st, 
                 s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, b, nullptr, r->refill,
                 nullptr, nullptr);
-        k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
-                                                          r->counters);
-        k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order, r->counters);
+        if (r->sort_shading) {
+            k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
+                                                              r->counters);
+            k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order, r->counters);
+        }
         launch_shade(r, grid(r, 1, cap, r->block_shade), r->block_shade, st, 
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
-            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers, r->shade_order);
+            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers,
+            r->sort_shading ? r->shade_order : nullptr);
         bool fork = r->params.photons.enabled != 0;
         if (fork) {  // gathers on a parallel branch: they and the shadow rays write different buffers
             WF_CUDA(cudaEventRecord(r->fork_event, st));
@@ -1316,12 +1309,15 @@ wf_status capture_stream_graph(wf_renderer* r) {
             s, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->counters, kMaxBounces, nullptr, r->refill,
             camera, nullptr);
         k_merge_camera<<<1, 1, 0, st>>>(r->counters, cur);
-        k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
-                                                          r->counters);
-        k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order, r->counters);
+        if (r->sort_shading) {
+            k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst, r->shade_key,
+                                                              r->counters);
+            k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order, r->counters);
+        }
         launch_shade(r, grid(r, 1, cap, r->block_shade), r->block_shade, st, 
             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms, r->shade_out,
-            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers, r->shade_order);
+            r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters, next_count, r->gathers,
+            r->sort_shading ? r->shade_order : nullptr);
         bool fork = r->params.photons.enabled != 0;
         if (fork) {  // gathers on a parallel branch: they and the shadow rays write different buffers
             WF_CUDA(cudaEventRecord(r->fork_event, st));
@@ -1506,6 +1502,11 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
     r->regenerate_percent = c.regenerate_percent ? std::min(c.regenerate_percent, 100u) : kDefaultRegeneratePercent;
     r->opaque = !scene->alpha_textures;
     r->textured = scene->textured;
+    // Sorting by category pays only when hits can need different long
+    // shading branches: with one of diffuse / metal / dielectric / other
+    // (misses and emitters are short) the sort's two launches per bounce
+    // would buy nothing.
+    r->sort_shading = __builtin_popcount(scene->material_categories & 0x3cu) > 1;
     if (stream) {
         r->stream = static_cast<cudaStream_t>(stream);
     } else {
@@ -1897,14 +1898,16 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                                 nullptr, r->refill, nullptr, nullptr);
                     };
                     auto shade = [&] {  // with the category sort it feeds on
-                        k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst,
-                                                                          r->shade_key, r->counters);
-                        k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key, r->shade_order,
-                                                                         r->counters);
+                        if (r->sort_shading) {
+                            k_classify<<<grid(r, 3, cap, 256), 256, 0, st>>>(s, cur_count, r->hit_a, r->hit_inst,
+                                                                              r->shade_key, r->counters);
+                            k_scatter<<<grid(r, 3, cap, 256), 256, 0, st>>>(cur_count, r->shade_key,
+                                                                             r->shade_order, r->counters);
+                        }
                         launch_shade(r, grid(r, 1, cap, r->block_shade), r->block_shade, st, 
                             s, r->params, r->paths, r->queue[cur], cur_count, r->hit_a, r->hit_inst, r->terms,
                             r->shade_out, r->shadow_origin, r->shadow_dir, r->shadow_capacity, r->counters,
-                            next_count, r->gathers, r->shade_order);
+                            next_count, r->gathers, r->sort_shading ? r->shade_order : nullptr);
                     };
                     auto gather = [&] {
                         k_gather<<<grid(r, 4, cap, r->block_gather), r->block_gather, 0, st>>>(r->params, r->gathers,

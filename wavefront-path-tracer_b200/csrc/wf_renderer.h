@@ -95,6 +95,7 @@ struct wf_renderer {
     bool own_stream = false;
     bool opaque = true;     // no alpha-textured material: the Opaque<> trace and shadow kernels
     bool textured = false;  // some textured material: k_shade<true>
+    bool sort_shading = true;  // material-sort the hits before shading (k_classify, k_scatter)
     int device = 0;
     int sm_count = 148;
     uint32_t capacity = 0;

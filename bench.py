@@ -48,14 +48,16 @@ WORKLOADS = {
     "sphere_field": (dict(width=1280, height=720), dict(max_depth=16)),
     "cornell": (dict(width=256, height=256), dict(max_depth=8, rr_start_depth=3)),
 }
-# Samples per pixel that one step renders (the streaming mode overlaps the
-# tail bounces of these samples).
-SPP_PER_STEP = {"large_mesh": 1, "large_mesh_medium": 1, "large_mesh_small": 4, "sphere_field": 4, "cornell": 16}
-# Schedule per workload: the streaming loop pays where deep paths are cheap
-# (sphere field, Cornell); on the large mesh regenerated camera rays lose
-# the coherence of a pure primary-ray bounce, so it replays the graph.
+# Samples per pixel that one step renders (of the configs' 256 / 64 / 16):
+# one step traces them as waves of several samples, whose long last bounces
+# share one chain of launches.  The medium case stays at one sample per step
+# for the ncu captures that index its launches.
+SPP_PER_STEP = {"large_mesh": 8, "large_mesh_medium": 1, "large_mesh_small": 4, "sphere_field": 16, "cornell": 16}
+# Schedule per workload when not autotuned: the per-wave graph, with this
+# many samples per wave (wf_render_config.samples_per_wave).
 DEFAULT_MODE = {"large_mesh": "graph", "large_mesh_medium": "graph", "large_mesh_small": "graph",
-                "sphere_field": "stream", "cornell": "stream"}
+                "sphere_field": "graph", "cornell": "graph"}
+DEFAULT_WAVE = {"large_mesh": 8, "large_mesh_medium": 1, "large_mesh_small": 4, "sphere_field": 16, "cornell": 16}
 MODES = {"graph": 0, "persistent": 1, "stream": 2}
 HBM_FALLBACK_GBS = 6650.0
 
@@ -72,7 +74,7 @@ def make_scene(name):
     return scene, cam, kw["width"], kw["height"], dict(rkw)
 
 
-def reference_cuda_comparison(workload, steps=5):
+def reference_cuda_comparison(workload, steps=5, own_mode=None, own_fields=None):
     """The reference's own CUDA renderer built for sm_100a
     (oracle/_ref/libwfref_cuda.so), in its graph and persistent schedules,
     and this renderer, timed the same way on the same whole-frame tasks in a
@@ -83,8 +85,12 @@ def reference_cuda_comparison(workload, steps=5):
     script = ROOT / "oracle" / "ref_cuda_bench.py"
     if not (ROOT / "oracle" / "_ref" / "libwfref_cuda.so").exists():
         return {"unavailable": "reference CUDA build absent (make -C oracle cuda)"}
-    run = subprocess.run([sys.executable, str(script), "--workload", workload, "--mode", "graph,persistent",
-                          "--steps", str(steps)], capture_output=True, text=True, timeout=1200, cwd=ROOT)
+    cmd = [sys.executable, str(script), "--workload", workload, "--mode", "graph,persistent", "--steps", str(steps)]
+    if own_mode:
+        cmd += ["--own-mode", own_mode]
+    if own_fields:
+        cmd += ["--own-fields", json.dumps(own_fields)]
+    run = subprocess.run(cmd, capture_output=True, text=True, timeout=1200, cwd=ROOT)
     if run.returncode != 0:
         return {"failed": (run.stdout + run.stderr)[-400:]}
     return json.loads(run.stdout.strip().splitlines()[-1])
@@ -528,6 +534,9 @@ def main():
                          "elementary functions (make -C wavefront-path-tracer_b200 fast)")
     ap.add_argument("--persistent-kernel", default="auto", choices=["auto", "fused", "staged"],
                     help="persistent mode: the fused per-path kernel, the staged kernel, or by tile size (default)")
+    ap.add_argument("--samples-per-wave", type=int, default=0,
+                    help="graph mode: samples of every pixel traced by one launch of the bounce chain "
+                         "(wf_render_config.samples_per_wave; 0 = per workload)")
     ap.add_argument("--regenerate-percent", type=int, default=0,
                     help="streaming mode: share of idle slots (%%) at which waiting slots start their next "
                          "samples together (0 = the renderer's default)")
@@ -574,33 +583,39 @@ def main():
     args.mode = args.mode or DEFAULT_MODE[args.workload]
     stages = {"auto": wfpt.abi.PERSISTENT_AUTO, "fused": wfpt.abi.PERSISTENT_FUSED,
               "staged": wfpt.abi.PERSISTENT_STAGED}[args.persistent_kernel]
-    cfg = wfpt.render_config(width, height, mode=MODES[args.mode], concurrent_tiles=args.concurrent_tiles,
-                             regenerate_percent=args.regenerate_percent, persistent_stages=stages, **rkw)
     spp = args.spp or SPP_PER_STEP[args.workload]
+    wave = args.samples_per_wave or min(spp, DEFAULT_WAVE[args.workload])
+    cfg = wfpt.render_config(width, height, mode=MODES[args.mode], concurrent_tiles=args.concurrent_tiles,
+                             regenerate_percent=args.regenerate_percent, persistent_stages=stages,
+                             samples_per_wave=wave, **rkw)
     tune = None
     if args.autotune:
         # wf_renderer_autotune: one timed frame of `spp` samples per candidate
         # (schedule, CTA size, refill threshold and the schedule's own
-        # setting); options given on the command line stay fixed
+        # settings); options given on the command line stay fixed
         modes = (MODES[args.mode],) if mode_given else (MODES["graph"], MODES["stream"])
+        waves = (args.samples_per_wave,) if args.samples_per_wave else tuple(sorted({1, max(1, wave // 2), wave}))
         t_tune = time.perf_counter()
         best, table = wfpt.autotune(
             dev_scene, cam, cfg, modes=modes, block_sizes=(128, 256), refill_thresholds=(8, 16),
             concurrent_tiles=(args.concurrent_tiles,) if args.concurrent_tiles else (1, 2),
             regenerate_percents=(args.regenerate_percent,) if args.regenerate_percent else (10, 25),
-            samples=spp, stream=stream.cuda_stream, key=f"{args.workload}/{spp}/{args.build}/{modes}")
+            samples_per_waves=waves, samples=spp, stream=stream.cuda_stream,
+            key=f"{args.workload}/{spp}/{args.build}/{modes}/{waves}")
         cfg = best
         args.mode = {v: k for k, v in MODES.items()}[cfg.mode]
         args.concurrent_tiles = cfg.concurrent_tiles
         tune = {"seconds": round(time.perf_counter() - t_tune, 2), "candidates": len(table),
                 "chosen": {"mode": args.mode, "block_size": cfg.block_size, "refill_threshold": cfg.refill_threshold,
-                           "concurrent_tiles": cfg.concurrent_tiles, "regenerate_percent": cfg.regenerate_percent},
+                           "concurrent_tiles": cfg.concurrent_tiles, "regenerate_percent": cfg.regenerate_percent,
+                           "samples_per_wave": cfg.samples_per_wave},
                 "frame_ms": [dict(c, ms=round(ms, 3)) for c, ms in table]}
     renderer = wfpt.Renderer(dev_scene, cam, cfg, stream=stream.cuda_stream)
     setup_s = time.perf_counter() - t_setup
     scene_bytes = dev_scene.info().device_bytes
     # path state (6 x 16 B), queues, hit records, terms and shadow requests per slot
-    renderer_bytes = width * height * (96 + 8 + 20 + 16 * 8 + 16 + 5 * 33 + 12)
+    slots = width * height * (max(1, cfg.samples_per_wave) if args.mode == "graph" else 1)
+    renderer_bytes = slots * (96 + 8 + 20 + 16 * 8 + 16 + 5 * 33) + width * height * 12
     pixels = width * height
     # Each rank owns its own absolute sample range (weak scaling).
     from wfpt import shard
@@ -712,7 +727,9 @@ def main():
 
     reference_cuda = None
     if rank == 0 and world == 1 and args.reference_cuda:
-        reference_cuda = reference_cuda_comparison(args.workload)
+        own = {k: getattr(cfg, k) for k in ("block_size", "refill_threshold", "concurrent_tiles",
+                                            "regenerate_percent", "samples_per_wave", "persistent_stages")}
+        reference_cuda = reference_cuda_comparison(args.workload, own_mode=args.mode, own_fields=own)
     guides = time_frame_guides(dev_scene, cam, width, height) if rank == 0 else None
 
     if rank == 0:
@@ -726,6 +743,7 @@ def main():
                        "photons": int(cfg.photon_count) if cfg.caustics else 0, "mode": args.mode,
                        "regenerate_percent": (cfg.regenerate_percent or None) if args.mode == "stream" else None,
                        "persistent_kernel": args.persistent_kernel if args.mode == "persistent" else None,
+                       "samples_per_wave": max(1, cfg.samples_per_wave) if args.mode == "graph" else None,
                        "build": args.build,
                        "wavefronts": 1 if args.mode != "graph" or args.concurrent_tiles == 1 else 2,
                        "block_size": cfg.block_size or 128, "refill_threshold": cfg.refill_threshold or 8,

@@ -409,6 +409,15 @@ typedef struct wf_render_config {
                                   (trace, shade, shadow rays inline, as persistentWavefrontTrace);
                                   WF_PERSISTENT_STAGED = the wavefront stages between grid barriers.
                                   Same sums either way. */
+    uint32_t samples_per_wave; /* graph mode and the staged persistent kernel: samples of every pixel
+                                  of the tile that one launch traces together (0 or 1 = one, as the
+                                  reference's per-sample replay; at most 1024; in persistent mode a
+                                  wave above 1 selects the staged kernel unless persistent_stages is
+                                  WF_PERSISTENT_FUSED, which ignores it).  The long last bounces of these
+                                  samples then share one chain of launches.  Each path's radiance is
+                                  added to the framebuffer after the launch, per pixel in sample
+                                  order, so the sums do not depend on it; queue memory grows with it,
+                                  and wf_queue_counts reports the counts of the whole launch. */
 } wf_render_config;
 enum { WF_PERSISTENT_AUTO = 0, WF_PERSISTENT_FUSED = 1, WF_PERSISTENT_STAGED = 2 };
 
@@ -542,6 +551,7 @@ typedef struct wf_tune_space {
     const uint32_t* tile_sizes;          uint32_t tile_size_count;          /* square tile edge = queue
                                                                                capacity; 0 = full frame */
     uint32_t samples;  /* samples per pixel of each timed frame (0 = 1) */
+    const uint32_t* samples_per_waves;   uint32_t samples_per_wave_count;   /* graph mode: samples per wave */
 } wf_tune_space;
 
 /* Single-scene autotuner (no counterpart in the reference, whose block size
@@ -552,14 +562,16 @@ typedef struct wf_tune_space {
  * keeps the fastest.  `best` receives that config; times_ms[i] (optional,
  * times_capacity entries) the frame time of candidate i in loop order
  * (modes outermost, then block sizes, refill thresholds, tile sizes, and the
- * mode's own settings: concurrent tiles; regenerate percents; persistent
- * stages, each fused one by chunk); *evaluated the number of candidates.  All candidates
+ * mode's own settings: concurrent tiles, each by samples per wave;
+ * regenerate percents; persistent stages, each fused one by chunk);
+ * *evaluated the number of candidates.  All candidates
  * render the same image, so the choice does not change any result. */
 wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, const wf_render_config* base,
                                const wf_tune_space* space, void* stream, wf_render_config* best,
                                float* times_ms, uint32_t times_capacity, uint32_t* evaluated);
 
-/* Kernel-level profile of one sample pass over the whole frame. */
+/* Kernel-level profile of one pass over the whole frame (one wave of
+ * samples_per_wave samples in graph mode, one sample otherwise). */
 enum { WF_KERNEL_RAYGEN = 0, WF_KERNEL_TRACE = 1, WF_KERNEL_SHADE = 2, WF_KERNEL_SHADOW = 3,
        WF_KERNEL_FINALIZE = 4, WF_KERNEL_PERSISTENT = 5, WF_KERNEL_GATHER = 6, WF_KERNEL_KINDS = 7 };
 enum { WF_PROFILE_BOUNCES = 32 };
@@ -579,10 +591,10 @@ typedef struct wf_kernel_profile {
     uint32_t bounce_extension_rays[WF_PROFILE_BOUNCES];
     uint32_t bounce_shadow_rays[WF_PROFILE_BOUNCES];
 } wf_kernel_profile;
-/* Renders one more sample over all tiles with every kernel launched eagerly
- * and bracketed by CUDA events on the renderer stream (the timing replay),
- * then one more with counting traversal kernels (the work tally).  The two
- * samples accumulate into the framebuffer and advance the sample index.
+/* Renders one more pass (a wave in graph mode) over all tiles with every
+ * kernel launched eagerly and bracketed by CUDA events on the renderer
+ * stream (the timing replay), then one more with counting traversal kernels
+ * (the work tally).  Both passes accumulate into the framebuffer.
  * Supplements the reference's --profile-queues record (render_driver.cu:393-400). */
 wf_status wf_profile_sample(wf_renderer* renderer, wf_kernel_profile* profile);
 

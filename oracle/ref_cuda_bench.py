@@ -53,7 +53,7 @@ def rel_rmse(image, reference):
 
 
 def compare(workload=None, modes=("graph", "persistent"), steps=5, spp=0, own_mode=None, sample_start=1000,
-            manifest=None, size="1280x720", caustics=True):
+            manifest=None, size="1280x720", caustics=True, own_fields=None):
     """Times the reference's CUDA renderer (each of `modes`) and this
     renderer on the same whole-frame tasks; returns the result dict."""
     import bench
@@ -78,6 +78,10 @@ def compare(workload=None, modes=("graph", "persistent"), steps=5, spp=0, own_mo
     own_mode = own_mode or bench.DEFAULT_MODE.get(workload, "graph")
     cfg = wfpt.render_config(width, height, **rkw)
     own_cfg = wfpt.render_config(width, height, mode=bench.MODES[own_mode], **rkw)
+    if own_mode == "graph" and workload in bench.DEFAULT_WAVE:
+        own_cfg.samples_per_wave = min(spp, bench.DEFAULT_WAVE[workload])
+    for k, v in (own_fields or {}).items():  # e.g. the settings bench.py's autotuner chose
+        setattr(own_cfg, k, v)
     cam_struct = native.camera_struct(cam)
     paths = width * height * spp
 
@@ -143,7 +147,8 @@ def compare(workload=None, modes=("graph", "persistent"), steps=5, spp=0, own_mo
         "workload": workload, "triangles": int(scene.triangle_count()), "width": width, "height": height,
         "spp_per_task": spp, "max_depth": cfg.max_depth,
         "caustics": int(cfg.caustics), "photons": int(cfg.photon_count) if cfg.caustics else 0,
-        "own_mode": own_mode, "reference_cuda": ref, "reference_scene_setup_s": round(ref_setup, 2),
+        "own_mode": own_mode, "own_samples_per_wave": max(1, own_cfg.samples_per_wave) if own_mode == "graph" else None,
+        "reference_cuda": ref, "reference_scene_setup_s": round(ref_setup, 2),
         "b200_renderer": {"Mpaths/s": paths / own_t / 1e3, "Mrays/s": rays_per_task / own_t / 1e3,
                           "ms_per_task": own_t, "ms_per_task_all": [round(x, 3) for x in own_ms],
                           "extension_rays_per_task": stats["extension_rays"] / steps,
@@ -202,6 +207,8 @@ def main():
     ap.add_argument("--manifest", default=None,
                     help="a scene manifest of the reference's presets, loaded by wfpt.assets, instead of a workload")
     ap.add_argument("--size", default="1280x720", help="image size for --manifest")
+    ap.add_argument("--own-fields", default="{}",
+                    help="JSON object of wf_render_config fields for the B200 renderer (e.g. the autotuned settings)")
     ap.add_argument("--batch-jobs", type=int, default=0,
                     help="render the batch workload's jobs one after another with the reference instead")
     args = ap.parse_args()
@@ -209,7 +216,7 @@ def main():
         print(json.dumps(batch_sequential(args.batch_jobs)), flush=True)
         return
     out = compare(args.workload, tuple(args.mode.split(",")), args.steps, args.spp, args.own_mode, args.sample_start,
-                  args.manifest, args.size, caustics=not args.no_caustics)
+                  args.manifest, args.size, caustics=not args.no_caustics, own_fields=json.loads(args.own_fields))
     print(json.dumps(out), flush=True)
 
 

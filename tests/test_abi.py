@@ -28,6 +28,17 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_fast_build_exports_every_declared_symbol():
+    """The fast build (when built) carries the same entry points: a stale
+    copy would fail every test that loads it."""
+    fast = wfpt.native.PACKAGE_DIR / "libwavefront_b200_fast.so"
+    if not fast.exists():
+        pytest.skip("fast build not built")
+    lib = ctypes.CDLL(str(fast))
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
 def test_python_mirror_declares_every_symbol():
     lib = ctypes.CDLL(str(wfpt.native.LIB_PATH))
     assert sorted(abi.declare(lib)) == declared_functions()
@@ -39,7 +50,7 @@ def test_struct_layouts_match_header():
     assert abi.MATERIAL_DTYPE.itemsize == 124
     assert abi.HIT_DTYPE.itemsize == 68
     assert ctypes.sizeof(abi.SceneDesc) == 184
-    assert ctypes.sizeof(abi.RenderConfig) == 132
+    assert ctypes.sizeof(abi.RenderConfig) == 136
     assert ctypes.sizeof(abi.Camera) == 56
 
 

@@ -189,6 +189,82 @@ def test_tiles_and_accumulation(cuda):
     r.close()
 
 
+@pytest.mark.parametrize("wave", [2, 3, 8])
+@pytest.mark.parametrize("concurrent,tiles", [(1, None), (2, None), (2, (32, 24))])
+def test_sample_waves_match_one_sample_per_launch(cuda, wave, concurrent, tiles):
+    """samples_per_wave: several samples of every pixel in one launch of the
+    bounce chain give the same sums and sample indices as one sample per
+    launch, for sample counts that do not divide into waves, for frames and
+    for tile tasks."""
+    results = []
+    for w in (1, wave):
+        fields = dict(max_depth=8, rr_start_depth=3, concurrent_tiles=concurrent, samples_per_wave=w)
+        if tiles:
+            fields.update(tile_width=tiles[0], tile_height=tiles[1])
+        scene, cam = scenes.cornell_box(64, 48)
+        cfg = wfpt.render_config(64, 48, **fields)
+        dev = wfpt.DeviceScene(scene)
+        r = wfpt.Renderer(dev, cam, cfg)
+        r.set_sample_index(40)
+        r.render_frame(7)
+        frame = r.download()
+        index = r.sample_index()
+        r.render(5, 7, 24, 17, 90, 5, True)
+        task = r.download()
+        after = r.sample_index()
+        stats = r.stats()
+        r.close()
+        dev.close()
+        results.append((frame, index, task, after, stats))
+    one, many = results
+    for a, b in ((one[0], many[0]), (one[2], many[2])):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert one[1] == many[1] == 47 and one[3] == many[3] == 95
+    for k in ("extension_rays", "shadow_rays", "paths"):
+        assert one[4][k] == many[4][k], k
+
+
+@pytest.mark.parametrize("wave", [2, 5])
+def test_persistent_sample_waves_match(cuda, wave):
+    """Waves in persistent mode (the staged kernel): the same sums and
+    sample indices as one sample per cooperative launch."""
+    results = []
+    for w in (1, wave):
+        scene, cam = scenes.cornell_box(64, 48)
+        cfg = wfpt.render_config(64, 48, max_depth=8, rr_start_depth=3, mode=abi.MODE_PERSISTENT,
+                                 persistent_stages=abi.PERSISTENT_STAGED, samples_per_wave=w)
+        dev = wfpt.DeviceScene(scene)
+        r = wfpt.Renderer(dev, cam, cfg)
+        r.set_sample_index(7)
+        r.render_frame(6)
+        frame = r.download()
+        index = r.sample_index()
+        task = r.render_task((3, 5, 30, 20), 50, 7)
+        r.close()
+        dev.close()
+        results.append((frame, index, task))
+    one, many = results
+    assert np.array_equal(one[0].view(np.uint32), many[0].view(np.uint32))
+    assert np.array_equal(one[2].view(np.uint32), many[2].view(np.uint32))
+    assert one[1] == many[1] == 13
+
+
+def test_sample_waves_large_mesh_bit_exact(cuda):
+    """A wave of 3 samples on the reduced large mesh (caustics, environment,
+    instances) against the host-compiled reference's sums."""
+    scene, cam = small_large_mesh()
+    w, h = int(round(cam["aspect_ratio"] * 54)), 54
+    cfg = wfpt.render_config(w, h, max_depth=12, samples_per_wave=3)
+    dev = wfpt.DeviceScene(scene)
+    r = wfpt.Renderer(dev, cam, cfg)
+    got = r.render_task((0, 0, w, h), 100, 4)
+    r.close()
+    dev.close()
+    ref = oracle.RefScene(scene, det=True)
+    want, _, _ = ref.render(cam, cfg, sample_start=100, sample_count=4)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
 @pytest.mark.parametrize("concurrent", [1, 2])
 def test_async_download_matches_each_step(cuda, concurrent):
     """wf_framebuffer_download_async: each copy holds the framebuffer as it

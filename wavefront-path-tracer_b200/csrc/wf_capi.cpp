@@ -373,9 +373,11 @@ wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, c
     for (uint32_t mode : modes) {
         // the mode's own settings: (setting, fused-kernel chunk) pairs
         std::vector<std::pair<uint32_t, uint32_t>> own;
-        if (mode == WF_MODE_GRAPH) {
+        if (mode == WF_MODE_GRAPH) {  // (concurrent tiles, samples per wave)
             for (uint32_t v : values(space->concurrent_tiles, space->concurrent_tiles_count, base->concurrent_tiles))
-                own.push_back({v, base->chunk});
+                for (uint32_t w :
+                     values(space->samples_per_waves, space->samples_per_wave_count, base->samples_per_wave))
+                    own.push_back({v, w});
         } else if (mode == WF_MODE_STREAM) {
             for (uint32_t v :
                  values(space->regenerate_percents, space->regenerate_percent_count, base->regenerate_percent))
@@ -401,6 +403,7 @@ wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, c
                         c.tile_width = c.tile_height = tile;
                         if (mode == WF_MODE_GRAPH) {
                             c.concurrent_tiles = setting.first;
+                            c.samples_per_wave = setting.second;
                         } else if (mode == WF_MODE_STREAM) {
                             c.regenerate_percent = setting.first;
                         } else {

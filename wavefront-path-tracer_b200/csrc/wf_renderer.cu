@@ -39,9 +39,13 @@ wf_status cuda_fail(cudaError_t e, const char* what) {
 
 namespace {
 
+// Camera rays of tile.samples samples (graph mode's wave; 1 elsewhere):
+// slot k * P + q is pixel q of the tile in sample sample_index + k, so each
+// sample's rays sit together in pixel order.
 WF_DEV void raygen_stage(RenderParams rp, const TileDev* tile_ptr, Counters* c, PathSoA ps, uint32_t* queue, uint32_t capacity) {
     TileDev tile = *tile_ptr;
-    uint32_t n = min(tile.width * tile.height, capacity);
+    uint32_t pixels = tile.width * tile.height;
+    uint32_t n = uint32_t(min(uint64_t(pixels) * tile.samples, uint64_t(capacity)));
     uint32_t sample = c->sample_index;
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
@@ -50,8 +54,9 @@ WF_DEV void raygen_stage(RenderParams rp, const TileDev* tile_ptr, Counters* c, 
         c->work_trace = 0;
     }
     for (uint32_t lp = gid; lp < n; lp += gridDim.x * blockDim.x) {
+        uint32_t k = lp / pixels;
         Path path;
-        init_path(rp, tile, sample, lp, path);
+        init_path(rp, tile, sample + k, lp - k * pixels, path);
         store_path(ps, lp, path);
         ps.radiance[lp] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         queue[lp] = lp;
@@ -460,6 +465,10 @@ WF_DEV void finalize_stage(PathSoA ps, const uint32_t* queue, const uint32_t* co
             alive = so.z != 0 && !(so.y >= 0 && !shadow_result[so.y]);
             if (alive) {
                 ps.radiance[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+            } else if (!kRegenerate && tile_ptr->samples > 1) {
+                // a wave of several samples: k_accumulate_wave adds the
+                // finished paths per pixel in sample order after the wave
+                ps.radiance[p] = make_float4(rad.x, rad.y, rad.z, 1.0f);
             } else {
                 uint32_t pixel = ps.info[p].x;
                 float* f = framebuffer + 3 * size_t(pixel);
@@ -478,6 +487,31 @@ WF_DEV void finalize_stage(PathSoA ps, const uint32_t* queue, const uint32_t* co
         out = __shfl_sync(0xffffffffu, out, 0);
         uint32_t rank = __popc(mask & ((1u << lane) - 1u));
         if (alive && out + rank < capacity) next[out + rank] = p;
+    }
+}
+
+// After a wave of several samples (graph mode): each pixel adds the
+// radiance of its finished paths in sample order, the order in which
+// one-sample launches would have added them, so the sums are the same.
+__global__ void k_accumulate_wave(PathSoA ps, const TileDev* tile_ptr, float* framebuffer, Counters* c) {
+    count_launch(c);
+    TileDev tile = *tile_ptr;
+    if (tile.samples <= 1) return;
+    uint32_t pixels = tile.width * tile.height;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < pixels; q += gridDim.x * blockDim.x) {
+        float* f = framebuffer + 3 * size_t(ps.info[q].x);
+        float r = f[0], g = f[1], b = f[2];
+        for (uint32_t k = 0; k < tile.samples; ++k) {
+            float4 rad = ps.radiance[size_t(k) * pixels + q];
+            if (rad.w != 0.0f) {
+                r += rad.x;
+                g += rad.y;
+                b += rad.z;
+            }
+        }
+        f[0] = r;
+        f[1] = g;
+        f[2] = b;
     }
 }
 
@@ -1253,6 +1287,9 @@ wf_status capture_graph(wf_renderer* r) {
             r->paths, r->queue[cur], cur_count, r->terms, r->shade_out, r->shadow_result, r->queue[nxt], next_count,
             cap, r->framebuffer, &r->counters->work_trace, r->params, r->tile, r->counters);
     }
+    if (r->wave > 1)
+        k_accumulate_wave<<<grid_for(r, r->tile_capacity, 256), 256, 0, st>>>(r->paths, r->tile, r->framebuffer,
+                                                                                r->counters);
     k_advance<<<1, 1, 0, st>>>(r->counters, r->tile);
     cudaError_t e = cudaStreamEndCapture(st, &r->graph);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
@@ -1425,7 +1462,7 @@ cudaError_t launch_fused(wf_renderer* r, cudaStream_t st, uint64_t paths) {
 constexpr uint64_t kStagedMinPaths = 262144;
 cudaError_t launch_persistent(wf_renderer* r, cudaStream_t st, uint64_t paths) {
     uint32_t k = r->config.persistent_stages;
-    bool staged = k == WF_PERSISTENT_STAGED || (k == WF_PERSISTENT_AUTO && paths >= kStagedMinPaths);
+    bool staged = k == WF_PERSISTENT_STAGED || r->wave > 1 || (k == WF_PERSISTENT_AUTO && paths >= kStagedMinPaths);
     return staged ? launch_phased(r, st, paths) : launch_fused(r, st, paths);
 }
 
@@ -1437,7 +1474,10 @@ wf_status launch_tile(wf_renderer* r, const TileDev& tile) {
         WF_CUDA(cudaGraphLaunch(r->graph_exec, r->stream));
         return WF_OK;
     }
-    WF_CUDA(launch_persistent(r, r->stream, uint64_t(tile.width) * tile.height));
+    WF_CUDA(launch_persistent(r, r->stream, uint64_t(tile.width) * tile.height * tile.samples));
+    if (tile.samples > 1)
+        k_accumulate_wave<<<grid_for(r, r->tile_capacity, 256), 256, 0, r->stream>>>(r->paths, r->tile,
+                                                                                     r->framebuffer, r->counters);
     k_advance<<<1, 1, 0, r->stream>>>(r->counters, r->tile);
     WF_CUDA(cudaGetLastError());
     return WF_OK;
@@ -1465,6 +1505,7 @@ wf_status check_render_config(const wf_scene* scene, const wf_render_config& c) 
     if (!(c.gather_radius > 0.0f))
         return fail(WF_ERR_INVALID_ARG, "Caustic gather radius must be greater than zero");
     if (c.refill_threshold > 32) return fail(WF_ERR_INVALID_ARG, "refill threshold must be between 0 and 32");
+    if (c.samples_per_wave > 1024) return fail(WF_ERR_INVALID_ARG, "samples_per_wave must be at most 1024");
     if (scene->view.punctual_count - scene->view.directional_count > 0 && scene->view.directional_count > 2)
         return fail(WF_ERR_UNSUPPORTED, "more than two directional lights");
     return WF_OK;
@@ -1490,7 +1531,14 @@ wf_status renderer_create_impl(const wf_scene* scene, const wf_camera* camera, c
     std::unique_ptr<wf_renderer, wf_status (*)(wf_renderer*)> r(new wf_renderer(), renderer_destroy);
     r->scene = scene;
     r->config = c;
-    r->capacity = uint32_t(std::min(capacity, pixels));
+    r->tile_capacity = uint32_t(std::min(capacity, pixels));
+    // waves: graph mode, and the staged persistent kernel (the fused one
+    // adds each path to the framebuffer itself)
+    bool waves = c.mode == WF_MODE_GRAPH || (c.mode == WF_MODE_PERSISTENT && c.persistent_stages != WF_PERSISTENT_FUSED);
+    r->wave = waves && c.samples_per_wave > 1 ? c.samples_per_wave : 1u;
+    if (uint64_t(r->tile_capacity) * r->wave > 0xffffffffull)
+        return fail(WF_ERR_INVALID_ARG, "samples_per_wave x tile pixels exceeds the supported queue index range");
+    r->capacity = r->tile_capacity * r->wave;
     WF_CUDA(cudaGetDevice(&r->device));
     WF_CUDA(cudaDeviceGetAttribute(&r->sm_count, cudaDevAttrMultiProcessorCount, r->device));
     r->grid_cap = uint32_t(r->sm_count) * 64;
@@ -1693,7 +1741,7 @@ wf_status renderer_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, ui
                           uint32_t sample_count, uint32_t clear) {
     const wf_render_config& c = r->config;
     if (w == 0 || h == 0 || x >= c.width || y >= c.height || w > c.width - x || h > c.height - y ||
-        uint64_t(w) * h > r->capacity)
+        uint64_t(w) * h > r->tile_capacity)
         return fail(WF_ERR_INVALID_ARG, "Render task tile is outside the prepared renderer bounds");
     if (sample_count == 0) return fail(WF_ERR_INVALID_ARG, "Render task sample range is empty");
     if (clear) {
@@ -1712,7 +1760,8 @@ wf_status renderer_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, ui
                                 t->stream));
         TileDev a{x, y, w, top, 1}, b{x, y + top, w, h - top, 1};
         r->last_tile_parts = 3;
-        for (uint32_t s = 0; s < sample_count; ++s) {
+        for (uint32_t s = 0; s < sample_count; s += a.samples) {
+            a.samples = b.samples = std::min(r->wave, sample_count - s);
             if (wf_status e = launch_tile(r, a)) return e;
             if (wf_status e = launch_tile(t, b)) return e;
         }
@@ -1726,8 +1775,10 @@ wf_status renderer_render(wf_renderer* r, uint32_t x, uint32_t y, uint32_t w, ui
         tile.samples = sample_count;
         return launch_tile(r, tile);
     }
-    for (uint32_t s = 0; s < sample_count; ++s)
+    for (uint32_t s = 0; s < sample_count; s += tile.samples) {
+        tile.samples = std::min(r->wave, sample_count - s);
         if (wf_status e = launch_tile(r, tile)) return e;
+    }
     r->last_tile_parts = 1;
     if (r->twin) {  // a one-row task ran here alone: the twin's sample index follows
         uint32_t end = sample_start + sample_count;
@@ -1780,31 +1831,38 @@ wf_status renderer_render_frame(wf_renderer* r, uint32_t sample_count) {
                                                         : (tiles.size() % 2 ? 1u : 2u);
         WF_CUDA(cudaEventRecord(r->twin_fork, r->stream));
         WF_CUDA(cudaStreamWaitEvent(twin->stream, r->twin_fork, 0));
-        for (uint32_t s = 0; s < sample_count; ++s)
+        for (uint32_t s = 0, k = 0; s < sample_count; s += k) {
+            k = std::min(r->wave, sample_count - s);
             for (int part = 0; part < 2; ++part) {
                 std::vector<TileDev>& list = part ? theirs : mine;
                 for (size_t t = 0; t < list.size(); ++t) {
                     TileDev tile = list[t];
                     tile.advance_sample = t + 1 == list.size() ? 1u : 0u;
+                    tile.samples = k;
                     if (wf_status e = launch_tile(part ? twin : r, tile)) return e;
                 }
                 if (list.empty() && part) {  // a single one-row frame: keep the twin's sample index in step
                     TileDev idle{0, 0, 0, 0, 1};
+                    idle.samples = k;
                     WF_CUDA(cudaMemcpyAsync(twin->tile, &idle, sizeof(TileDev), cudaMemcpyHostToDevice, twin->stream));
                     k_advance<<<1, 1, 0, twin->stream>>>(twin->counters, twin->tile);
                     WF_CUDA(cudaGetLastError());
                 }
             }
+        }
         WF_CUDA(cudaEventRecord(r->twin_join, twin->stream));
         WF_CUDA(cudaStreamWaitEvent(r->stream, r->twin_join, 0));
         return WF_OK;
     }
-    for (uint32_t s = 0; s < sample_count; ++s)
+    for (uint32_t s = 0, k = 0; s < sample_count; s += k) {
+        k = std::min(r->wave, sample_count - s);
         for (size_t t = 0; t < tiles.size(); ++t) {
             TileDev tile = tiles[t];
             tile.advance_sample = t + 1 == tiles.size() ? 1u : 0u;
+            tile.samples = k;
             if (wf_status e = launch_tile(r, tile)) return e;
         }
+    }
     return WF_OK;
 }
 
@@ -1868,7 +1926,8 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
         for (int pass = 0; pass < 2; ++pass) {
             bool count = pass == 1;
             if (count) WF_CUDA(cudaMemsetAsync(r->tally, 0, 2 * sizeof(TallyTotals), st));
-            for (const TileDev& tile : tiles) {
+            for (TileDev tile : tiles) {
+                tile.samples = r->wave;  // the graph's launches: one wave of samples
                 WF_CUDA(cudaMemcpyAsync(r->tile, &tile, sizeof(TileDev), cudaMemcpyHostToDevice, st));
                 auto raygen = [&] {
                     k_raygen<<<grid_for(r, cap, 256), 256, 0, st>>>(r->params, r->tile, r->counters, r->paths,
@@ -1966,6 +2025,10 @@ wf_status renderer_profile(wf_renderer* r, wf_kernel_profile* out) {
                         }
                     }
                 }
+                if (tile.samples > 1)
+                    k_accumulate_wave<<<grid_for(r, r->tile_capacity, 256), 256, 0, st>>>(r->paths, r->tile,
+                                                                                            r->framebuffer,
+                                                                                            r->counters);
                 k_advance<<<1, 1, 0, st>>>(r->counters, r->tile);
             }
             if (!count)

@@ -98,7 +98,9 @@ struct wf_renderer {
     bool sort_shading = true;  // material-sort the hits before shading (k_classify, k_scatter)
     int device = 0;
     int sm_count = 148;
-    uint32_t capacity = 0;
+    uint32_t capacity = 0;       // path slots: tile_capacity x wave
+    uint32_t tile_capacity = 0;  // pixels of the largest tile
+    uint32_t wave = 1;           // graph mode: samples per launch of the bounce chain (samples_per_wave)
     uint32_t block_trace = 128, block_shade = 128, block_finalize = 256, block_gather = 128, block_camera = 128;
     uint32_t grid_cap = 0;
     std::vector<void*> allocations;

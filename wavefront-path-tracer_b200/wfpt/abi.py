@@ -145,6 +145,7 @@ class RenderConfig(C.Structure):
         ("profile_queues", C.c_uint32), ("refill_threshold", C.c_uint32), ("concurrent_tiles", C.c_uint32),
         ("shadow_queue_capacity", C.c_uint32), ("regenerate_percent", C.c_uint32),
         ("persistent_stages", C.c_uint32),
+        ("samples_per_wave", C.c_uint32),
     ]
 
 
@@ -157,7 +158,8 @@ class TuneSpace(C.Structure):
                 ("chunks", C.c_void_p), ("chunk_count", C.c_uint32),
                 ("persistent_stages", C.c_void_p), ("persistent_stage_count", C.c_uint32),
                 ("tile_sizes", C.c_void_p), ("tile_size_count", C.c_uint32),
-                ("samples", C.c_uint32)]
+                ("samples", C.c_uint32),
+                ("samples_per_waves", C.c_void_p), ("samples_per_wave_count", C.c_uint32)]
 
 
 class BatchJob(C.Structure):

@@ -432,7 +432,7 @@ _TUNED = {}
 def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREAM), block_sizes=(128,),
              refill_thresholds=(4, 8, 16), concurrent_tiles=(1, 2), regenerate_percents=(10, 25),
              chunks=(), persistent_stages=(abi.PERSISTENT_FUSED, abi.PERSISTENT_STAGED), tile_sizes=(), samples=1,
-             stream=None, key=None, cache_path=None):
+             samples_per_waves=(), stream=None, key=None, cache_path=None):
     """wf_renderer_autotune: times one frame per candidate setting and
     returns (best RenderConfig, [(candidate settings, ms), ...]).
 
@@ -442,12 +442,12 @@ def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREA
     settings without rendering (the table is then empty)."""
     import json
     fields = ("mode", "block_size", "refill_threshold", "tile_width", "tile_height", "concurrent_tiles",
-              "regenerate_percent", "chunk", "persistent_stages")
+              "regenerate_percent", "chunk", "persistent_stages", "samples_per_wave")
     if key is None:
         key = repr((device_scene.handle.value, sorted((k, tuple(v) if hasattr(v, "__len__") else v)
                                                       for k, v in camera.items()),
                     bytes(config), modes, block_sizes, refill_thresholds, concurrent_tiles, regenerate_percents,
-                    chunks, persistent_stages, tile_sizes, samples))
+                    chunks, persistent_stages, tile_sizes, samples, samples_per_waves))
     stored = _TUNED.get(key)
     if stored is None and cache_path is not None and os.path.exists(cache_path):
         with open(cache_path) as f:
@@ -455,7 +455,7 @@ def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREA
     if stored is not None:
         best = abi.RenderConfig.from_buffer_copy(bytes(config))
         for k in fields:
-            setattr(best, k, stored[k])
+            setattr(best, k, stored.get(k, getattr(config, k)))
         return best, []
 
     def arr(v):
@@ -465,14 +465,16 @@ def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREA
     space = abi.TuneSpace()
     for name, vals in (("modes", modes), ("block_sizes", block_sizes), ("refill_thresholds", refill_thresholds),
                        ("concurrent_tiles", concurrent_tiles), ("regenerate_percents", regenerate_percents),
-                       ("chunks", chunks), ("persistent_stages", persistent_stages), ("tile_sizes", tile_sizes)):
+                       ("chunks", chunks), ("persistent_stages", persistent_stages), ("tile_sizes", tile_sizes),
+                       ("samples_per_waves", samples_per_waves)):
         a, n = arr(list(vals))
         lists[name] = a
         setattr(space, name, C.cast(a, C.c_void_p))
         count_field = {"modes": "mode_count", "block_sizes": "block_size_count",
                        "refill_thresholds": "refill_threshold_count", "concurrent_tiles": "concurrent_tiles_count",
                        "regenerate_percents": "regenerate_percent_count", "chunks": "chunk_count",
-                       "persistent_stages": "persistent_stage_count", "tile_sizes": "tile_size_count"}[name]
+                       "persistent_stages": "persistent_stage_count", "tile_sizes": "tile_size_count",
+                       "samples_per_waves": "samples_per_wave_count"}[name]
         setattr(space, count_field, n)
     space.samples = samples
     capacity = 4096
@@ -487,7 +489,9 @@ def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREA
     base_tile = config.tile_width if config.tile_width == config.tile_height else 0
     for mode in (modes or (config.mode,)):
         if mode == abi.MODE_GRAPH:
-            own = [{"concurrent_tiles": v} for v in (concurrent_tiles or (config.concurrent_tiles,))]
+            own = [{"concurrent_tiles": v, "samples_per_wave": w}
+                   for v in (concurrent_tiles or (config.concurrent_tiles,))
+                   for w in (samples_per_waves or (config.samples_per_wave,))]
         elif mode == abi.MODE_STREAM:
             own = [{"regenerate_percent": v} for v in (regenerate_percents or (config.regenerate_percent,))]
         else:

@@ -163,6 +163,14 @@ def ncu_summary(kernel, workload):
     return json.loads(p.read_text()) if p.exists() else {}
 
 
+def dram_traffic(kernel, workload, rays_per_launch):
+    """DRAM bytes of one launch: the ncu summary's DRAM bytes per ray
+    (dram__bytes_read + write of a captured launch over its rays) scaled to
+    this launch's rays, or None."""
+    per_ray = ncu_summary(kernel, workload).get("dram_bytes_per_ray")
+    return per_ray * rays_per_launch if per_ray and rays_per_launch else None
+
+
 def l2_term(kernel, workload, rays_per_launch, avg_ms):
     """L2 traffic of one launch from the ncu summary's L2 bytes per ray
     (lts__t_bytes of a captured launch over its rays), scaled to this
@@ -695,7 +703,7 @@ def main():
         rays_key = "extension_rays" if dominant == "trace" else "shadow_rays"
         roofline = {"bound": "hbm", "kernel": f"k_{dominant}", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": peak_kind,
-                    "traffic": ncu_summary(f"k_{dominant}", args.workload).get("dram_bytes_per_launch_full_size"),
+                    "traffic": dram_traffic(f"k_{dominant}", args.workload, profile[rays_key] / launches),
                     "l2": l2_term(f"k_{dominant}", args.workload, profile[rays_key] / launches, avg_ms),
                     "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
                     "kernel_share": {k: v["ms"] / total_ms for k, v in kernels.items()}}

@@ -751,7 +751,7 @@ def main():
                        "photons": int(cfg.photon_count) if cfg.caustics else 0, "mode": args.mode,
                        "regenerate_percent": (cfg.regenerate_percent or None) if args.mode == "stream" else None,
                        "persistent_kernel": args.persistent_kernel if args.mode == "persistent" else None,
-                       "samples_per_wave": max(1, cfg.samples_per_wave) if args.mode == "graph" else None,
+                       "samples_per_wave": max(1, cfg.samples_per_wave) if args.mode != "stream" else None,
                        "build": args.build,
                        "wavefronts": 1 if args.mode != "graph" or args.concurrent_tiles == 1 else 2,
                        "block_size": cfg.block_size or 128, "refill_threshold": cfg.refill_threshold or 8,

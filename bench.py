@@ -457,8 +457,15 @@ def run_batch(args):
     e_ms = max_over_ranks(a.elapsed_time(b))
     e2e = total_paths * args.steps / (e_ms / 1e3) / 1e6
 
-    # Sequential baseline: one per-job renderer each, rendered one after another.
-    renderers = [wfpt.Renderer(j["scene"], j["camera"], j["config"], stream=stream.cuda_stream) for j in jobs]
+    # Sequential baseline: one per-job renderer each, rendered one after
+    # another, each tracing its samples in waves (up to 16 per wave).
+    seq_configs = []
+    for j in jobs:
+        c = wfpt.abi.RenderConfig.from_buffer_copy(bytes(j["config"]))
+        c.samples_per_wave = min(j["sample_count"], args.sequential_wave)
+        seq_configs.append(c)
+    renderers = [wfpt.Renderer(j["scene"], j["camera"], c, stream=stream.cuda_stream)
+                 for j, c in zip(jobs, seq_configs)]
     for r, j in zip(renderers, jobs):
         r.render(0, 0, j["config"].width, j["config"].height, 0, j["sample_count"], True)
     torch.cuda.synchronize()
@@ -501,7 +508,8 @@ def run_batch(args):
             "e2e": {"value": e2e, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": sum(h.numel() * 4 for h in hosts)},
             "sequential": {"value": sequential, "unit": "Mpaths/s", "ms_per_step": s_ms / args.steps,
-                           "how": "one graph-mode renderer per job, rendered one after another"},
+                           "how": "one graph-mode renderer per job, rendered one after another, "
+                                  f"in waves of up to {args.sequential_wave} samples"},
             "speedup_vs_sequential": value / sequential,
             "reference_cuda_sequential": reference_sequential,
             "e2e_speedup_vs_reference_sequential": (e2e / reference_sequential["Mpaths/s"]
@@ -542,6 +550,8 @@ def main():
                          "elementary functions (make -C wavefront-path-tracer_b200 fast)")
     ap.add_argument("--persistent-kernel", default="auto", choices=["auto", "fused", "staged"],
                     help="persistent mode: the fused per-path kernel, the staged kernel, or by tile size (default)")
+    ap.add_argument("--sequential-wave", type=int, default=16,
+                    help="batch workload: samples per wave of the per-job sequential baseline")
     ap.add_argument("--samples-per-wave", type=int, default=0,
                     help="graph mode: samples of every pixel traced by one launch of the bounce chain "
                          "(wf_render_config.samples_per_wave; 0 = per workload)")

@@ -622,16 +622,21 @@ typedef struct wf_batch_job {
     uint32_t sample_count;
 } wf_batch_job;
 typedef struct wf_batch_config {
-    uint32_t slot_capacity;    /* paths in flight; 0 = min(total pixels, 4M) */
+    uint32_t slot_capacity;    /* paths in flight; 0 = min(paths of a pass, 4M) */
     uint32_t block_size;       /* trace/shade/shadow CTA size; 0 = 128 */
     uint32_t refill_threshold; /* as in wf_render_config; 0 = 8 */
     uint32_t longest_first;    /* 1 = start the jobs with the most samples x depth per pixel first */
+    uint32_t pass_paths;       /* paths (pixel samples) per pass, each holding a 16-byte radiance
+                                  record until its pixel adds it; 0 = 2^27 (2 GB) */
 } wf_batch_config;
 void wf_batch_config_default(wf_batch_config* config);
 wf_status wf_batch_create(const wf_batch_job* jobs, uint32_t job_count, const wf_batch_config* config,
                           void* stream, wf_batch** out);
-/* Renders every job's sample range once (one graph launch; asynchronous on
- * the batch stream), adding to the job framebuffers. */
+/* Renders every job's sample range once (one graph launch per pass of
+ * pass_paths paths; asynchronous on the batch stream), adding to the job
+ * framebuffers: each pixel adds its samples in sample order after the pass
+ * that traced them, so every framebuffer equals a per-job wf_render's.
+ * A batch holds fewer than 2^32 paths. */
 wf_status wf_batch_run(wf_batch* batch);
 wf_status wf_batch_synchronize(wf_batch* batch);
 wf_status wf_batch_reset(wf_batch* batch);   /* zero every job framebuffer */

@@ -1,9 +1,10 @@
 """Job batch (wf_batch_*): uneven jobs in one captured graph.
 
 Each job's framebuffer must equal a per-job render of the same sample range
-bit for bit (each pixel still adds its samples in order), with any slot
-capacity, including one far below the batch's pixel count, so that slots
-work through many (job, pixel) units one after another."""
+bit for bit (each pixel adds its samples in order after the pass that traced
+them), with any slot capacity, including one far below the batch's path
+count, so that slots work through many (job, sample, pixel) units one after
+another, and with passes that split jobs' sample ranges."""
 import numpy as np
 import pytest
 
@@ -42,11 +43,11 @@ def _per_job(job):
         r.close()
 
 
-@pytest.mark.parametrize("capacity", [0, 700])
-def test_batch_matches_per_job_renders(cuda, capacity):
+@pytest.mark.parametrize("capacity,pass_paths", [(0, 0), (700, 0), (0, 5003), (300, 1024)])
+def test_batch_matches_per_job_renders(cuda, capacity, pass_paths):
     jobs = _jobs()
     want = [_per_job(j) for j in jobs]
-    batch = wfpt.Batch(jobs, slot_capacity=capacity)
+    batch = wfpt.Batch(jobs, slot_capacity=capacity, pass_paths=pass_paths)
     try:
         for run in range(2):
             batch.reset()

@@ -1,16 +1,20 @@
 // Job batch: many independent renders (own scene, camera, resolution, depth,
 // sample range) in one captured CUDA graph.
 //
-// Work is a list of (job, pixel) units.  A pool of path slots runs the
-// wavefront stages of the single-scene renderer (lane-refill closest hit,
-// shading with deferred shadow rays, lane-refill occlusion, ordered term
-// accumulation and compaction) inside a device-side WHILE loop.  A slot
-// renders every sample of its unit in sample order, and only then takes
-// the next unit from a device counter, so every pixel adds its samples to
-// its job's framebuffer one after another exactly as a per-job wf_render
-// does: the framebuffers are bit-identical.  Jobs with few pixels or few
-// samples no longer pay per-launch and per-bounce overheads of their own,
-// and the slots of finished jobs immediately work on the others.
+// Work is a list of path units, one per (job, sample, pixel), job by job
+// and, within a job, sample by sample in pixel order.  A pool of path slots
+// runs the wavefront stages of the single-scene renderer (lane-refill
+// closest hit, shading with deferred shadow rays, lane-refill occlusion,
+// ordered term accumulation and compaction) inside a device-side WHILE
+// loop; a slot whose path ends stores the path's radiance by unit and takes
+// the next unit from a device counter, so the pool stays full until the
+// last paths of the pass.  After each pass, k_batch_accumulate adds every
+// pixel's radiances to its job's framebuffer in sample order, the order in
+// which a per-job wf_render adds them: the framebuffers are bit-identical.
+// Jobs with few pixels or few samples pay no per-launch and per-bounce
+// overheads of their own, and no pixel's samples form a serial chain.  A
+// batch of more units than one pass holds (the radiance buffer's size) runs
+// as several passes in unit order.
 #include "wf_wavefront.cuh"
 #include "wf_lane_traverse.cuh"
 
@@ -27,7 +31,7 @@ struct BatchJob {
     DeviceScene scene;
     RenderParams rp;
     unsigned long long fb_offset;  // first float of the job framebuffer
-    uint32_t unit_begin;           // first unit (pixel 0) of the job
+    uint32_t unit_begin;           // first unit of the job: unit_begin + k * pixels + q is sample k of pixel q
     uint32_t pixels;
     uint32_t sample_start, sample_count;
 };
@@ -35,11 +39,15 @@ struct BatchJob {
 // Device view of a batch (kernel parameter).
 struct BatchView {
     const BatchJob* jobs;
-    const uint32_t* unit_job;  // job of each unit
-    uint32_t units;
+    const uint32_t* job_order;    // jobs in unit order
+    const uint32_t* order_units;  // first unit of each job in unit order (ascending)
+    const uint32_t* order_pixels; // first pixel of each job in unit order, over all jobs' pixels
+    uint32_t job_count;
+    uint32_t units;               // path units of the whole batch
+    uint32_t pixels;              // pixels of all jobs
     uint32_t* slot_job;
     uint32_t* slot_unit;
-    uint32_t* slot_sample;     // sample of the slot's path, relative to its job's sample_start
+    float4* unit_radiance;        // radiance of each unit of the current pass, by unit - pass_begin
     float* framebuffer;
 };
 
@@ -57,7 +65,7 @@ struct wf_batch {
     size_t fb_floats = 0;
     wf::BatchView view{};
     wf::BatchJob* jobs_dev = nullptr;
-    uint32_t* unit_job = nullptr;
+    uint32_t* order_dev = nullptr;  // job_order, order_units, order_pixels
     wf::PathSoA paths{};
     uint32_t* queue[2] = {nullptr, nullptr};
     float4* hit_a = nullptr;
@@ -69,7 +77,7 @@ struct wf_batch {
     uint8_t* shadow_result = nullptr;
     uint32_t shadow_capacity = 0;
     wf::Counters* counters = nullptr;
-    uint32_t capacity = 0, units = 0, block = 128, refill = 8, max_depth = 1, max_samples = 1;
+    uint32_t capacity = 0, units = 0, pass_units = 0, block = 128, refill = 8, max_depth = 1;
     uint32_t grid_resident[4] = {0, 0, 0, 0};
     unsigned long long total_paths = 0;
     cudaGraph_t graph = nullptr;
@@ -85,35 +93,73 @@ namespace {
         if (wf_e_ != cudaSuccess) return cuda_fail(wf_e_, #call); \
     } while (0)
 
-// Starts sample `rel` of `unit` in `slot`.
-WF_DEV void batch_start(const BatchView& b, const PathSoA& ps, uint32_t slot, uint32_t unit, uint32_t rel) {
-    uint32_t job = b.unit_job[unit];
+// Position (in unit order) of the largest first value <= v in ascending `first`.
+WF_DEV uint32_t batch_position(const uint32_t* first, uint32_t count, uint32_t v) {
+    uint32_t lo = 0, hi = count;  // first[lo] <= v < first[hi]
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (first[mid] <= v) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Starts `unit` (a sample of one pixel of one job) in `slot`.
+WF_DEV void batch_start(const BatchView& b, const PathSoA& ps, uint32_t slot, uint32_t unit) {
+    uint32_t job = b.job_order[batch_position(b.order_units, b.job_count, unit)];
     const BatchJob& J = b.jobs[job];
+    uint32_t local = unit - J.unit_begin;
+    uint32_t k = local / J.pixels;
     TileDev tile{0, 0, J.rp.width, J.rp.height, 0};
     Path path;
-    init_path(J.rp, tile, J.sample_start + rel, unit - J.unit_begin, path);
+    init_path(J.rp, tile, J.sample_start + k, local - k * J.pixels, path);
     store_path(ps, slot, path);
     ps.radiance[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     b.slot_job[slot] = job;
     b.slot_unit[slot] = unit;
-    b.slot_sample[slot] = rel;
 }
 
-__global__ void k_batch_raygen(BatchView b, Counters* c, PathSoA ps, uint32_t* queue, uint32_t capacity,
-                               unsigned long long total_paths) {
+__global__ void k_batch_raygen(BatchView b, Counters* c, PathSoA ps, uint32_t* queue, uint32_t capacity) {
     count_launch(c);
-    uint32_t n = min(capacity, b.units);
+    uint32_t begin = c->pass_begin;
+    uint32_t n = min(capacity, c->pass_end - begin);
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) {
         c->queue_count[0] = n;
-        c->next_unit = n;
-        c->paths += total_paths;
+        c->next_unit = begin + n;
+        c->paths += c->pass_end - begin;
         c->work_trace = 0;
         c->stream_iterations = 0;
     }
     for (uint32_t slot = gid; slot < n; slot += gridDim.x * blockDim.x) {
-        batch_start(b, ps, slot, slot, 0);
+        batch_start(b, ps, slot, begin + slot);
         queue[slot] = slot;
+    }
+}
+
+// After a pass: every pixel of every job adds the radiances of its samples
+// in the pass to the job framebuffer, in sample order.
+__global__ void k_batch_accumulate(BatchView b, const Counters* c) {
+    uint32_t begin = c->pass_begin, end = c->pass_end;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < b.pixels; t += gridDim.x * blockDim.x) {
+        uint32_t pos = batch_position(b.order_pixels, b.job_count, t);
+        const BatchJob& J = b.jobs[b.job_order[pos]];
+        uint32_t q = t - b.order_pixels[pos];
+        uint64_t first = J.unit_begin, last = first + uint64_t(J.pixels) * J.sample_count;
+        if (last <= begin || first >= end) continue;
+        float* f = b.framebuffer + J.fb_offset + 3 * size_t(q);
+        float r = f[0], g = f[1], bl = f[2];
+        for (uint32_t k = 0; k < J.sample_count; ++k) {
+            uint64_t unit = first + uint64_t(k) * J.pixels + q;
+            if (unit < begin) continue;
+            if (unit >= end) break;
+            float4 rad = b.unit_radiance[unit - begin];
+            r += rad.x;
+            g += rad.y;
+            bl += rad.z;
+        }
+        f[0] = r;
+        f[1] = g;
+        f[2] = bl;
     }
 }
 
@@ -245,8 +291,8 @@ __global__ void k_batch_shadow(BatchView b, const float4* shadow_origin, const f
 }
 
 // Term accumulation, kill rule and compaction as in the single-scene
-// finalize; an ended path adds to its job framebuffer, then its slot starts
-// the unit's next sample or, when the unit is done, the next unit.
+// finalize; an ended path stores its radiance by unit (k_batch_accumulate
+// adds it after the pass), then its slot starts the pass's next unit.
 __global__ void k_batch_finalize(BatchView b, PathSoA ps, const uint32_t* queue, const uint32_t* count,
                                  const float4* terms, const int4* shade_out, const uint8_t* shadow_result,
                                  uint32_t* next, uint32_t* next_count, uint32_t capacity, Counters* c) {
@@ -274,18 +320,8 @@ __global__ void k_batch_finalize(BatchView b, PathSoA ps, const uint32_t* queue,
             if (alive) {
                 ps.radiance[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
             } else {
-                const BatchJob& J = b.jobs[b.slot_job[p]];
-                float* f = b.framebuffer + J.fb_offset + 3 * size_t(ps.info[p].x);
-                f[0] += rad.x;
-                f[1] += rad.y;
-                f[2] += rad.z;
-                uint32_t started = b.slot_sample[p] + 1;
-                if (started < J.sample_count) {
-                    batch_start(b, ps, p, b.slot_unit[p], started);
-                    alive = true;
-                } else {
-                    need_unit = true;
-                }
+                b.unit_radiance[b.slot_unit[p] - c->pass_begin] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+                need_unit = true;
             }
         }
         unsigned want = __ballot_sync(0xffffffffu, need_unit);
@@ -295,8 +331,8 @@ __global__ void k_batch_finalize(BatchView b, PathSoA ps, const uint32_t* queue,
             first = __shfl_sync(0xffffffffu, first, 0);
             if (need_unit) {
                 uint32_t unit = first + __popc(want & ((1u << lane) - 1u));
-                if (unit < b.units) {
-                    batch_start(b, ps, p, unit, 0);
+                if (unit < c->pass_end) {
+                    batch_start(b, ps, p, unit);
                     alive = true;
                 }
             }
@@ -311,7 +347,7 @@ __global__ void k_batch_finalize(BatchView b, PathSoA ps, const uint32_t* queue,
 }
 
 // Loop condition with a hard bound (every slot runs at most
-// units * max_samples * max_depth bounces in total).
+// units * max_depth bounces in a pass).
 __global__ void k_batch_condition(cudaGraphConditionalHandle handle, Counters* c, unsigned long long bound) {
     count_launch(c);
     uint32_t it = ++c->stream_iterations;
@@ -343,13 +379,35 @@ cudaError_t batch_resident(wf_batch* b, int kernel, K* fn, uint32_t block) {
     return e;
 }
 
+// Units per pass: the radiance buffer holds one float4 per unit of a pass
+// (2 GB at this size); larger batches run as several passes.
+constexpr uint64_t kBatchPassUnits = 1ull << 27;
+
+// One run of the batch: for each pass, the pass's units go to the device,
+// the graph renders them, and the pixels add their samples in order.
+cudaError_t batch_run(wf_batch* b) {
+    for (uint64_t begin = 0; begin < b->units; begin += b->pass_units) {
+        uint32_t range[2] = {uint32_t(begin), uint32_t(std::min<uint64_t>(b->units, begin + b->pass_units))};
+        cudaError_t e = cudaMemcpyAsync(&b->counters->pass_begin, range, sizeof(range), cudaMemcpyHostToDevice,
+                                        b->stream);
+        if (e == cudaSuccess) e = cudaGraphLaunch(b->exec, b->stream);
+        if (e == cudaSuccess) {
+            uint32_t blocks = std::max(1u, std::min((b->view.pixels + 255) / 256, uint32_t(b->sm_count) * 16));
+            k_batch_accumulate<<<blocks, 256, 0, b->stream>>>(b->view, b->counters);
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 wf_status capture_batch(wf_batch* b) {
     cudaStream_t st = b->stream;
     uint32_t cap = b->capacity;
     WF_BATCH_CUDA(cudaGraphCreate(&b->graph, 0));
     WF_BATCH_CUDA(cudaStreamBeginCaptureToGraph(st, b->graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     k_batch_raygen<<<std::max(1u, std::min((cap + 255) / 256, uint32_t(b->sm_count) * 16)), 256, 0, st>>>(
-        b->view, b->counters, b->paths, b->queue[0], cap, b->total_paths);
+        b->view, b->counters, b->paths, b->queue[0], cap);
     cudaGraph_t captured = nullptr;
     cudaError_t e = cudaStreamEndCapture(st, &captured);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (batch prologue)");
@@ -401,7 +459,7 @@ wf_status capture_batch(wf_batch* b) {
             b->view, b->paths, b->queue[cur], cur_count, b->terms, b->shade_out, b->shadow_result, b->queue[nxt],
             next_count, cap, b->counters);
     }
-    unsigned long long bound = (unsigned long long)b->units * b->max_samples * b->max_depth / 2 + 2;
+    unsigned long long bound = (unsigned long long)b->pass_units * b->max_depth / 2 + 2;
     k_batch_condition<<<1, 1, 0, st>>>(handle, b->counters, bound);
     e = cudaStreamEndCapture(st, &captured);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (batch body)");
@@ -484,7 +542,6 @@ wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_
                    uint64_t(jobs[c].sample_count) * jobs[c].config.max_depth;
         });
     std::vector<BatchJob> host(count);
-    std::vector<uint32_t> unit_job;
     uint64_t units = 0, fb = 0, max_directional = 0;
     for (uint32_t i = 0; i < count; ++i) {
         const wf_batch_job& j = jobs[i];
@@ -499,20 +556,27 @@ wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_
         fb += 3 * pixels;
         b->total_paths += pixels * j.sample_count;
         b->max_depth = std::max(b->max_depth, j.config.max_depth);
-        b->max_samples = std::max(b->max_samples, j.sample_count);
         max_directional = std::max<uint64_t>(max_directional, j.scene->view.directional_count);
     }
-    for (uint32_t job : order) {
-        uint64_t pixels = host[job].pixels;
+    // unit order: job by job (in `order`), each job sample by sample
+    std::vector<uint32_t> order_arrays(3 * size_t(count));
+    uint64_t pixels_total = 0;
+    for (uint32_t pos = 0; pos < count; ++pos) {
+        uint32_t job = order[pos];
         host[job].unit_begin = uint32_t(units);
-        units += pixels;
-        if (units > 0xffffffffull) return fail(WF_ERR_INVALID_ARG, "batch has more than 2^32 pixels");
-        unit_job.insert(unit_job.end(), size_t(pixels), job);
+        order_arrays[pos] = job;
+        order_arrays[count + pos] = uint32_t(units);
+        order_arrays[2 * size_t(count) + pos] = uint32_t(pixels_total);
+        units += uint64_t(host[job].pixels) * host[job].sample_count;
+        pixels_total += host[job].pixels;
+        if (units >= 0xffffffffull || pixels_total >= 0xffffffffull)
+            return fail(WF_ERR_INVALID_ARG, "batch has 2^32 or more paths");
     }
     b->units = uint32_t(units);
     b->fb_floats = fb;
+    b->pass_units = uint32_t(std::min<uint64_t>(units, config.pass_paths ? config.pass_paths : kBatchPassUnits));
     uint64_t cap = config.slot_capacity ? config.slot_capacity : std::min<uint64_t>(units, 4u << 20);
-    b->capacity = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(cap, units)));
+    b->capacity = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(cap, b->pass_units)));
 
     WF_BATCH_CUDA(cudaGetDevice(&b->device));
     WF_BATCH_CUDA(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, b->device));
@@ -524,11 +588,11 @@ wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_
     }
     uint32_t c = b->capacity;
     WF_BATCH_CUDA(batch_alloc(bp, &b->jobs_dev, count));
-    WF_BATCH_CUDA(batch_alloc(bp, &b->unit_job, units));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->order_dev, order_arrays.size()));
     WF_BATCH_CUDA(batch_alloc(bp, &b->view.framebuffer, fb));
     WF_BATCH_CUDA(batch_alloc(bp, &b->view.slot_job, c));
     WF_BATCH_CUDA(batch_alloc(bp, &b->view.slot_unit, c));
-    WF_BATCH_CUDA(batch_alloc(bp, &b->view.slot_sample, c));
+    WF_BATCH_CUDA(batch_alloc(bp, &b->view.unit_radiance, b->pass_units));
     WF_BATCH_CUDA(batch_alloc(bp, &b->paths.origin, c));
     WF_BATCH_CUDA(batch_alloc(bp, &b->paths.direction, c));
     WF_BATCH_CUDA(batch_alloc(bp, &b->paths.throughput, c));
@@ -549,15 +613,19 @@ wf_status batch_create(const wf_batch_job* jobs, uint32_t count, const wf_batch_
     WF_BATCH_CUDA(batch_alloc(bp, &b->counters, 1));
     WF_BATCH_CUDA(cudaMemcpyAsync(b->jobs_dev, host.data(), sizeof(BatchJob) * count, cudaMemcpyHostToDevice,
                                   b->stream));
-    WF_BATCH_CUDA(cudaMemcpyAsync(b->unit_job, unit_job.data(), sizeof(uint32_t) * units, cudaMemcpyHostToDevice,
-                                  b->stream));
+    WF_BATCH_CUDA(cudaMemcpyAsync(b->order_dev, order_arrays.data(), sizeof(uint32_t) * order_arrays.size(),
+                                  cudaMemcpyHostToDevice, b->stream));
     WF_BATCH_CUDA(cudaMemsetAsync(b->view.framebuffer, 0, sizeof(float) * fb, b->stream));
     WF_BATCH_CUDA(cudaMemsetAsync(b->counters, 0, sizeof(Counters), b->stream));
     b->paths.slot_sample = nullptr;
     b->paths.wait = nullptr;
     b->view.jobs = b->jobs_dev;
-    b->view.unit_job = b->unit_job;
+    b->view.job_order = b->order_dev;
+    b->view.order_units = b->order_dev + count;
+    b->view.order_pixels = b->order_dev + 2 * size_t(count);
+    b->view.job_count = count;
     b->view.units = b->units;
+    b->view.pixels = uint32_t(pixels_total);
     WF_BATCH_CUDA(b->opaque ? batch_resident(bp, 0, k_batch_trace<Opaque<NoTally>>, b->block)
                             : batch_resident(bp, 0, k_batch_trace<NoTally>, b->block));
     WF_BATCH_CUDA(b->textured ? batch_resident(bp, 1, k_batch_shade<true>, 128)
@@ -607,7 +675,7 @@ extern "C" wf_status wf_batch_create(const wf_batch_job* jobs, uint32_t job_coun
 
 extern "C" wf_status wf_batch_run(wf_batch* b) {
     if (!b) return fail(WF_ERR_INVALID_ARG, "null batch");
-    WF_BATCH_CUDA(cudaGraphLaunch(b->exec, b->stream));
+    WF_BATCH_CUDA(batch_run(b));
     return WF_OK;
 }
 
@@ -702,7 +770,7 @@ extern "C" wf_status wf_batch_autotune(const wf_batch_job* jobs, uint32_t job_co
                 cudaError_t err = cudaEventCreate(&e0);
                 if (err == cudaSuccess) err = cudaEventCreate(&e1);
                 if (err == cudaSuccess) err = cudaEventRecord(e0, b->stream);
-                if (err == cudaSuccess) err = cudaGraphLaunch(b->exec, b->stream);
+                if (err == cudaSuccess) err = batch_run(b);
                 if (err == cudaSuccess) err = cudaEventRecord(e1, b->stream);
                 if (err == cudaSuccess) err = cudaEventSynchronize(e1);
                 if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);

@@ -43,7 +43,8 @@ struct Counters {
     uint32_t work_dense;
     uint32_t shade_bucket[8];    // queue entries per shading category (current bounce)
     uint32_t shade_cursor[8];
-    uint32_t next_unit;          // job batch: next (job, pixel) unit to start
+    uint32_t next_unit;          // job batch: next (job, sample, pixel) unit to start
+    uint32_t pass_begin, pass_end;  // job batch: the units of the current pass
     unsigned long long extension_rays;
     unsigned long long shadow_rays;
     unsigned long long paths;

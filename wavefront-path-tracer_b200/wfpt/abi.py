@@ -169,7 +169,7 @@ class BatchJob(C.Structure):
 
 class BatchConfig(C.Structure):
     _fields_ = [("slot_capacity", C.c_uint32), ("block_size", C.c_uint32), ("refill_threshold", C.c_uint32),
-                ("longest_first", C.c_uint32)]
+                ("longest_first", C.c_uint32), ("pass_paths", C.c_uint32)]
 
 
 class DiffConfig(C.Structure):

@@ -526,7 +526,7 @@ class Batch:
     (render_config), sample_start, sample_count."""
 
     def __init__(self, jobs, slot_capacity=0, block_size=0, refill_threshold=0, longest_first=True, stream=None,
-                 config=None):
+                 config=None, pass_paths=0):
         arr = (abi.BatchJob * len(jobs))()
         self.jobs = list(jobs)
         for i, j in enumerate(jobs):
@@ -543,6 +543,7 @@ class Batch:
             config.block_size = block_size
             config.refill_threshold = refill_threshold
             config.longest_first = int(longest_first)
+            config.pass_paths = pass_paths
         self.config = config
         handle = C.c_void_p()
         check(library().wf_batch_create(arr, len(jobs), C.byref(config), stream, C.byref(handle)))

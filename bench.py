@@ -413,7 +413,7 @@ def run_batch(args):
     if not args.autotune:
         batch = wfpt.Batch(jobs, stream=stream.cuda_stream)
     else:
-        best, times = wfpt.Batch.autotune(jobs, slot_capacities=(1 << 20, 2 << 20, 4 << 20), block_sizes=(128, 256),
+        best, times = wfpt.Batch.autotune(jobs, slot_capacities=(4 << 20, 8 << 20, 16 << 20), block_sizes=(128, 256),
                                           refill_thresholds=(8,), stream=stream.cuda_stream)
         tune = {"candidates_ms": [round(t, 3) for t in times], "slot_capacity": best.slot_capacity,
                 "block_size": best.block_size, "refill_threshold": best.refill_threshold}

@@ -52,12 +52,12 @@ WORKLOADS = {
 # one step traces them as waves of several samples, whose long last bounces
 # share one chain of launches.  The medium case stays at one sample per step
 # for the ncu captures that index its launches.
-SPP_PER_STEP = {"large_mesh": 8, "large_mesh_medium": 1, "large_mesh_small": 4, "sphere_field": 16, "cornell": 16}
+SPP_PER_STEP = {"large_mesh": 16, "large_mesh_medium": 1, "large_mesh_small": 4, "sphere_field": 64, "cornell": 16}
 # Schedule per workload when not autotuned: the per-wave graph, with this
 # many samples per wave (wf_render_config.samples_per_wave).
 DEFAULT_MODE = {"large_mesh": "graph", "large_mesh_medium": "graph", "large_mesh_small": "graph",
                 "sphere_field": "graph", "cornell": "graph"}
-DEFAULT_WAVE = {"large_mesh": 8, "large_mesh_medium": 1, "large_mesh_small": 4, "sphere_field": 16, "cornell": 16}
+DEFAULT_WAVE = {"large_mesh": 16, "large_mesh_medium": 1, "large_mesh_small": 4, "sphere_field": 64, "cornell": 16}
 MODES = {"graph": 0, "persistent": 1, "stream": 2}
 HBM_FALLBACK_GBS = 6650.0
 

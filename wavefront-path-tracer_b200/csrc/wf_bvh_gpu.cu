@@ -4,8 +4,9 @@
 // The reference builds its BVH2s on the GPU with NexusBVH (an H-PLOC builder
 // in an un-vendored submodule, called at src/scene/scene.cu:148-149,227-228,
 // 262-264).  This is this build's GPU builder for the same role:
-//   1. primitive centroids are quantised to 21 bits per axis and interleaved
-//      into 63-bit Morton keys;
+//   1. primitive centroids are quantised to 21 bits per axis (one scale,
+//      the widest extent, for all axes) and interleaved into 63-bit Morton
+//      keys;
 //   2. a stable LSD radix sort (8-bit digits, hand-written) orders the
 //      primitives along the curve;
 //   3. clusters start as one leaf per primitive in that order; each round,
@@ -106,10 +107,15 @@ __global__ void k_morton(const BvhBox* prims, uint32_t n, const uint32_t* bounds
                          uint32_t* values) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    // One scale for all three axes (the widest extent), so that the curve
+    // follows physical distance: per-axis scales would give a flat scene's
+    // thin axis (a heightfield's height) as many bits as its wide ones and
+    // scatter neighbours along the curve.
     uint32_t q[3];
+    float extent = 0.0f;
+    for (int k = 0; k < 3; ++k) extent = fmaxf(extent, unordered(bounds[3 + k]) - unordered(bounds[k]));
     for (int k = 0; k < 3; ++k) {
-        float lo = unordered(bounds[k]), hi = unordered(bounds[3 + k]);
-        float extent = hi - lo;
+        float lo = unordered(bounds[k]);
         float c = 0.5f * (prims[i].lo[k] + prims[i].hi[k]);
         float t = extent > 0.0f ? (c - lo) / extent : 0.0f;
         t = fminf(fmaxf(t, 0.0f), 1.0f);

@@ -627,7 +627,7 @@ def main():
                 "chosen": {"mode": args.mode, "block_size": cfg.block_size, "refill_threshold": cfg.refill_threshold,
                            "concurrent_tiles": cfg.concurrent_tiles, "regenerate_percent": cfg.regenerate_percent,
                            "samples_per_wave": cfg.samples_per_wave},
-                "frame_ms": [dict(c, ms=round(ms, 3)) for c, ms in table]}
+                "frame_ms": [dict(c, ms=None if ms is None else round(ms, 3)) for c, ms in table]}
     renderer = wfpt.Renderer(dev_scene, cam, cfg, stream=stream.cuda_stream)
     setup_s = time.perf_counter() - t_setup
     scene_bytes = dev_scene.info().device_bytes

@@ -564,7 +564,9 @@ typedef struct wf_tune_space {
  * (modes outermost, then block sizes, refill thresholds, tile sizes, and the
  * mode's own settings: concurrent tiles, each by samples per wave;
  * regenerate percents; persistent stages, each fused one by chunk);
- * *evaluated the number of candidates.  All candidates
+ * *evaluated the number of candidates.  A candidate whose buffers do not
+ * fit in device memory is skipped (its time is +inf; WF_ERR_OOM when none
+ * fits).  All candidates
  * render the same image, so the choice does not change any result. */
 wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, const wf_render_config* base,
                                const wf_tune_space* space, void* stream, wf_render_config* best,

@@ -3,6 +3,7 @@
 
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
@@ -370,6 +371,7 @@ wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, c
     uint32_t samples = space->samples ? space->samples : 1u;
     uint32_t count = 0;
     float best_ms = 0.0f;
+    bool have_best = false;
     for (uint32_t mode : modes) {
         // the mode's own settings: (setting, fused-kernel chunk) pairs
         std::vector<std::pair<uint32_t, uint32_t>> own;
@@ -411,7 +413,14 @@ wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, c
                             c.chunk = setting.second;
                         }
                         wf_renderer* r = nullptr;
-                        if (wf_status e = renderer_create(scene, camera, &c, stream, &r)) return e;
+                        if (wf_status e = renderer_create(scene, camera, &c, stream, &r)) {
+                            if (e != WF_ERR_OOM) return e;
+                            // a candidate whose queues do not fit (a large wave) is skipped
+                            cudaGetLastError();
+                            if (times_ms && count < times_capacity) times_ms[count] = INFINITY;
+                            ++count;
+                            continue;
+                        }
                         cudaEvent_t e0 = nullptr, e1 = nullptr;
                         float ms = 0.0f;
                         wf_status st = renderer_render_frame(r, samples);
@@ -430,14 +439,16 @@ wf_status wf_renderer_autotune(const wf_scene* scene, const wf_camera* camera, c
                         if (st != WF_OK) return st;
                         if (err != cudaSuccess) return cuda_fail(err, "autotune timing");
                         if (times_ms && count < times_capacity) times_ms[count] = ms;
-                        if (count == 0 || ms < best_ms) {
+                        if (!have_best || ms < best_ms) {
                             best_ms = ms;
                             *best = c;
+                            have_best = true;
                         }
                         ++count;
                     }
     }
     if (evaluated) *evaluated = count;
+    if (!have_best) return fail(WF_ERR_OOM, "no autotune candidate fits in device memory");
     return WF_OK;
 }
 

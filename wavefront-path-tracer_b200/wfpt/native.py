@@ -506,7 +506,8 @@ def autotune(device_scene, camera, config, modes=(abi.MODE_GRAPH, abi.MODE_STREA
                 for t in (tile_sizes or (base_tile,)):
                     for o in own:
                         table.append(dict({"mode": mode, "block_size": b, "refill_threshold": rf, "tile": t}, **o))
-    table = [(cand, times[i]) for i, cand in enumerate(table[:evaluated.value])]
+    # a candidate skipped for lack of device memory has no time (None)
+    table = [(cand, times[i] if times[i] != float("inf") else None) for i, cand in enumerate(table[:evaluated.value])]
     chosen = {k: getattr(best, k) for k in fields}
     _TUNED[key] = chosen
     if cache_path is not None:

@@ -686,6 +686,29 @@ wf_status wf_diff_backward(const wf_scene* scene, const wf_camera* camera, const
                            const float* albedo, const float* roughness, float emission_scale,
                            const float* d_image, double* d_albedo, double* d_roughness,
                            double* d_emission_scale, void* stream);
+/* Albedo gradients of the renderer's own image (no counterpart in the
+ * reference).  Replays samples [sample_start, sample_start + sample_count)
+ * of the pixels of the tile (x, y, width, height) with the renderer's
+ * shading, and ADDS to gradient[3*m .. 3*m+2] the derivative of
+ * sum over pixels and channels of adjoint * (sum of the samples' radiance)
+ * with respect to the RGB albedo of materials[m].  The random numbers are
+ * those wf_render draws, and Russian roulette's 1/survival weight is held
+ * constant: the result is the exact derivative of each sample's estimate
+ * for the survival decisions it drew (exact outright when rr_start_depth
+ * >= max_depth), an unbiased estimate of the gradient of the expected
+ * image.  When `image` is not null the replay also writes the tile's
+ * sample sums there, bit for bit the framebuffer wf_render leaves after
+ * rendering the same samples from a cleared framebuffer.  The parameter
+ * materials (1 to 8, distinct) must be untextured, non-metallic diffuse
+ * materials with non-zero albedo; the renderer must have caustics off,
+ * indirect_clamp 0 and no debug view (WF_ERR_UNSUPPORTED otherwise).
+ * `materials` is a host array; adjoint, image and gradient are device
+ * arrays (adjoint and image full width x height x 3 floats).  Runs on the
+ * renderer's stream and synchronizes it. */
+wf_status wf_render_albedo_gradient(wf_renderer* renderer, uint32_t x, uint32_t y, uint32_t width,
+                                    uint32_t height, uint32_t sample_start, uint32_t sample_count,
+                                    const uint32_t* materials, uint32_t material_count, const float* adjoint,
+                                    float* image, double* gradient);
 
 /* -------------------------------------------------------------- checkpoint */
 /* Checkpoint file: header {magic "PTCHKPT1", version 3, width, height,

@@ -223,6 +223,7 @@ def declare(lib):
         "wf_render_frame": (S, [P, U32]),
         "wf_diff_forward": (S, [P, C.POINTER(Camera), C.POINTER(DiffConfig), P, P, F, P, P]),
         "wf_diff_backward": (S, [P, C.POINTER(Camera), C.POINTER(DiffConfig), P, P, F, P, P, P, P, P]),
+        "wf_render_albedo_gradient": (S, [P, U32, U32, U32, U32, U32, U32, P, U32, P, P, P]),
         "wf_renderer_autotune": (S, [P, C.POINTER(Camera), C.POINTER(RenderConfig), C.POINTER(TuneSpace), P,
                                      C.POINTER(RenderConfig), P, U32, C.POINTER(U32)]),
         "wf_batch_config_default": (None, [C.POINTER(BatchConfig)]),

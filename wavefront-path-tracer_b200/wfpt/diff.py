@@ -6,6 +6,11 @@ and its backward is the path-replay adjoint of wf_diff_backward, which
 re-traces every path from its RNG key instead of storing it.  Parameters are
 CUDA float32 tensors: albedo (N, 3), roughness (N,) in radians, emission
 scale (1,).  The image is (height, width, 3).
+
+`albedo_gradient(renderer, materials, adjoint, ...)` differentiates the
+production renderer instead (wf_render_albedo_gradient): the gradient of
+sum(adjoint * image) with respect to the albedo of diffuse materials of the
+renderer's scene, replaying its own shading.
 """
 import ctypes as C
 
@@ -71,3 +76,31 @@ class DiffRender(torch.autograd.Function):
 
 def render(scene, camera, config, albedo, roughness, emission_scale):
     return DiffRender.apply(albedo, roughness, emission_scale, scene, camera, config)
+
+
+def albedo_gradient(renderer, materials, adjoint, tile=None, sample_start=0, sample_count=1, image=False):
+    """wf_render_albedo_gradient: gradients of the production renderer's image.
+
+    Returns the float64 (len(materials), 3) derivative of
+    sum(adjoint * image) with respect to the RGB albedo of each listed
+    diffuse material, where image is the sum of samples
+    [sample_start, sample_start + sample_count) that `renderer` (a
+    wfpt.Renderer) renders over `tile` (x, y, w, h; default the whole
+    image); Russian roulette's weights are held constant.  `adjoint` is a
+    (height, width, 3) CUDA float32 tensor.  With image=True also returns
+    the replayed (height, width, 3) image (only the tile is written), equal
+    bit for bit to what renderer.render_task returns for the same tile and
+    samples."""
+    x, y, w, h = tile if tile is not None else (0, 0, renderer.width, renderer.height)
+    adjoint = adjoint.contiguous().float()
+    if tuple(adjoint.shape) != (renderer.height, renderer.width, 3):
+        raise ValueError("adjoint must be (height, width, 3)")
+    ids = (C.c_uint32 * len(materials))(*[int(m) for m in materials])
+    grad = torch.zeros((len(materials), 3), dtype=torch.float64, device=adjoint.device)
+    out = torch.zeros_like(adjoint) if image else None
+    torch.cuda.current_stream().synchronize()  # the call runs on the renderer's stream
+    check(library().wf_render_albedo_gradient(renderer.handle, x, y, w, h, sample_start, sample_count, ids,
+                                              len(materials), C.c_void_p(adjoint.data_ptr()),
+                                              C.c_void_p(out.data_ptr()) if image else None,
+                                              C.c_void_p(grad.data_ptr())))
+    return (grad, out) if image else grad

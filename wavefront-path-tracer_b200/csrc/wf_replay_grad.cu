@@ -75,11 +75,14 @@ struct GradSink : InlineSink<Tally> {
     }
 };
 
+// Bounded to 8 CTAs of 128 per SM like the fused persistent kernel, whose
+// traversal it shares: four times the resident warps of the unbounded
+// build hide more of the dependent node loads than the spills cost.
 template <typename Tally, bool kTextures>
-__global__ void __launch_bounds__(128) k_albedo_gradient(const __grid_constant__ DeviceScene s,
-                                                         const __grid_constant__ RenderParams rp, TileDev tile,
-                                                         uint32_t sample_start, uint32_t samples, GradParams gp,
-                                                         const float* adjoint, float* image, double* gradient) {
+__global__ void __launch_bounds__(128, 8) k_albedo_gradient(const __grid_constant__ DeviceScene s,
+                                                            const __grid_constant__ RenderParams rp, TileDev tile,
+                                                            uint32_t sample_start, uint32_t samples, GradParams gp,
+                                                            const float* adjoint, float* image, double* gradient) {
     __shared__ double block_grad[3 * kGradMaterials];
     for (uint32_t k = threadIdx.x; k < 3 * kGradMaterials; k += blockDim.x) block_grad[k] = 0.0;
     __syncthreads();
@@ -195,7 +198,7 @@ extern "C" wf_status wf_render_albedo_gradient(wf_renderer* r, uint32_t x, uint3
     cudaStream_t st = r->stream;
     TileDev tile{x, y, width, height, 0};
     uint32_t pixels = width * height;
-    uint32_t blocks = std::max(1u, std::min((pixels + 127) / 128, uint32_t(r->sm_count) * 16));
+    uint32_t blocks = (pixels + 127) / 128;  // one pixel per thread; the hardware balances the CTAs
     // The variants of the fused persistent kernel: the alpha test only when
     // some material is alpha-textured, the texture code only when one is
     // textured.

@@ -1,16 +1,17 @@
 """Albedo gradients of the production renderer (wf_render_albedo_gradient).
 
 * The replay's image is bit for bit the framebuffer wf_render leaves for the
-  same tile and samples (graph mode with and without sample waves, the
-  persistent mode; Russian roulette on; the three scenes below), so the
-  gradient belongs to the image the renderer actually makes.
+  same tile and samples (graph mode with and without sample waves and with
+  two wavefronts, the persistent and streaming modes; Russian roulette on;
+  the three scenes below), so the gradient belongs to the image the
+  renderer actually makes.
 * With Russian roulette off the gradient is the exact derivative of the
   image: it matches central finite differences of wf_render (eps = 1e-3 on
   one albedo channel at a time, fresh scene per evaluation) on the Cornell
   box, the sphere field (glass, metal and sky on the paths) and a small
   large-mesh scene (instanced rocks, emissive terrain triangles, glass
   spheres, HDR sun-and-sky environment), within 1e-3 of each entry plus
-  1e-4 of the largest.
+  1e-4 of the largest; on the sphere field also with 8 materials at once.
 * With Russian roulette on (weights held constant) it estimates the same
   gradient: 256 samples per pixel agree with the roulette-free gradient
   within 2 % of the gradient's norm.
@@ -32,12 +33,12 @@ def _cornell():
     return scene, cam, [0, 1, 2, 3]
 
 
-def _sphere_field():
+def _sphere_field(spheres=2):
     scene, cam = scenes.sphere_field(96, 54, frequency=16)
     mats = scene.materials
-    spheres = [k for k in range(4, len(mats))
-               if mats[k]["type"] == abi.MAT_DIFFUSE and mats[k]["albedo"].min() > 0.1][:2]
-    return scene, cam, [0, 3] + spheres
+    picked = [k for k in range(4, len(mats))
+              if mats[k]["type"] == abi.MAT_DIFFUSE and mats[k]["albedo"].min() > 0.1][:spheres]
+    return scene, cam, [0, 3] + picked
 
 
 def _large_mesh():
@@ -46,7 +47,8 @@ def _large_mesh():
     return scene, cam, [0, 1, 2, 3]
 
 
-SCENES = {"cornell": (_cornell, 64, 64), "sphere_field": (_sphere_field, 96, 54), "large_mesh": (_large_mesh, 96, 54)}
+SCENES = {"cornell": (_cornell, 64, 64), "sphere_field": (_sphere_field, 96, 54), "large_mesh": (_large_mesh, 96, 54),
+          "sphere_field_8": (lambda: _sphere_field(6), 96, 54)}  # the most parameters a call takes
 
 
 def _adjoint(torch, w, h, seed):
@@ -68,11 +70,14 @@ def _render(scene, cam, cfg, tile, start, count):
     ("cornell", dict(mode=abi.MODE_GRAPH, max_depth=8, rr_start_depth=3), (0, 0, 64, 64), 100, 4),
     ("cornell", dict(mode=abi.MODE_GRAPH, max_depth=8, rr_start_depth=3, samples_per_wave=4), (5, 9, 40, 33), 7, 8),
     ("cornell", dict(mode=abi.MODE_PERSISTENT, max_depth=8, rr_start_depth=3), (0, 0, 64, 64), 0, 3),
+    ("cornell", dict(mode=abi.MODE_STREAM, max_depth=8, rr_start_depth=3), (0, 0, 64, 64), 5, 6),
     ("sphere_field", dict(mode=abi.MODE_GRAPH, max_depth=16), (0, 0, 96, 54), 100, 3),
     ("sphere_field", dict(mode=abi.MODE_GRAPH, max_depth=16, samples_per_wave=2), (17, 3, 64, 40), 11, 4),
+    ("sphere_field", dict(mode=abi.MODE_GRAPH, max_depth=16, samples_per_wave=2, concurrent_tiles=2), (0, 0, 96, 54),
+     3, 4),
     ("large_mesh", dict(mode=abi.MODE_GRAPH, max_depth=12), (0, 0, 96, 54), 100, 2),
-], ids=["cornell-graph", "cornell-wave-tile", "cornell-persistent", "sphere-graph", "sphere-wave-tile",
-        "large-mesh-graph"])
+], ids=["cornell-graph", "cornell-wave-tile", "cornell-persistent", "cornell-stream", "sphere-graph",
+        "sphere-wave-tile", "sphere-two-wavefronts", "large-mesh-graph"])
 def test_replay_image_bit_exact(cuda, case):
     torch = cuda
     name, fields, tile, start, count = case
@@ -114,7 +119,8 @@ def _finite_differences(scene, cam, cfg, params, adjoint, spp, eps):
     return out
 
 
-@pytest.mark.parametrize("name,depth,spp", [("cornell", 8, 8), ("sphere_field", 12, 4), ("large_mesh", 12, 2)])
+@pytest.mark.parametrize("name,depth,spp", [("cornell", 8, 8), ("sphere_field", 12, 4), ("large_mesh", 12, 2),
+                                            ("sphere_field_8", 12, 4)])
 def test_gradient_matches_central_differences(cuda, name, depth, spp):
     torch = cuda
     make, w, h = SCENES[name]

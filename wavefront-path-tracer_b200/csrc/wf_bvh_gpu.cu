@@ -16,11 +16,14 @@
 //      lower position keeps it), and an exclusive scan compacts the
 //      survivors and numbers the new nodes;
 //   4. rounds repeat until one cluster is left (at most kMaxRounds; the
-//      caller falls back to the host builder beyond that).
+//      caller falls back to the host builder beyond that);
+//   5. treelet restructuring (k_restructure) lowers the tree's SAH cost,
+//      and the leaf depth is measured on the device before the download.
 // Every step is deterministic (stable sort, index tie-breaks, scan-ordered
-// node numbering), so a scene always gets the same tree.  The output is the
-// host builder's format (bvh_build.h): 2n-1 nodes, leaves first with
-// left == kInvalidChild and right == primitive, the root last.
+// node numbering, subtree-local treelet choices), so a scene always gets the
+// same tree.  The output is the host builder's format (bvh_build.h): 2n-1
+// nodes, leaves first with left == kInvalidChild and right == primitive, the
+// root last (after restructuring, a child may follow its parent).
 #include "bvh_build.h"
 #include "wf_bvh_gpu.h"
 #include "wf_internal.h"
@@ -252,14 +255,13 @@ cudaError_t exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, cudaSt
 
 // ------------------------------------------------------------------ PLOC
 __global__ void k_leaves(const BvhBox* prims, const uint32_t* order, uint32_t n, BvhBinaryNode* nodes,
-                         uint32_t* clusters, BvhBox* boxes, uint32_t* heights) {
+                         uint32_t* clusters, BvhBox* boxes) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     nodes[i] = BvhBinaryNode{prims[i], kInvalidChild, i};
     uint32_t p = order[i];
     clusters[i] = p;
     boxes[i] = prims[p];
-    heights[i] = 0;
 }
 
 // Nearest neighbour of every cluster within +-kPlocRadius: the candidate
@@ -309,11 +311,11 @@ __global__ void k_merge_flags(const uint32_t* nearest, uint32_t m, uint32_t* ali
 }
 
 // Survivors move to their compacted position; each mutual pair becomes a new
-// node whose height (longest path to a leaf) is one more than its taller child.
-__global__ void k_merge(const uint32_t* clusters, const BvhBox* boxes, const uint32_t* heights,
-                        const uint32_t* nearest, uint32_t m, const uint32_t* alive, const uint32_t* alive_at,
-                        const uint32_t* leader, const uint32_t* leader_at, uint32_t node_base, BvhBinaryNode* nodes,
-                        uint32_t* clusters_out, BvhBox* boxes_out, uint32_t* heights_out) {
+// node.
+__global__ void k_merge(const uint32_t* clusters, const BvhBox* boxes, const uint32_t* nearest, uint32_t m,
+                        const uint32_t* alive, const uint32_t* alive_at, const uint32_t* leader,
+                        const uint32_t* leader_at, uint32_t node_base, BvhBinaryNode* nodes, uint32_t* clusters_out,
+                        BvhBox* boxes_out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m || !alive[i]) return;
     uint32_t dst = alive_at[i];
@@ -324,12 +326,231 @@ __global__ void k_merge(const uint32_t* clusters, const BvhBox* boxes, const uin
         nodes[node] = BvhBinaryNode{box, clusters[i], clusters[j]};
         clusters_out[dst] = node;
         boxes_out[dst] = box;
-        heights_out[dst] = 1u + max(heights[i], heights[j]);
     } else {
         clusters_out[dst] = clusters[i];
         boxes_out[dst] = boxes[i];
-        heights_out[dst] = heights[i];
     }
+}
+
+// ------------------------------------------------- treelet restructuring
+// Karras and Aila, "Fast Parallel Construction of High-Quality Bounding
+// Volume Hierarchies" (HPG 2013): after PLOC, one thread per leaf walks up
+// the tree; the second thread to reach a node owns it (both subtrees are
+// final by then).  A node with at least `min_leaves` leaves below it roots
+// a treelet: starting from its two children, the treelet leaf with the
+// largest surface area is expanded until there are kTreeletLeaves of them.
+// A dynamic programme over the 2^7 subsets of those leaves finds the
+// topology with the smallest summed surface area of its internal nodes
+// (the SAH with unit costs; the leaves' subtrees are fixed), and the
+// treelet's internal node slots are rewired to it if it beats the current
+// one.  A treelet only touches nodes below its root, which no other thread
+// reads or writes any more, and every choice is a pure function of that
+// subtree (ties keep the first split found), so the result does not depend
+// on thread timing.  Loads bypass L1 (__ldcg): another SM wrote the data.
+constexpr int kTreeletLeaves = 7;
+constexpr int kTreeletSubsets = 1 << kTreeletLeaves;
+constexpr int kRestructureRounds = 3;  // treelet roots with >= 7, 14, 28 leaves
+constexpr int kRestructureThreads = 128;
+
+__device__ __forceinline__ BvhBinaryNode load_node(const BvhBinaryNode* nodes, uint32_t i) {
+    const float4* p = reinterpret_cast<const float4*>(nodes + i);
+    float4 a = __ldcg(p), b = __ldcg(p + 1);
+    BvhBinaryNode n;
+    n.box.lo[0] = a.x;
+    n.box.lo[1] = a.y;
+    n.box.lo[2] = a.z;
+    n.box.hi[0] = a.w;
+    n.box.hi[1] = b.x;
+    n.box.hi[2] = b.y;
+    n.left = __float_as_uint(b.z);
+    n.right = __float_as_uint(b.w);
+    return n;
+}
+
+__device__ __forceinline__ void store_node(BvhBinaryNode* nodes, uint32_t i, const BvhBox& box, uint32_t left,
+                                           uint32_t right) {
+    float4* p = reinterpret_cast<float4*>(nodes + i);
+    __stcg(p, make_float4(box.lo[0], box.lo[1], box.lo[2], box.hi[0]));
+    __stcg(p + 1, make_float4(box.hi[1], box.hi[2], __uint_as_float(left), __uint_as_float(right)));
+}
+
+// parent[] of every node (the root's stays kInvalidChild, set by the caller).
+__global__ void k_parents(const BvhBinaryNode* nodes, uint32_t n, uint32_t* parent) {
+    uint32_t i = n + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * n - 1) return;
+    parent[nodes[i].left] = i;
+    parent[nodes[i].right] = i;
+}
+
+// Leaves: subtree cost = own half area, one leaf.
+__global__ void k_leaf_costs(const BvhBinaryNode* nodes, uint32_t n, float* cost, uint32_t* leafcount) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    cost[i] = half_area(nodes[i].box);
+    leafcount[i] = 1;
+}
+
+// Restructures the treelet rooted at internal node `root`; returns the
+// subtree's cost (summed half areas of its nodes).
+__device__ float optimize_treelet(BvhBinaryNode* nodes, uint32_t* parent, float* cost, uint32_t* leafcount,
+                                  uint32_t root, const BvhBinaryNode& top) {
+    uint32_t leaf[kTreeletLeaves], inner[kTreeletLeaves - 1], count[kTreeletLeaves];
+    BvhBox box[kTreeletLeaves];
+    float sub[kTreeletLeaves];
+    bool expandable[kTreeletLeaves];
+    int nl = 0, ni = 1;
+    inner[0] = root;
+    float old_cost = half_area(top.box);
+    auto add = [&](int slot, uint32_t node) {
+        BvhBinaryNode x = load_node(nodes, node);
+        leaf[slot] = node;
+        box[slot] = x.box;
+        expandable[slot] = x.left != kInvalidChild;
+        sub[slot] = __ldcg(cost + node);
+        count[slot] = __ldcg(leafcount + node);
+    };
+    add(nl++, top.left);
+    add(nl++, top.right);
+    while (nl < kTreeletLeaves) {
+        int pick = -1;
+        float largest = -1.0f;
+        for (int j = 0; j < nl; ++j) {
+            float a = half_area(box[j]);
+            if (expandable[j] && a > largest) {
+                largest = a;
+                pick = j;
+            }
+        }
+        if (pick < 0) break;
+        BvhBinaryNode x = load_node(nodes, leaf[pick]);
+        inner[ni++] = leaf[pick];
+        old_cost += half_area(x.box);
+        add(pick, x.left);
+        add(nl++, x.right);
+    }
+    for (int j = 0; j < nl; ++j) old_cost += sub[j];
+    if (nl < 3) return old_cost;  // one topology only
+    float area[kTreeletSubsets], best[kTreeletSubsets];
+    uint8_t split[kTreeletSubsets];
+    const int full = (1 << nl) - 1;
+    for (int s = 1; s <= full; ++s) {
+        int low = __ffs(s) - 1;
+        BvhBox u = box[low];
+        for (int j = low + 1; j < nl; ++j)
+            if (s & (1 << j)) u = merged(u, box[j]);
+        area[s] = half_area(u);
+        if ((s & (s - 1)) == 0) {
+            best[s] = sub[low];
+            split[s] = 0;
+            continue;
+        }
+        float b = INFINITY;
+        int bq = 0;
+        for (int q = (s - 1) & s; q > 0; q = (q - 1) & s) {
+            if (!(q & (1 << low))) continue;  // each split once: the side holding the lowest leaf
+            float c = best[q] + best[s ^ q];
+            if (c < b) {
+                b = c;
+                bq = q;
+            }
+        }
+        best[s] = area[s] + b;
+        split[s] = uint8_t(bq);
+    }
+    // Keep the current treelet unless the new one is clearly cheaper (the two
+    // sums round differently).
+    if (!(best[full] < old_cost * (1.0f - 1e-5f))) return old_cost;
+    // A finite best cost implies a proper split at every set of the chosen
+    // topology; check that before writing anything (non-finite boxes).
+    int set_stack[kTreeletLeaves];
+    {
+        int n_sets = 0, pending = 0;
+        set_stack[pending++] = full;
+        while (pending > 0) {
+            int s = set_stack[--pending];
+            int q = split[s];
+            if (q == 0 || (q & ~s) != 0 || q == s || ++n_sets > kTreeletLeaves - 1) return old_cost;
+            int sides[2] = {q, s ^ q};
+            for (int k = 0; k < 2; ++k)
+                if ((sides[k] & (sides[k] - 1)) != 0) set_stack[pending++] = sides[k];
+        }
+    }
+    uint32_t node_stack[kTreeletLeaves];
+    int top_at = 0, next_inner = 1;
+    set_stack[top_at] = full;
+    node_stack[top_at++] = root;
+    while (top_at > 0) {
+        --top_at;
+        int s = set_stack[top_at];
+        uint32_t slot = node_stack[top_at];
+        int sides[2] = {split[s], s ^ split[s]};
+        uint32_t child[2];
+        for (int k = 0; k < 2; ++k) {
+            int t = sides[k];
+            if ((t & (t - 1)) == 0) {
+                child[k] = leaf[__ffs(t) - 1];
+            } else {
+                child[k] = inner[next_inner++];
+                set_stack[top_at] = t;
+                node_stack[top_at++] = child[k];
+            }
+        }
+        int low = __ffs(s) - 1;
+        BvhBox u = box[low];
+        uint32_t leaves = 0;
+        for (int j = low; j < nl; ++j) {
+            if (!(s & (1 << j))) continue;
+            u = merged(u, box[j]);
+            leaves += count[j];
+        }
+        store_node(nodes, slot, u, child[0], child[1]);
+        __stcg(parent + child[0], slot);
+        __stcg(parent + child[1], slot);
+        __stcg(cost + slot, best[s]);
+        __stcg(leafcount + slot, leaves);
+    }
+    return best[full];
+}
+
+// One bottom-up round: thread i starts at leaf i.
+__global__ void __launch_bounds__(kRestructureThreads) k_restructure(BvhBinaryNode* nodes, uint32_t* parent,
+                                                                     uint32_t* visits, float* cost,
+                                                                     uint32_t* leafcount, uint32_t n,
+                                                                     uint32_t min_leaves) {
+    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    for (uint32_t step = 0; step < 2 * n; ++step) {  // a path to the root is shorter than the node count
+        uint32_t p = __ldcg(parent + v);
+        if (p == kInvalidChild) return;
+        __threadfence();  // this subtree's writes before the arrival
+        if (atomicAdd(visits + p, 1u) == 0u) return;  // the other subtree is still being built
+        __threadfence();
+        BvhBinaryNode node = load_node(nodes, p);
+        uint32_t leaves = __ldcg(leafcount + node.left) + __ldcg(leafcount + node.right);
+        float c = leaves >= min_leaves ? optimize_treelet(nodes, parent, cost, leafcount, p, node)
+                                       : half_area(node.box) + __ldcg(cost + node.left) + __ldcg(cost + node.right);
+        __stcg(cost + p, c);
+        __stcg(leafcount + p, leaves);
+        v = p;
+    }
+}
+
+// Longest leaf-to-root path; depth[1] is set if a walk does not reach the
+// root within the node count (a broken parent chain).
+__global__ void k_tree_depth(const uint32_t* parent, uint32_t n, uint32_t* depth) {
+    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    uint32_t d = 0;
+    while (true) {
+        uint32_t p = parent[v];
+        if (p == kInvalidChild) break;
+        if (++d >= 2 * n) {
+            atomicOr(depth + 1, 1u);
+            return;
+        }
+        v = p;
+    }
+    atomicMax(depth, d);
 }
 
 // Device -> host.  Large copies go through two pinned staging buffers, so
@@ -400,7 +621,6 @@ bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t n, std::vector<BvhBinary
     uint32_t* bounds = scratch.alloc<uint32_t>(6);
     uint32_t* clusters[2] = {scratch.alloc<uint32_t>(n), scratch.alloc<uint32_t>(n)};
     BvhBox* boxes[2] = {scratch.alloc<BvhBox>(n), scratch.alloc<BvhBox>(n)};
-    uint32_t* heights[2] = {scratch.alloc<uint32_t>(n), scratch.alloc<uint32_t>(n)};
     uint32_t* nearest = scratch.alloc<uint32_t>(n);
     uint32_t* alive = scratch.alloc<uint32_t>(n);
     uint32_t* alive_at = scratch.alloc<uint32_t>(n);
@@ -424,8 +644,7 @@ bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t n, std::vector<BvhBinary
         if ((e = cudaGetLastError())) return failed("sort scatter", e);
         cur ^= 1;
     }
-    k_leaves<<<blocks_for(n, 256), 256, 0, st>>>(d_prims, values[cur], n, d_nodes, clusters[0], boxes[0],
-                                                 heights[0]);
+    k_leaves<<<blocks_for(n, 256), 256, 0, st>>>(d_prims, values[cur], n, d_nodes, clusters[0], boxes[0]);
     if ((e = cudaGetLastError())) return failed("PLOC leaves", e);
 
     uint32_t m = n, node_base = n;
@@ -440,9 +659,8 @@ bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t n, std::vector<BvhBinary
         if ((e = cudaGetLastError())) return failed("PLOC neighbours", e);
         if ((e = exclusive_scan(alive, alive_at, m, st, scratch))) return failed("PLOC scan", e);
         if ((e = exclusive_scan(leader, leader_at, m, st, scratch))) return failed("PLOC scan", e);
-        k_merge<<<blocks_for(m, 256), 256, 0, st>>>(clusters[c], boxes[c], heights[c], nearest, m, alive, alive_at,
-                                                    leader, leader_at, node_base, d_nodes, clusters[c ^ 1],
-                                                    boxes[c ^ 1], heights[c ^ 1]);
+        k_merge<<<blocks_for(m, 256), 256, 0, st>>>(clusters[c], boxes[c], nearest, m, alive, alive_at, leader,
+                                                    leader_at, node_base, d_nodes, clusters[c ^ 1], boxes[c ^ 1]);
         if ((e = cudaGetLastError())) return failed("PLOC merge", e);
         uint32_t tail[4];
         e = cudaMemcpyAsync(&tail[0], alive_at + m - 1, 4, cudaMemcpyDeviceToHost, st);
@@ -461,11 +679,40 @@ bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t n, std::vector<BvhBinary
         c ^= 1;
     }
     uint32_t depth = 0;
-    e = cudaMemcpyAsync(&depth, heights[c], 4, cudaMemcpyDeviceToHost, st);
-    if (!e) e = cudaStreamSynchronize(st);
-    if (e) return failed("BVH depth", e);
+    if (n >= 2) {
+        // Treelet restructuring; it may change the depth, which is measured
+        // afterwards.
+        uint32_t* parent = scratch.alloc<uint32_t>(node_count);
+        uint32_t* visits = scratch.alloc<uint32_t>(node_count);
+        uint32_t* leafcount = scratch.alloc<uint32_t>(node_count);
+        float* cost = scratch.alloc<float>(node_count);
+        uint32_t* d_depth = scratch.alloc<uint32_t>(2);
+        if (scratch.error != cudaSuccess) return failed("device memory for the BVH restructuring", scratch.error);
+        e = cudaMemsetAsync(parent + node_count - 1, 0xff, sizeof(uint32_t), st);
+        if (!e) e = cudaMemsetAsync(d_depth, 0, 2 * sizeof(uint32_t), st);
+        if (e) return failed("BVH restructuring setup", e);
+        k_parents<<<blocks_for(n - 1, 256), 256, 0, st>>>(d_nodes, n, parent);
+        k_leaf_costs<<<blocks_for(n, 256), 256, 0, st>>>(d_nodes, n, cost, leafcount);
+        if ((e = cudaGetLastError())) return failed("BVH parents", e);
+        for (int round = 0; round < kRestructureRounds; ++round) {
+            if ((e = cudaMemsetAsync(visits, 0, sizeof(uint32_t) * node_count, st))) return failed("BVH visits", e);
+            k_restructure<<<blocks_for(n, kRestructureThreads), kRestructureThreads, 0, st>>>(
+                d_nodes, parent, visits, cost, leafcount, n, uint32_t(kTreeletLeaves) << round);
+            if ((e = cudaGetLastError())) return failed("BVH treelet restructuring", e);
+        }
+        k_tree_depth<<<blocks_for(n, 256), 256, 0, st>>>(parent, n, d_depth);
+        uint32_t result[2] = {0, 0};
+        e = cudaMemcpyAsync(result, d_depth, sizeof(result), cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaStreamSynchronize(st);
+        if (e) return failed("BVH depth", e);
+        if (result[1]) {
+            if (why && why_size) std::snprintf(why, why_size, "restructured BVH has a broken parent chain");
+            return false;
+        }
+        depth = result[0];
+    }
     if (int(depth) > max_depth) {
-        if (why && why_size) std::snprintf(why, why_size, "PLOC tree depth %u exceeds %d", depth, max_depth);
+        if (why && why_size) std::snprintf(why, why_size, "GPU BVH depth %u exceeds %d", depth, max_depth);
         return false;
     }
     // Leaves are known on the host (box i, primitive i); only the n-1

@@ -10,7 +10,9 @@
 namespace wf {
 
 // Builds the tree over `count` primitive boxes (host memory) on the current
-// device, in the host builder's output format (bvh_build.h).  Synchronous.
+// device, in the host builder's output format (bvh_build.h), except that after
+// the treelet restructuring a child may come after its parent (readers walk
+// from the root, the last node).  Synchronous.
 // Returns false with a message in `why` on a CUDA error, a stalled build or a
 // leaf deeper than `max_depth` (checked on the device before the download).
 bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t count, std::vector<BvhBinaryNode>& nodes, int max_depth,

@@ -553,6 +553,45 @@ __global__ void k_tree_depth(const uint32_t* parent, uint32_t n, uint32_t* depth
     atomicMax(depth, d);
 }
 
+// ------------------------------------------------ top-level rebuild
+// The restructured tree is cut into clusters, the largest subtrees with at
+// most kTopClusterLeaves leaves; the host's binned-SAH builder rebuilds the
+// tree above them, whose n_c - 1 internal nodes take the slots of the n_c - 1
+// nodes above the cut.  Treelets cannot see past 7 leaves, and a full SAH
+// sweep over ~n/10 clusters costs a fraction of one over n primitives.
+constexpr uint32_t kTopClusterLeaves = 16;
+
+__global__ void k_cut_flags(const uint32_t* parent, const uint32_t* leafcount, uint32_t node_count, uint32_t limit,
+                            uint32_t* is_cut, uint32_t* is_top) {
+    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= node_count) return;
+    uint32_t leaves = leafcount[v], p = parent[v];
+    is_top[v] = leaves > limit ? 1u : 0u;
+    is_cut[v] = leaves <= limit && (p == kInvalidChild || leafcount[p] > limit) ? 1u : 0u;
+}
+
+__global__ void k_compact(const uint32_t* flag, const uint32_t* at, uint32_t count, uint32_t* out) {
+    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < count && flag[v]) out[at[v]] = v;
+}
+
+// Height of every cluster (longest path from it down to a leaf); error[0] is
+// set if a leaf has no cluster above it.
+__global__ void k_cut_heights(const uint32_t* parent, const uint32_t* is_cut, const uint32_t* cut_at, uint32_t n,
+                              uint32_t* height, uint32_t* error) {
+    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    uint32_t d = 0;
+    while (!is_cut[v]) {
+        v = parent[v];
+        if (v == kInvalidChild || ++d >= 2 * n) {
+            atomicOr(error, 1u);
+            return;
+        }
+    }
+    atomicMax(height + cut_at[v], d);
+}
+
 // Device -> host.  Large copies go through two pinned staging buffers, so
 // the copy of one chunk overlaps the host copy of the previous one (fresh
 // pageable memory would otherwise take the transfer through page faults);
@@ -592,6 +631,48 @@ cudaError_t download(void* dst, const void* src, size_t bytes, cudaStream_t st) 
 }
 
 uint32_t blocks_for(uint32_t n, uint32_t threads) { return (n + threads - 1) / threads; }
+
+// Replaces the nodes above the clusters with the host builder's tree over
+// the clusters' boxes: its root takes the root's slot (the last node), its
+// other internal nodes the remaining slots in order.  Skipped, keeping the
+// tree as it is, if the result would be deeper than `max_depth`.
+void rebuild_top(std::vector<BvhBinaryNode>& nodes, const std::vector<uint32_t>& clusters,
+                 const std::vector<uint32_t>& cluster_height, const std::vector<uint32_t>& top_slots,
+                 int max_depth) {
+    const uint32_t root_slot = uint32_t(nodes.size() - 1);
+    std::vector<BvhBox> boxes(clusters.size());
+    for (size_t k = 0; k < clusters.size(); ++k) boxes[k] = nodes[clusters[k]].box;
+    std::vector<BvhBinaryNode> top;
+    build_binary_bvh(boxes.data(), uint32_t(boxes.size()), top, 0);
+    if (top.size() != 2 * clusters.size() - 1) return;
+    // depth of every cluster in the new top tree plus its own height
+    std::vector<std::pair<uint32_t, uint32_t>> stack{{uint32_t(top.size() - 1), 0u}};
+    uint32_t deepest = 0;
+    while (!stack.empty()) {
+        auto [k, d] = stack.back();
+        stack.pop_back();
+        if (top[k].left == kInvalidChild) {
+            deepest = std::max(deepest, d + cluster_height[top[k].right]);
+            continue;
+        }
+        stack.push_back({top[k].left, d + 1});
+        stack.push_back({top[k].right, d + 1});
+    }
+    if (int(deepest) > max_depth) return;
+    std::vector<uint32_t> slot(top.size(), kInvalidChild);
+    size_t next = 0;
+    for (size_t k = 0; k + 1 < top.size(); ++k) {
+        if (top[k].left == kInvalidChild) continue;
+        while (next < top_slots.size() && top_slots[next] == root_slot) ++next;
+        if (next == top_slots.size()) return;
+        slot[k] = top_slots[next++];
+    }
+    slot[top.size() - 1] = root_slot;
+    auto ref = [&](uint32_t k) { return top[k].left == kInvalidChild ? clusters[top[k].right] : slot[k]; };
+    for (size_t k = 0; k < top.size(); ++k)
+        if (top[k].left != kInvalidChild)
+            nodes[slot[k]] = BvhBinaryNode{top[k].box, ref(top[k].left), ref(top[k].right)};
+}
 
 }  // namespace
 
@@ -679,6 +760,7 @@ bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t n, std::vector<BvhBinary
         c ^= 1;
     }
     uint32_t depth = 0;
+    std::vector<uint32_t> top_clusters, cluster_height, top_slots;  // top-level rebuild (empty: none)
     if (n >= 2) {
         // Treelet restructuring; it may change the depth, which is measured
         // afterwards.
@@ -710,6 +792,51 @@ bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t n, std::vector<BvhBinary
             return false;
         }
         depth = result[0];
+        // Clusters of the top-level rebuild, their heights and the slots
+        // above them.
+        uint32_t* is_cut = scratch.alloc<uint32_t>(node_count);
+        uint32_t* is_top = scratch.alloc<uint32_t>(node_count);
+        uint32_t* cut_at = scratch.alloc<uint32_t>(node_count);
+        uint32_t* top_at = scratch.alloc<uint32_t>(node_count);
+        if (scratch.error != cudaSuccess) return failed("device memory for the BVH top rebuild", scratch.error);
+        k_cut_flags<<<blocks_for(node_count, 256), 256, 0, st>>>(parent, leafcount, node_count, kTopClusterLeaves,
+                                                                 is_cut, is_top);
+        if ((e = cudaGetLastError())) return failed("BVH clusters", e);
+        if ((e = exclusive_scan(is_cut, cut_at, node_count, st, scratch))) return failed("BVH cluster scan", e);
+        if ((e = exclusive_scan(is_top, top_at, node_count, st, scratch))) return failed("BVH cluster scan", e);
+        uint32_t tail[4];
+        e = cudaMemcpyAsync(&tail[0], cut_at + node_count - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaMemcpyAsync(&tail[1], is_cut + node_count - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaMemcpyAsync(&tail[2], top_at + node_count - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaMemcpyAsync(&tail[3], is_top + node_count - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaStreamSynchronize(st);
+        if (e) return failed("BVH cluster counts", e);
+        uint32_t clusters_n = tail[0] + tail[1], top_n = tail[2] + tail[3];
+        if (clusters_n >= 3 && top_n == clusters_n - 1) {
+            uint32_t* cut_list = scratch.alloc<uint32_t>(clusters_n);
+            uint32_t* top_list = scratch.alloc<uint32_t>(top_n);
+            uint32_t* cut_height = scratch.alloc<uint32_t>(clusters_n);
+            if (scratch.error != cudaSuccess) return failed("device memory for the BVH top rebuild", scratch.error);
+            if ((e = cudaMemsetAsync(cut_height, 0, sizeof(uint32_t) * clusters_n, st)) ||
+                (e = cudaMemsetAsync(d_depth + 1, 0, sizeof(uint32_t), st)))
+                return failed("BVH cluster heights", e);
+            k_compact<<<blocks_for(node_count, 256), 256, 0, st>>>(is_cut, cut_at, node_count, cut_list);
+            k_compact<<<blocks_for(node_count, 256), 256, 0, st>>>(is_top, top_at, node_count, top_list);
+            k_cut_heights<<<blocks_for(n, 256), 256, 0, st>>>(parent, is_cut, cut_at, n, cut_height, d_depth + 1);
+            if ((e = cudaGetLastError())) return failed("BVH cluster heights", e);
+            top_clusters.resize(clusters_n);
+            cluster_height.resize(clusters_n);
+            top_slots.resize(top_n);
+            uint32_t broken = 0;
+            e = cudaMemcpyAsync(top_clusters.data(), cut_list, 4 * size_t(clusters_n), cudaMemcpyDeviceToHost, st);
+            if (!e) e = cudaMemcpyAsync(cluster_height.data(), cut_height, 4 * size_t(clusters_n),
+                                        cudaMemcpyDeviceToHost, st);
+            if (!e) e = cudaMemcpyAsync(top_slots.data(), top_list, 4 * size_t(top_n), cudaMemcpyDeviceToHost, st);
+            if (!e) e = cudaMemcpyAsync(&broken, d_depth + 1, 4, cudaMemcpyDeviceToHost, st);
+            if (!e) e = cudaStreamSynchronize(st);
+            if (e) return failed("BVH clusters download", e);
+            if (broken) top_clusters.clear();  // keep the restructured tree
+        }
     }
     if (int(depth) > max_depth) {
         if (why && why_size) std::snprintf(why, why_size, "GPU BVH depth %u exceeds %d", depth, max_depth);
@@ -724,6 +851,7 @@ bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t n, std::vector<BvhBinary
         out.clear();
         return failed("BVH download", e);
     }
+    if (!top_clusters.empty()) rebuild_top(out, top_clusters, cluster_height, top_slots, max_depth);
     return true;
 }
 

@@ -18,7 +18,9 @@
 //   4. rounds repeat until one cluster is left (at most kMaxRounds; the
 //      caller falls back to the host builder beyond that);
 //   5. treelet restructuring (k_restructure) lowers the tree's SAH cost,
-//      and the leaf depth is measured on the device before the download.
+//      and the leaf depth is measured on the device before the download;
+//   6. the host's binned-SAH builder rebuilds the levels above the largest
+//      subtrees of at most kTopClusterLeaves leaves (rebuild_top).
 // Every step is deterministic (stable sort, index tie-breaks, scan-ordered
 // node numbering, subtree-local treelet choices), so a scene always gets the
 // same tree.  The output is the host builder's format (bvh_build.h): 2n-1

@@ -217,10 +217,11 @@ typedef struct wf_scene_desc {
     uint32_t build_threads; /* 0 = all host threads */
     /* WF_BVH_HOST_SAH (0, default): binned-SAH BVH2s built on the host.
      * WF_BVH_GPU_PLOC: BVH2s over >= 4096 primitives built on the GPU by
-     * PLOC (the role of the reference's NexusBVH builder, scene.cu:148-149,
-     * 227-228, 262-264); smaller ones, and any build that fails or exceeds
-     * the 60-level depth bound, use the host builder.  No counterpart field
-     * in the reference. */
+     * PLOC and treelet restructuring, with the levels above 16-leaf
+     * subtrees rebuilt by the host builder (the role of the reference's
+     * NexusBVH builder, scene.cu:148-149, 227-228, 262-264); smaller ones,
+     * and any build that fails or exceeds the 60-level depth bound, use the
+     * host builder.  No counterpart field in the reference. */
     uint32_t bvh_builder;
     uint32_t reserved;
     /* Textured materials (all optional): RGBA8 textures, one

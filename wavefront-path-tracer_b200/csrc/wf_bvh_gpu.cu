@@ -640,12 +640,12 @@ uint32_t blocks_for(uint32_t n, uint32_t threads) { return (n + threads - 1) / t
 // tree as it is, if the result would be deeper than `max_depth`.
 void rebuild_top(std::vector<BvhBinaryNode>& nodes, const std::vector<uint32_t>& clusters,
                  const std::vector<uint32_t>& cluster_height, const std::vector<uint32_t>& top_slots,
-                 int max_depth) {
+                 int max_depth, int threads) {
     const uint32_t root_slot = uint32_t(nodes.size() - 1);
     std::vector<BvhBox> boxes(clusters.size());
     for (size_t k = 0; k < clusters.size(); ++k) boxes[k] = nodes[clusters[k]].box;
     std::vector<BvhBinaryNode> top;
-    build_binary_bvh(boxes.data(), uint32_t(boxes.size()), top, 0);
+    build_binary_bvh(boxes.data(), uint32_t(boxes.size()), top, threads);
     if (top.size() != 2 * clusters.size() - 1) return;
     // depth of every cluster in the new top tree plus its own height
     std::vector<std::pair<uint32_t, uint32_t>> stack{{uint32_t(top.size() - 1), 0u}};
@@ -679,7 +679,7 @@ void rebuild_top(std::vector<BvhBinaryNode>& nodes, const std::vector<uint32_t>&
 }  // namespace
 
 bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t n, std::vector<BvhBinaryNode>& out, int max_depth,
-                          char* why, size_t why_size) {
+                          char* why, size_t why_size, int threads) {
     auto failed = [&](const char* what, cudaError_t e) {
         if (why && why_size) std::snprintf(why, why_size, "%s: %s", what, cudaGetErrorString(e));
         return false;
@@ -853,7 +853,7 @@ bool build_binary_bvh_gpu(const BvhBox* prims, uint32_t n, std::vector<BvhBinary
         out.clear();
         return failed("BVH download", e);
     }
-    if (!top_clusters.empty()) rebuild_top(out, top_clusters, cluster_height, top_slots, max_depth);
+    if (!top_clusters.empty()) rebuild_top(out, top_clusters, cluster_height, top_slots, max_depth, threads);
     return true;
 }
 

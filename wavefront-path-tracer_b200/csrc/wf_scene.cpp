@@ -385,7 +385,7 @@ wf_status build_host_scene(const wf_scene_desc* d, HostScene& s) {
         bool done = false;
         if (d->bvh_builder == WF_BVH_GPU_PLOC && n >= kGpuBvhMinPrimitives) {
             char why[256] = {0};
-            done = build_binary_bvh_gpu(prims, n, out, kMaxBvhDepth, why, sizeof(why));
+            done = build_binary_bvh_gpu(prims, n, out, kMaxBvhDepth, why, sizeof(why), threads);
             if (done) ++s.gpu_bvh_builds;
         }
         if (!done) build_binary_bvh(prims, n, out, threads);

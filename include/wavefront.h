@@ -252,6 +252,13 @@ wf_status wf_scene_create(const wf_scene_desc* desc, wf_scene** out);
  * (src/scene/environment.cpp:10-64).  env == NULL clears the map
  * (clearEnvironmentMap, scene.cu:298-306). */
 wf_status wf_scene_set_environment(wf_scene* scene, const wf_environment* env);
+/* Sets the RGB albedo of `count` materials (host arrays: material indices,
+ * and 3 floats each) in the device scene, in place.  Waits until the device
+ * is idle first; every renderer made from the scene renders with the new
+ * albedos from its next call on.  Photon maps that renderers built at
+ * creation are not retraced.  For inverse rendering with
+ * wf_render_albedo_gradient; no counterpart in the reference. */
+wf_status wf_scene_set_albedos(wf_scene* scene, const uint32_t* materials, const float* rgb, uint32_t count);
 /* Replaces destroyDeviceScene, src/scene/scene.cu:391-420. */
 wf_status wf_scene_destroy(wf_scene* scene);
 

@@ -17,6 +17,8 @@
   within 2 % of the gradient's norm.
 * Inverse rendering with it: Adam recovers the Cornell walls' albedos from
   a target image rendered with the same samples.
+* wf_scene_set_albedos: renderers see the new albedos, bit for bit those of
+  a scene built with them.
 * The argument checks of the entry point.
 """
 import numpy as np
@@ -188,6 +190,34 @@ def test_inverse_rendering_recovers_wall_albedos(cuda):
     err = np.abs(x.detach().numpy() - truth).max()
     assert losses[-1] < 1e-4 * losses[0], losses[::10]
     assert err < 0.01, (x.detach().numpy(), truth)
+
+
+def test_set_albedos_matches_a_fresh_scene(cuda):
+    """wf_scene_set_albedos: a renderer made before the update renders, and
+    replays, exactly what a scene built with the new albedos renders."""
+    torch = cuda
+    scene, cam, _ = _cornell()
+    cfg = wfpt.render_config(64, 64, mode=abi.MODE_GRAPH, max_depth=8, rr_start_depth=3, indirect_clamp=0.0)
+    new = np.array([[0.3, 0.6, 0.2], [0.9, 0.1, 0.4]], np.float32)
+    dev = wfpt.DeviceScene(scene)
+    r = wfpt.Renderer(dev, cam, cfg)
+    try:
+        before = r.render_task((0, 0, 64, 64), 0, 4)
+        dev.set_albedos([0, 2], new)
+        got = r.render_task((0, 0, 64, 64), 0, 4)
+        _, replay = diff.albedo_gradient(r, [0, 2], _adjoint(torch, 64, 64, 5), None, 0, 4, image=True)
+        for bad in (([99], new[:1]), ([0], np.array([[np.nan, 0.5, 0.5]], np.float32))):
+            with pytest.raises(wfpt.WavefrontError) as e:
+                dev.set_albedos(*bad)
+            assert e.value.status == abi.WF_ERR_INVALID_ARG
+    finally:
+        r.close()
+        dev.close()
+    scene.materials["albedo"][[0, 2]] = new
+    want = _render(scene, cam, cfg, (0, 0, 64, 64), 0, 4)
+    assert not np.array_equal(before, want)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert np.array_equal(replay.cpu().numpy().view(np.uint32), want.view(np.uint32))
 
 
 def test_argument_checks(cuda):

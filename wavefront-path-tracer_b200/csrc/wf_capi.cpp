@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cstddef>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -217,6 +218,29 @@ wf_status wf_scene_create(const wf_scene_desc* desc, wf_scene** out) {
     s->bvh_build_ms = h.bvh_build_ms;
     s->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = s.release();
+    return WF_OK;
+}
+
+// No counterpart in the reference, whose materials are fixed at upload.
+// Overwrites the albedo of each listed material in the device scene, in
+// place: renderers made from the scene read it at their next render
+// (captured graphs keep the materials' address, not their contents).
+wf_status wf_scene_set_albedos(wf_scene* s, const uint32_t* materials, const float* rgb, uint32_t count) {
+    if (!s || (count && (!materials || !rgb))) return fail(WF_ERR_INVALID_ARG, "null argument");
+    for (uint32_t k = 0; k < count; ++k) {
+        if (materials[k] >= s->material_count)
+            return fail(WF_ERR_INVALID_ARG, "material %u out of range (%u materials)", materials[k], s->material_count);
+        for (int c = 0; c < 3; ++c)
+            if (!std::isfinite(rgb[3 * k + c])) return fail(WF_ERR_INVALID_ARG, "albedo of material %u is not finite",
+                                                            materials[k]);
+    }
+    WF_CUDA(cudaDeviceSynchronize());  // no kernel may be reading the materials
+    for (uint32_t k = 0; k < count; ++k) {
+        // the scene owns the array; the view only exposes it read-only to kernels
+        char* dst = const_cast<char*>(reinterpret_cast<const char*>(s->view.materials + materials[k])) +
+                    offsetof(wf::Material, albedo);
+        WF_CUDA(cudaMemcpy(dst, rgb + 3 * size_t(k), 3 * sizeof(float), cudaMemcpyHostToDevice));
+    }
     return WF_OK;
 }
 

@@ -210,6 +210,7 @@ def declare(lib):
         "wf_material_default": (None, [P, U32]),
         "wf_scene_create": (S, [C.POINTER(SceneDesc), C.POINTER(P)]),
         "wf_scene_set_environment": (S, [P, C.POINTER(Environment)]),
+        "wf_scene_set_albedos": (S, [P, P, P, U32]),
         "wf_scene_destroy": (S, [P]),
         "wf_scene_get_info": (S, [P, C.POINTER(SceneInfo)]),
         "wf_bvh_build": (S, [U32, P, U32, P, P]),

@@ -202,6 +202,13 @@ class DeviceScene:
         check(library().wf_scene_get_info(self.handle, C.byref(info)))
         return info
 
+    def set_albedos(self, materials, rgb):
+        """wf_scene_set_albedos: new RGB albedos (len(materials), 3) for the
+        listed materials, in place on the device."""
+        ids = np.ascontiguousarray(materials, np.uint32).reshape(-1)
+        values = np.ascontiguousarray(rgb, np.float32).reshape(len(ids), 3)
+        check(library().wf_scene_set_albedos(self.handle, ids.ctypes.data, values.ctypes.data, len(ids)))
+
     def set_environment(self, environment):
         lib = library()
         if environment is None:
